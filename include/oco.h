@@ -1,0 +1,139 @@
+/*
+ * oco.h -- C ABI of the B200 engine for ocotillo's per-column, per-wavelength radiative
+ * transfer (Saha ionization -> continuous H opacities -> Feautrier solve along z).
+ *
+ * The engine replaces the reference's xy/lambda loop, source/flux_feautrier.f90:160-228,
+ * and the module state it reads (wavelength tables, gas-state and grey parameters, grid
+ * spacing).  The caller keeps everything around that loop: namelist input, the synthetic
+ * disk or Athena reader, and the output writers.
+ *
+ * Plain types only (int32_t, int64_t, double, pointers), so Fortran binds it with
+ * ISO_C_BINDING, Python with ctypes.  All functions return 0 (OCO_OK) or a negative OCO_E*
+ * code; oco_last_error() gives the message.  A context is used by one host thread at a
+ * time (the reference is single-threaded); separate contexts may run concurrently.
+ *
+ * Array layouts
+ *   OCO_LAYOUT_REFERENCE (Fortran column-major, exactly the reference's arrays):
+ *     rho, T       (nz, ny, nx)        z fastest          flux_feautrier.f90:42 rho3d/temp3d
+ *     U            (nz+6, ny, nx, nw)  ghosts included    flux_feautrier.f90:36
+ *     kappa, V     (nz, ny, nx, nw)                       flux_feautrier.f90:37
+ *     Vtop, Vbot   (ny, nx, nw)        V at z index nz (top) and 1 (bottom)
+ *   OCO_LAYOUT_LAMBDA_FASTEST (device-native, coalesced for one thread per (column, lambda)):
+ *     U [nz+6][ny*nx][nw], kappa and V [nz][ny*nx][nw] (C order, lambda fastest);
+ *     rho, T, Vtop, Vbot as in the reference layout.
+ *   Column index col = ix*ny + iy (y fastest), as in the reference's loops.
+ */
+#ifndef OCO_H
+#define OCO_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OCO_ABI_VERSION 1
+
+/* Return codes.  The first group mirrors the reference's 'print ... ; stop' sites. */
+#define OCO_OK 0
+#define OCO_EINVAL (-1)      /* bad argument or dimension (nz < 2, nw < 1, NULL input) */
+#define OCO_ENOMEM (-2)      /* allocation failed; flux_feautrier.f90:95-104 */
+#define OCO_EZEROPIVOT (-3)  /* a Thomas pivot was exactly 0; auxiliary.f90:27-39 */
+#define OCO_EGREY (-4)       /* grey RT with nw != 1; flux_feautrier.f90:84-87 */
+#define OCO_ECUDA (-5)       /* CUDA runtime error */
+#define OCO_ETIMEDOUT (-6)   /* a bounded wait ran out (serving loop) */
+#define OCO_EAGAIN (-7)      /* result not ready yet (serving loop) */
+#define OCO_EADMIT (-8)      /* job refused: its footprint exceeds the admission limit */
+#define OCO_EIO (-9)         /* missing or truncated input file; read_athena.f90:112-116 */
+#define OCO_EDIM (-10)       /* input dimensions do not match; read_athena.f90:124-137 */
+#define OCO_ENOWAVES (-11)   /* oco_set_wavelengths was not called or nw mismatches */
+#define OCO_ENAN (-12)       /* rho_floor not set; read_athena.f90:243-247 */
+#define OCO_ECLOSED (-13)    /* serving loop is shut down */
+
+/* Solver forms. */
+#define OCO_FORM_PLAIN 0  /* the reference's FP64 arithmetic, operation for operation */
+#define OCO_FORM_STABLE 1 /* FP64, difference-form Thomas pivots (no cancellation) */
+#define OCO_FORM_MIXED 2  /* FP64 Saha; FP32 log-space opacities, pivots and back-substitution */
+
+#define OCO_LAYOUT_REFERENCE 0
+#define OCO_LAYOUT_LAMBDA_FASTEST 1
+
+typedef struct oco_ctx oco_ctx;
+
+/* Per-block parameters: the module state the reference's loop reads.
+ *   nx, ny         nxloc, nyloc of resolution.in (columns of this block)
+ *   nz, nw         resolution.in (run-time here)
+ *   dz             grid spacing in cm (flux_feautrier.f90:151-154 derives dz1, dz2)
+ *   sigma_grey     &input sigma_grey (cm^2/g), used when lgrey != 0
+ *   fully_ionized_T  &gas_state_input fully_ionized_T (K), gas_state.f90:70-74
+ *   lgrey          &input lgrey (grey RT; requires nw == 1)
+ *   form           OCO_FORM_*
+ *   layout         OCO_LAYOUT_* (device-array entry points only; host arrays always use
+ *                  the reference layout) */
+typedef struct oco_params {
+  int32_t nx, ny, nz, nw;
+  double dz;
+  double sigma_grey;
+  double fully_ionized_T;
+  int32_t lgrey;
+  int32_t form;
+  int32_t layout;
+  int32_t reserved; /* must be 0 */
+} oco_params;
+
+/* ABI version of the loaded library (OCO_ABI_VERSION). */
+int oco_abi_version(void);
+
+/* Creates a context on CUDA device `device` (streams, workspace, wavelength tables).
+ * No reference counterpart: replaces the reference's module-level state and the static
+ * allocations of flux_feautrier.f90:36-37, 94-104. */
+int oco_create(oco_ctx **ctx, int device);
+
+/* Releases the context and its device memory. */
+void oco_destroy(oco_ctx *ctx);
+
+/* Message of the last failed call on this context (or on this thread when ctx is NULL). */
+const char *oco_last_error(const oco_ctx *ctx);
+
+/* Linear wavelength grid in Angstrom: wa[i] = w0 + i*(w1-w0)/(nw-1); nw == 1 gives w0.
+ * Replaces calc_wavelength, continuous_opacity.f90:37-62 (argument order as there). */
+int oco_calc_wavelength(double w1, double w0, int32_t nw, double *wa);
+
+/* Builds the wavelength tables (chi, nu, lambda^3, H- fits, bound-free Gaunt factors, ...)
+ * for an arbitrary grid wa[nw] (Angstrom) and uploads them.  Replaces
+ * pre_calc_opacity_quantities, continuous_opacity.f90:64-141.  Must precede a solve. */
+int oco_set_wavelengths(oco_ctx *ctx, const double *wa_angstrom, int32_t nw);
+
+/* The xy/lambda loop of one block on HOST arrays (reference layout), including the
+ * host<->device copies.  Replaces flux_feautrier.f90:160-228 (and the stores at :205,
+ * :215-216).  U is required; kappa, V, Vtop, Vbot may be NULL.  Returns OCO_EZEROPIVOT
+ * when some (column, wavelength) met an exactly zero pivot (all other results are
+ * written; oco_last_error names the first such item). */
+int oco_solve_block(oco_ctx *ctx, const oco_params *p, const double *rho, const double *T,
+                    double *U, double *kappa, double *V, double *Vtop, double *Vbot);
+
+/* Same loop on DEVICE arrays (p->layout selects the output layout), enqueued on `stream`
+ * (a cudaStream_t; NULL is the CUDA default stream); returns after enqueueing.  Zero pivots are
+ * reported by the next oco_synchronize.  Outputs may be NULL except U.  The inputs must stay
+ * valid and the outputs untouched until the stream reaches this work. */
+int oco_solve_block_device(oco_ctx *ctx, const oco_params *p, const double *rho,
+                           const double *T, double *U, double *kappa, double *V,
+                           double *Vtop, double *Vbot, void *stream);
+
+/* Waits for the context's work; returns OCO_EZEROPIVOT if a device-array solve since the
+ * last call met a zero pivot. */
+int oco_synchronize(oco_ctx *ctx);
+
+/* Number of kernel launches this context has issued since creation (for accounting). */
+int64_t oco_kernel_launches(const oco_ctx *ctx);
+
+/* Kernel timing: when enabled, every pillar and solve launch is bracketed by CUDA events
+ * on its stream.  oco_kernel_times waits for the recorded launches, returns the summed
+ * durations (ms) and the number of solve launches since the last call, and resets them. */
+int oco_set_profiling(oco_ctx *ctx, int enable);
+int oco_kernel_times(oco_ctx *ctx, double *solve_ms, double *pillars_ms, int64_t *solve_launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OCO_H */

@@ -1,0 +1,13 @@
+"""ocotillo_b200: B200-native engine for ocotillo's per-column, per-wavelength radiative
+transfer (Saha ionization -> continuous H opacities -> Feautrier solve along z).
+
+The compute path is the CUDA library liboco_b200.so behind the C ABI in include/oco.h;
+this package is its Python binding (ctypes, with numpy host arrays or torch device
+tensors).  There is no CPU fallback: if the library is missing, importing the binding
+raises.
+"""
+from .engine import (Engine, OcoError, FORM_PLAIN, FORM_STABLE, FORM_MIXED, LAYOUT_REFERENCE,
+                     LAYOUT_LAMBDA_FASTEST, calc_wavelength, load_library)
+
+__all__ = ["Engine", "OcoError", "FORM_PLAIN", "FORM_STABLE", "FORM_MIXED", "LAYOUT_REFERENCE",
+           "LAYOUT_LAMBDA_FASTEST", "calc_wavelength", "load_library"]

@@ -1,0 +1,404 @@
+/*
+ * kernels_fp64.cu -- the FP64 hot path on sm_100a.
+ *
+ *   k_pillars   one thread per (column, z): Saha ionization and every factor of the
+ *               reference's per-(z, lambda) opacity that depends on z only
+ *               (gas_state.f90:30-110, continuous_opacity.f90:143-163 and the z-only
+ *               parts of :203-300).  Hoisting changes no bits: each hoisted expression is
+ *               the reference's expression with its operand order.
+ *   k_solve     persistent kernel, one thread per (column, wavelength), warps take tasks
+ *               of 32 consecutive items (lambda fastest) from a device counter.  Per item:
+ *               opacity, albedo and source function (continuous_opacity.f90:175-201,
+ *               :377-409), tridiagonal coefficients (auxiliary.f90:111-201), the Thomas
+ *               forward sweep (auxiliary.f90:14-41) streaming gamma, u and 1/kappa to a
+ *               per-warp-slot scratch, then the back-substitution (:43-45), ghost zones
+ *               (:49-62) and 6th-order flux (:64-109) in one reverse sweep with a 7-point
+ *               register window.
+ *
+ * This translation unit is compiled with -fmad=false (no FMA contraction) and IEEE
+ * division/square root, and calls the ocomath functions, so FORM_PLAIN reproduces the CPU
+ * oracle (ocomath back-end) bit for bit.  FORM_STABLE replaces the pivot recursion
+ * bet_j = b_j - a_j*gam_j by its difference form (no cancellation; same linear system).
+ */
+#include <cuda_runtime.h>
+
+#include "ocomath.h"
+#include "oco_consts.h"
+#include "oco_internal.h"
+
+namespace oco {
+using namespace k;
+
+#if defined(__CUDACC__) && !defined(__CUDACC_RTC__)
+#if defined(__FMA__) || defined(__USE_FAST_MATH__)
+#error "kernels_fp64.cu must be compiled without fast math"
+#endif
+#endif
+
+/* ---- pillars ------------------------------------------------------------------------ */
+__global__ void __launch_bounds__(256) k_pillars(const double *__restrict__ rho,
+                                                 const double *__restrict__ T, int64_t n,
+                                                 double fully_ionized_T, int grey,
+                                                 double *__restrict__ pil) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double r = rho[i], t = T[i];
+  double *o = pil + i * NF;
+  if (grey) { /* grey_parameters, continuous_opacity.f90:383-384 */
+    double t2 = t * t;
+    o[G_RHO] = r;
+    o[G_S] = sigma_sb * (t2 * t2);
+    o[G_ALPHA] = (3.68e22 * oco_pow(t, -3.5)) * r;
+    return;
+  }
+  const double rho1 = 1.0 / r; /* gas_state.f90:34-35 */
+  const double T1 = 1.0 / t;
+  /* calc_hydrogen_ion_frac, gas_state.f90:57-74 */
+  double constants = saha_const * oco_pow(t, 1.5);
+  double exparg = (T1 * hydrogen_ionization_eV) * k1_eV;
+  double niine_ni = constants * oco_exp(-exparg);
+  double c_ion = (mp * rho1) * niine_ni;
+  double x = 0.5 * (sqrt(c_ion * c_ion + 4.0 * c_ion) - c_ion);
+  if (t > fully_ionized_T) x = 1.0;
+  /* solve_gas_state, gas_state.f90:85-97 */
+  double nn = r * mp1;
+  double invn = rho1 * mp;
+  double nHII = x * nn;
+  double nHI = nn - nHII;
+  double ne = nHII;
+  double ionf = (nHI != 0.0) ? nHI / (nHI + nHII) : 0.0;
+  double Pe = (ne * k_cgs) * t;                    /* gas_state.f90:108 */
+  double escat = (alpha_e * nHII) * invn;          /* c_o :149 */
+  double theta = 5040.0 * T1;                      /* gas_state.f90:40-43 */
+  double theta1 = 1.0 / theta;
+  double lgt = oco_log10(theta);
+  double hmbf = ((4.158e-10 * Pe) * oco_pow(theta, 2.5)) * oco_pow(10.0, 0.754 * theta); /* c_o :161 */
+  /* z-only factors of get_kappa_H_bf, c_o :234-242.  chi_n(n) = Ry*(1 - 1*(1/n)**2) as
+   * in pre_calc_opacity_quantities :121-129; chi_m equals chi_n(6). */
+  double ktemp = k_cgs * t, ktemp1 = k1_cgs * T1;
+  double E[6];
+#pragma unroll
+  for (int nq = 1; nq <= 6; nq++) {
+    double n1 = 1.0 / (double)nq;
+    double chi_n = RydbergEnergy * (1.0 - 1.0 * (n1 * n1));
+    E[nq - 1] = oco_exp(-(chi_n * ktemp1));
+  }
+  double unsold = ((0.5 * ktemp) * RydbergEnergy1) * (E[5] - oco_exp(-(RydbergEnergy * ktemp1)));
+  o[F_RHO] = r;
+  o[F_RHO1] = rho1;
+  o[F_T1] = T1;
+  o[F_DFT1] = damping_factor_const * T1;
+  o[F_THETA] = theta;
+  o[F_TH1L] = theta1 * log10e;
+  o[F_LGT] = lgt;
+  o[F_LGT2] = lgt * lgt;
+  o[F_IONF] = ionf;
+  o[F_ESCAT] = escat;
+  o[F_ESCM] = escat * mp1;
+  o[F_HMBF] = hmbf;
+  o[F_NEUTRAL] = ((1.0 - x) > switch_ionfraction) ? 1.0 : 0.0;
+#pragma unroll
+  for (int q = 0; q < 6; q++) o[F_E1 + q] = E[q];
+  o[F_UNSOLD] = unsold;
+  o[F_AFF] = ((ionf * ne) * k_cgs) * t;                                             /* c_o :339 */
+  o[F_EF] = (((0.5 * log10e) * theta1) * Iev1) * oco_pow(10.0, -(theta * Iev));   /* c_o :265 */
+  o[F_TPOW] = oco_pow(t * 1e-4, -1.5);                                              /* c_o :290 */
+  o[F_LZ] = (oco_log(ne * (nHI + nHII)) + 2.0 * oco_log(1.0)) - 0.5 * oco_log(t);   /* c_o :292-294 */
+  o[F_LNRHO] = oco_log(r);
+  o[F_PAD] = 0.0;
+}
+
+/* ---- per-wavelength constants ------------------------------------------------------- */
+struct Lam {
+  double chi, chi1, gff, wa3, s, hmon, f1, f2, f3, gn[6], nu9, l3nu, hnuk, wcm1, sw5;
+};
+
+__device__ __forceinline__ void load_lam(Lam &L, const double *__restrict__ lam, int iw, int nw) {
+#define LD(f) __ldg(lam + (int64_t)(f) * nw + iw)
+  L.chi = LD(L_CHI);
+  L.chi1 = LD(L_CHI1);
+  L.gff = LD(L_GFF);
+  L.wa3 = LD(L_WA3);
+  L.s = LD(L_SCOEF);
+  L.hmon = LD(L_HMON);
+  L.f1 = LD(L_F1);
+  L.f2 = LD(L_F2);
+  L.f3 = LD(L_F3);
+#pragma unroll
+  for (int q = 0; q < 6; q++) L.gn[q] = LD(L_GN1 + q);
+  L.nu9 = LD(L_NU9);
+  L.l3nu = LD(L_L3NU);
+  L.hnuk = LD(L_HNUK);
+  L.wcm1 = LD(L_WCM1);
+  L.sw5 = LD(L_SW5);
+#undef LD
+}
+
+struct Opac {
+  double op, alb, S;
+};
+
+/* calc_opacity_and_albedo for one (z, lambda), continuous_opacity.f90:175-201 with
+ * :171, :233-244, :318-322, :337-339, :261-277, :290-298, :399-407. */
+__device__ __forceinline__ Opac opacity_at(const double *__restrict__ P, const Lam &L) {
+  const double theta = __ldg(P + F_THETA);
+  const double ionf = __ldg(P + F_IONF);
+  const double stim = 1.0 - oco_pow(10.0, -(L.chi * theta));
+  double sm = 0.0;
+#pragma unroll
+  for (int q = 0; q < 6; q++) sm = sm + L.gn[q] * __ldg(P + F_E1 + q);
+  double kHbf = (((AHbf * stim) * ionf) * L.wa3) * (__ldg(P + F_UNSOLD) + sm);
+  double kHmbf = (L.hmon != 0.0) ? ((__ldg(P + F_HMBF) * stim) * ionf) * L.s : 0.0;
+  double flam = ((L.f1 + L.f2 * __ldg(P + F_LGT)) + L.f3 * __ldg(P + F_LGT2)) - 26.0;
+  double kHmff = __ldg(P + F_AFF) * oco_pow(10.0, flam);
+  double kr = (((kHbf + kHmbf) + kHmff) + __ldg(P + F_ESCAT)) * mp1;
+  const double rho = __ldg(P + F_RHO);
+  double op = kr * rho;
+  if (__ldg(P + F_NEUTRAL) != 0.0) {
+    double g_ff = 1.0 + L.gff * ((__ldg(P + F_TH1L) * L.chi1) + 0.5);
+    double kHff = ((((stim * ionf) * alpha0) * L.wa3) * g_ff) * __ldg(P + F_EF);
+    kr = kr + kHff * mp1;
+    op = op + kr * rho;
+  } else {
+    double gaunt = oco_log(oco_exp(5.960 - (sqrt3 * pi1) * oco_log(L.nu9 * __ldg(P + F_TPOW))) + exp1);
+    double lnq = (__ldg(P + F_LZ) - L.l3nu) + oco_log(1.0 - oco_exp(-(L.hnuk * __ldg(P + F_T1))));
+    double krho = (bremsstrahlung_constant * oco_exp(lnq)) * gaunt;
+    op = op + krho;
+    kr = kr + op * __ldg(P + F_RHO1);
+  }
+  Opac o;
+  o.op = op;
+  o.alb = __ldg(P + F_ESCM) / kr;
+  double damping = __ldg(P + F_DFT1) * L.wcm1;
+  if (damping > log_overflow_limit) damping = log_overflow_limit;
+  o.S = L.sw5 / (oco_exp(damping) - 1.0);
+  return o;
+}
+
+/* grey_parameters, continuous_opacity.f90:377-390 */
+__device__ __forceinline__ Opac opacity_grey(const double *__restrict__ P, double sg) {
+  double alpha = __ldg(P + G_ALPHA);
+  Opac o;
+  o.op = (alpha + sg) * __ldg(P + G_RHO);
+  o.alb = sg / (alpha + sg);
+  o.S = __ldg(P + G_S);
+  return o;
+}
+
+/* ---- the solve ----------------------------------------------------------------------- */
+template <int FORM, bool GREY>
+__device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int iw,
+                                           double *__restrict__ gam, double *__restrict__ uu,
+                                           double *__restrict__ o1s) {
+  const int nz = a.nz;
+  const int64_t ss = a.slot_stride;
+  const double *__restrict__ P = a.pil + cl * (int64_t)nz * NF;
+  Lam L;
+  if (!GREY) load_lam(L, a.lam, iw, a.nw);
+  const int64_t idx = (a.layout == 0) ? (int64_t)iw * a.ld_col + a.c_off + cl
+                                      : (a.c_off + cl) * a.nw + iw;
+  double *Ub = a.U + idx * a.U_is;
+  double *Kb = a.K ? a.K + idx * a.K_is : nullptr;
+  double *Vb = a.V ? a.V + idx * a.V_is : nullptr;
+  const double dz = a.dz, dz2 = a.dz2;
+  bool bad = false;
+
+  /* forward sweep: row 0 (fill_boundary_coeffs :187-191) */
+  Opac cur = GREY ? opacity_grey(P, a.sigma_grey) : opacity_at(P, L);
+  Opac nxt = GREY ? opacity_grey(P + NF, a.sigma_grey) : opacity_at(P + NF, L);
+  double o1 = 1.0 / cur.op, o2 = cur.op * cur.op;
+  double zeta = ((cur.op * dz2) * (1.0 - cur.alb)) * 0.25;
+  double bet, h = 0.0;
+  if (FORM == 0) {
+    bet = -(((o1 + dz) + zeta) * o2);
+  } else {
+    h = (dz + zeta) * o2;
+    bet = -(cur.op + h);
+  }
+  if (bet == 0.0) bad = true;
+  double u = (-((cur.S * zeta) * o2)) / bet;
+  uu[0] = u;
+  o1s[0] = o1;
+  if (Kb) Kb[0] = cur.op;
+  double c_prev = cur.op;
+  double kh_prev = 0.5 * (nxt.op + cur.op); /* kappa_p(1) = kappa_m(2), :147-154 */
+  cur = nxt;
+  for (int j = 1; j < nz; j++) {
+    const double op = cur.op;
+    o1 = 1.0 / op;
+    o2 = op * op;
+    double aa, bb, cc, dd, ee;
+    if (j < nz - 1) { /* fill_center_coeffs :159-165 */
+      nxt = GREY ? opacity_grey(P + (int64_t)(j + 1) * NF, a.sigma_grey)
+                 : opacity_at(P + (int64_t)(j + 1) * NF, L);
+      aa = o2 / kh_prev;
+      double kh = 0.5 * (nxt.op + op);
+      cc = o2 / kh;
+      double z3 = (dz2 * (op * (op * op))) * (1.0 - cur.alb);
+      bb = -((aa + cc) + z3);
+      dd = -(cur.S * z3);
+      ee = z3;
+      kh_prev = kh;
+    } else { /* fill_boundary_coeffs :193-197 */
+      aa = op;
+      double zt = ((op * dz2) * (1.0 - cur.alb)) * 0.25;
+      bb = -(((o1 + dz) + zt) * o2);
+      cc = 0.0;
+      dd = -((cur.S * zt) * o2);
+      ee = (dz + zt) * o2;
+    }
+    double g;
+    if (FORM == 0) { /* tridag :34-35 */
+      g = c_prev / bet;
+      bet = bb - aa * g;
+    } else { /* difference form: bet = -(c + h), h = e + a*h_prev/(c_prev + h_prev) */
+      double den = c_prev + h;
+      g = -(c_prev / den);
+      h = ee + (aa * h) / den;
+      bet = -(cc + h);
+      (void)bb;
+    }
+    if (bet == 0.0) bad = true;
+    u = (dd - aa * u) / bet; /* tridag :40 */
+    gam[j * ss] = g;
+    uu[j * ss] = u;
+    o1s[j * ss] = o1;
+    if (Kb) Kb[j * a.K_zs] = op;
+    c_prev = cc;
+    cur = nxt;
+  }
+  if (bad) {
+    atomicAdd(&a.status[0], 1ull);
+    atomicMin(&a.status[1], (unsigned long long)((a.c_off + cl) * a.nw + iw));
+  }
+
+  /* reverse sweep: back-substitution (tridag :43-45), ghosts (:49-62), flux (:96-109) */
+  const double dz1 = a.dz1;
+  const int64_t uz = a.U_zs;
+  double vtop = 0.0, vbot = 0.0;
+  if (nz >= 4) {
+    auto emitV = [&](int j, double w0, double w1, double w2, double w3, double w4, double w5,
+                     double w6) -> double {
+      double df = (1.0 / 60.0) * (((45.0 * (w4 - w2)) - 9.0 * (w5 - w1)) + (w6 - w0));
+      double v = ((-1.0 * o1s[j * ss]) * df) * dz1;
+      if (Vb) Vb[j * a.V_zs] = v;
+      return v;
+    };
+    const int n = nz;
+    double u1 = u; /* U_{n-1} */
+    double u2 = uu[(n - 2) * ss] - gam[(n - 1) * ss] * u1;
+    double u3 = uu[(n - 3) * ss] - gam[(n - 2) * ss] * u2;
+    double u4 = uu[(n - 4) * ss] - gam[(n - 3) * ss] * u3;
+    Ub[(3 + n - 1) * uz] = u1;
+    Ub[(3 + n - 2) * uz] = u2;
+    Ub[(3 + n - 3) * uz] = u3;
+    Ub[(3 + n - 4) * uz] = u4;
+    double g1 = 2.0 * u1 - u2, g2 = 2.0 * u1 - u3, g3 = 2.0 * u1 - u4;
+    Ub[(n + 3) * uz] = g1;
+    Ub[(n + 4) * uz] = g2;
+    Ub[(n + 5) * uz] = g3;
+    double w0 = u4, w1 = u3, w2 = u2, w3 = u1, w4 = g1, w5 = g2, w6 = g3;
+    vtop = emitV(n - 1, w0, w1, w2, w3, w4, w5, w6);
+    for (int kk = n - 5; kk >= 0; kk--) {
+      double Uk = uu[kk * ss] - gam[(kk + 1) * ss] * w0;
+      Ub[(3 + kk) * uz] = Uk;
+      w6 = w5; w5 = w4; w4 = w3; w3 = w2; w2 = w1; w1 = w0; w0 = Uk;
+      emitV(kk + 3, w0, w1, w2, w3, w4, w5, w6);
+    }
+    double b1 = 2.0 * w0 - w1, b2 = 2.0 * w0 - w2, b3 = 2.0 * w0 - w3;
+    Ub[2 * uz] = b1;
+    Ub[1 * uz] = b2;
+    Ub[0] = b3;
+    w6 = w5; w5 = w4; w4 = w3; w3 = w2; w2 = w1; w1 = w0; w0 = b1;
+    emitV(2, w0, w1, w2, w3, w4, w5, w6);
+    w6 = w5; w5 = w4; w4 = w3; w3 = w2; w2 = w1; w1 = w0; w0 = b2;
+    emitV(1, w0, w1, w2, w3, w4, w5, w6);
+    w6 = w5; w5 = w4; w4 = w3; w3 = w2; w2 = w1; w1 = w0; w0 = b3;
+    vbot = emitV(0, w0, w1, w2, w3, w4, w5, w6);
+  } else { /* nz = 2 or 3: the reference's ghost update order matters (ghosts feed ghosts) */
+    double f[9];
+    const int n1 = 3, n2 = nz + 2;
+    f[n1 + nz - 1] = u;
+    for (int j = nz - 2; j >= 0; j--) f[n1 + j] = uu[j * ss] - gam[(j + 1) * ss] * f[n1 + j + 1];
+    for (int i = 1; i <= 3; i++) {
+      f[n1 - i] = 2.0 * f[n1] - f[n1 + i];
+      f[n2 + i] = 2.0 * f[n2] - f[n2 - i];
+    }
+    for (int m = 0; m < nz + 6; m++) Ub[m * uz] = f[m];
+    for (int j = 0; j < nz; j++) {
+      int c = n1 + j;
+      double df = (1.0 / 60.0) * (((45.0 * (f[c + 1] - f[c - 1])) - 9.0 * (f[c + 2] - f[c - 2])) +
+                                  (f[c + 3] - f[c - 3]));
+      double v = ((-1.0 * o1s[j * ss]) * df) * dz1;
+      if (Vb) Vb[j * a.V_zs] = v;
+      if (j == 0) vbot = v;
+      if (j == nz - 1) vtop = v;
+    }
+  }
+  const int64_t pidx = (int64_t)iw * a.ld_col + a.c_off + cl;
+  if (a.Vtop) a.Vtop[pidx] = vtop;
+  if (a.Vbot) a.Vbot[pidx] = vbot;
+}
+
+template <int FORM, bool GREY>
+__global__ void __launch_bounds__(128) k_solve(const SolveArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nitems = a.ncol * a.nw;
+  const unsigned long long ntasks = (unsigned long long)((nitems + 31) / 32);
+  double *gam = a.gam + slot * 32 + lane;
+  double *uu = a.uu + slot * 32 + lane;
+  double *o1 = a.o1 + slot * 32 + lane;
+  for (;;) {
+    unsigned long long task = 0;
+    if (lane == 0) task = atomicAdd(a.work, 1ull);
+    task = __shfl_sync(0xffffffffu, task, 0);
+    if (task >= ntasks) break;
+    const int64_t item = (int64_t)task * 32 + lane;
+    if (item < nitems) {
+      const int64_t cl = item / a.nw;
+      const int iw = (int)(item - cl * a.nw);
+      solve_item<FORM, GREY>(a, cl, iw, gam, uu, o1);
+    }
+  }
+}
+
+cudaError_t launch_pillars(const double *rho, const double *T, int64_t ncol, int nz,
+                           double fully_ionized_T, int grey, double *pil, cudaStream_t s) {
+  int64_t n = ncol * nz;
+  if (n == 0) return cudaSuccess;
+  int threads = 256;
+  int64_t blocks = (n + threads - 1) / threads;
+  k_pillars<<<(unsigned)blocks, threads, 0, s>>>(rho, T, n, fully_ionized_T, grey, pil);
+  return cudaGetLastError();
+}
+
+static const void *solve_fn(int form, int grey) {
+  if (form == 0) return grey ? (const void *)k_solve<0, true> : (const void *)k_solve<0, false>;
+  return grey ? (const void *)k_solve<1, true> : (const void *)k_solve<1, false>;
+}
+
+int solve_fp64_max_blocks_per_sm(int form, int grey, int threads) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, solve_fn(form, grey), threads, 0) != cudaSuccess)
+    return 1;
+  return nb > 0 ? nb : 1;
+}
+
+cudaError_t launch_solve_fp64(const SolveArgs &a, int form, int grey, int blocks, int threads,
+                              cudaStream_t s) {
+  if (form == 0) {
+    if (grey)
+      k_solve<0, true><<<blocks, threads, 0, s>>>(a);
+    else
+      k_solve<0, false><<<blocks, threads, 0, s>>>(a);
+  } else {
+    if (grey)
+      k_solve<1, true><<<blocks, threads, 0, s>>>(a);
+    else
+      k_solve<1, false><<<blocks, threads, 0, s>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace oco

@@ -1,0 +1,552 @@
+/*
+ * oco_api.cu -- the C ABI (include/oco.h): context, wavelength tables, workspace, and the
+ * block solve on host or device arrays.
+ *
+ * A block solve runs in column chunks.  For each chunk: the pillar kernel computes the
+ * wavelength-independent per-(column, z) quantities, then the persistent solve kernel
+ * processes the chunk's (column, wavelength) items.  The device-array entry point writes
+ * straight into the caller's arrays (either layout); the host-array entry point stages
+ * each chunk through device buffers in the reference layout and copies them back with one
+ * pitched copy per output, overlapping the next chunk's kernels with the copy-back.
+ */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/oco.h"
+#include "ocomath.h"
+#include "oco_consts.h"
+#include "oco_internal.h"
+
+using namespace oco;
+
+static thread_local std::string g_thread_err;
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t n = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= n) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaSuccess) n = bytes;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  template <class T>
+  T *as() const {
+    return (T *)p;
+  }
+};
+
+/* Per-chunk staging for the host-array path (two sets, used alternately). */
+struct Stage {
+  DevBuf rho, T, U, K, V, top, bot;
+  cudaEvent_t done = nullptr; /* copy-back of this set finished */
+};
+
+struct oco_ctx {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr; /* kernels */
+  cudaStream_t copy = nullptr;   /* host<->device copies of the host-array path */
+  std::string err;
+  /* wavelength tables */
+  int nw = 0;
+  std::vector<double> wa;
+  DevBuf lam;
+  /* workspace */
+  DevBuf pil, scratch, work, status;
+  Stage stage[2];
+  int64_t launches = 0;
+  size_t budget_bytes = 8ull << 30; /* chunk budget for pillars + staged outputs */
+  /* kernel timing (oco_set_profiling) */
+  bool prof = false;
+  /* device-array calls defer the zero-pivot check to oco_synchronize */
+  bool status_pending = false;
+  cudaStream_t status_stream = nullptr;
+  oco_params status_params{};
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_solve, ev_pil;
+  cudaEvent_t take_event() {
+    if (!ev_pool.empty()) {
+      cudaEvent_t e = ev_pool.back();
+      ev_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+  }
+};
+
+static int set_err(oco_ctx *c, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  g_thread_err = buf;
+  return code;
+}
+
+#define CU(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return set_err(c, e_ == cudaErrorMemoryAllocation ? OCO_ENOMEM : OCO_ECUDA,        \
+                     "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+extern "C" int oco_abi_version(void) { return OCO_ABI_VERSION; }
+
+extern "C" const char *oco_last_error(const oco_ctx *c) {
+  return c ? c->err.c_str() : g_thread_err.c_str();
+}
+
+extern "C" int oco_create(oco_ctx **out, int device) {
+  oco_ctx *c = nullptr;
+  if (!out) return set_err(nullptr, OCO_EINVAL, "oco_create: out is NULL");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_err(nullptr, OCO_ECUDA, "oco_create: no CUDA device");
+  if (device < 0 || device >= ndev) return set_err(nullptr, OCO_EINVAL, "oco_create: bad device %d", device);
+  c = new (std::nothrow) oco_ctx();
+  if (!c) return set_err(nullptr, OCO_ENOMEM, "oco_create: out of host memory");
+  c->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking);
+  for (int i = 0; i < 2 && e == cudaSuccess; i++)
+    e = cudaEventCreateWithFlags(&c->stage[i].done, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = c->work.ensure(64);
+  if (e == cudaSuccess) e = c->status.ensure(64);
+  if (e != cudaSuccess) {
+    int code = set_err(nullptr, OCO_ECUDA, "oco_create: %s", cudaGetErrorString(e));
+    oco_destroy(c);
+    return code;
+  }
+  if (const char *g = getenv("OCO_WORKSPACE_GB")) {
+    double gb = atof(g);
+    if (gb > 0.0) c->budget_bytes = std::max<size_t>((size_t)(gb * (1ull << 30)), 1);
+  }
+  *out = c;
+  return OCO_OK;
+}
+
+extern "C" void oco_destroy(oco_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->copy) cudaStreamSynchronize(c->copy);
+  c->lam.release();
+  c->pil.release();
+  c->scratch.release();
+  c->work.release();
+  c->status.release();
+  for (auto &s : c->stage) {
+    s.rho.release();
+    s.T.release();
+    s.U.release();
+    s.K.release();
+    s.V.release();
+    s.top.release();
+    s.bot.release();
+    if (s.done) cudaEventDestroy(s.done);
+  }
+  if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->copy) cudaStreamDestroy(c->copy);
+  for (auto *v : {&c->ev_solve, &c->ev_pil})
+    for (auto &pr : *v) {
+      cudaEventDestroy(pr.first);
+      cudaEventDestroy(pr.second);
+    }
+  for (auto e : c->ev_pool) cudaEventDestroy(e);
+  delete c;
+}
+
+extern "C" int oco_calc_wavelength(double w1, double w0, int32_t nw, double *wa) {
+  if (nw < 1 || !wa) return set_err(nullptr, OCO_EINVAL, "oco_calc_wavelength: nw < 1 or NULL wa");
+  if (nw > 1) { /* continuous_opacity.f90:48-54 */
+    double dw = (w1 - w0) / (double)(nw - 1);
+    for (int i = 1; i <= nw; i++) wa[i - 1] = w0 + (double)(i - 1) * dw;
+  } else {
+    wa[0] = w0;
+  }
+  return OCO_OK;
+}
+
+/* Right-to-left binary powering: the operation order of the library routine gfortran
+ * calls for REAL**INTEGER with a non-constant exponent (continuous_opacity.f90:108, :136). */
+static double powi_var(double x, int m) {
+  unsigned n = m < 0 ? -(unsigned)m : (unsigned)m;
+  double y = (n % 2) ? x : 1.0;
+  while (n >>= 1) {
+    x = x * x;
+    if (n % 2) y = y * x;
+  }
+  return m < 0 ? 1.0 / y : y;
+}
+
+/* gaunt, continuous_opacity.f90:343-375 */
+static double gaunt_bf(int n, double wave_cm) {
+  double lam_n = (double)(n * n) * k::hcR1;
+  if (wave_cm <= lam_n) {
+    double t = (wave_cm / lam_n) - 1.0;
+    double eps2 = t * t;
+    return 1.0 - (0.17285714285714285 * (1.0 - eps2)) * std::pow((double)n * (1.0 + eps2), -k::two_thirds);
+  }
+  return 0.0;
+}
+
+/* pre_calc_opacity_quantities (continuous_opacity.f90:64-141) with the C library's pow and
+ * log10, as the reference; then the hot loop's lambda-only factors (ocomath, as the
+ * device computes everything inside the loop). */
+static void build_lambda_table(const double *waves, int nw, std::vector<double> &tab) {
+  static const double a_coeff[7] = {+1.99654,     -1.18267e-6,  +2.62423e-7, -4.40524e-11,
+                                    +3.23992e-15, -1.39568e-19, +2.78701e-24};
+  static const double b_coeff[3][5] = {{-2.276300, -1.685000, +0.766610, -0.053356, +0.000000},
+                                       {+15.28270, -9.284600, +1.993810, -0.142631, +0.000000},
+                                       {-197.789, +190.266, -67.9775, +10.6913, -0.62515}};
+  tab.assign((size_t)NL * nw, 0.0);
+  auto T = [&](int f, int iw) -> double & { return tab[(size_t)f * nw + iw]; };
+  for (int iw = 0; iw < nw; iw++) {
+    const double wa = waves[iw];
+    const double wcm = wa * 1e-8;
+    const double wcm1 = 1.0 / wcm;
+    const double nu = k::c_light * wcm1;
+    const double chi = 1.2398e4 / wa;
+    const double x2 = wcm1 * wcm1;
+    const double w1cm5 = x2 * (wcm1 * x2);
+    double s = 0.0;
+    for (int i = 1; i <= 7; i++) s = s + (1e-17 * a_coeff[i - 1]) * powi_var(wa, i - 1);
+    const double lg = std::log10(wa);
+    T(L_CHI, iw) = chi;
+    T(L_CHI1, iw) = 1.0 / chi;
+    T(L_GFF, iw) = 0.3456 * std::pow(wa * k::Rangstrom, -k::one_third);
+    T(L_WA3, iw) = wa * (wa * wa);
+    T(L_SCOEF, iw) = s;
+    T(L_HMON, iw) = (wa < 16000.0) ? 1.0 : 0.0;
+    for (int i = 0; i < 3; i++) {
+      double f = 0.0;
+      for (int j = 1; j <= 5; j++) f = f + powi_var(lg, j - 1) * b_coeff[i][j - 1];
+      T(L_F1 + i, iw) = f;
+    }
+    for (int n = 1; n <= 6; n++) {
+      double n1 = 1.0 / (double)n;
+      T(L_GN1 + n - 1, iw) = gaunt_bf(n, wcm) * (n1 * (n1 * n1));
+    }
+    T(L_NU9, iw) = nu * 1e-9;
+    T(L_L3NU, iw) = 3.0 * oco_log(nu);
+    T(L_HNUK, iw) = (k::h_planck * nu) * k::k1_cgs;
+    T(L_WCM1, iw) = wcm1;
+    T(L_SW5, iw) = k::source_function_const * w1cm5;
+    T(L_LNSW5, iw) = std::log(k::source_function_const * w1cm5);
+  }
+}
+
+extern "C" int oco_set_wavelengths(oco_ctx *c, const double *wa, int32_t nw) {
+  if (!c) return set_err(nullptr, OCO_EINVAL, "oco_set_wavelengths: NULL context");
+  if (!wa || nw < 1) return set_err(c, OCO_EINVAL, "oco_set_wavelengths: nw < 1 or NULL wa");
+  for (int i = 0; i < nw; i++)
+    if (!(wa[i] > 0.0) || !std::isfinite(wa[i]))
+      return set_err(c, OCO_EINVAL, "oco_set_wavelengths: wavelength %d is not positive", i);
+  CU(cudaSetDevice(c->device));
+  std::vector<double> tab;
+  build_lambda_table(wa, nw, tab);
+  CU(cudaStreamSynchronize(c->stream));
+  CU(c->lam.ensure(tab.size() * sizeof(double)));
+  CU(cudaMemcpy(c->lam.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
+  c->wa.assign(wa, wa + nw);
+  c->nw = nw;
+  return OCO_OK;
+}
+
+static int check_params(oco_ctx *c, const oco_params *p) {
+  if (!c) return set_err(nullptr, OCO_EINVAL, "NULL context");
+  if (!p) return set_err(c, OCO_EINVAL, "NULL params");
+  if (p->nx < 1 || p->ny < 1 || p->nz < 2 || p->nw < 1)
+    return set_err(c, OCO_EINVAL, "bad dimensions nx=%d ny=%d nz=%d nw=%d (need nz >= 2)", p->nx, p->ny,
+                   p->nz, p->nw);
+  if (p->lgrey && p->nw != 1)
+    return set_err(c, OCO_EGREY, "For Grey RT use only one wavelength. Switch nw=1 in resolution.in");
+  if (!p->lgrey && (c->nw != p->nw))
+    return set_err(c, OCO_ENOWAVES, "wavelength tables hold %d wavelengths, block has nw=%d", c->nw, p->nw);
+  if (p->form != OCO_FORM_PLAIN && p->form != OCO_FORM_STABLE && p->form != OCO_FORM_MIXED)
+    return set_err(c, OCO_EINVAL, "unknown form %d", p->form);
+  if (p->layout != OCO_LAYOUT_REFERENCE && p->layout != OCO_LAYOUT_LAMBDA_FASTEST)
+    return set_err(c, OCO_EINVAL, "unknown layout %d", p->layout);
+  if (!(p->dz > 0.0)) return set_err(c, OCO_EINVAL, "dz must be positive");
+  return OCO_OK;
+}
+
+static const int kSolveThreads = 128;
+
+/* Grid of the persistent solve kernel and its scratch (gamma, u, 1/kappa per z). */
+static int prepare_solve(oco_ctx *c, int form, int grey, int64_t nitems, int nz, int *blocks) {
+  int bps = solve_fp64_max_blocks_per_sm(form == OCO_FORM_STABLE ? 1 : 0, grey, kSolveThreads);
+  int64_t maxb = (int64_t)bps * c->num_sms;
+  int64_t need = (nitems + kSolveThreads - 1) / kSolveThreads;
+  *blocks = (int)std::max<int64_t>(1, std::min(maxb, need));
+  size_t slots = (size_t)(*blocks) * kSolveThreads;
+  CU(c->scratch.ensure(slots * (size_t)nz * 3 * sizeof(double)));
+  return OCO_OK;
+}
+
+/* Columns per chunk so that pillars (+ staged outputs on the host path) fit the budget. */
+static int64_t chunk_columns(oco_ctx *c, const oco_params *p, bool host_path) {
+  const int64_t ncol = (int64_t)p->nx * p->ny;
+  size_t per_col = (size_t)p->nz * NF * sizeof(double);
+  if (host_path)
+    per_col += 2 * ((size_t)p->nz * 2 + (size_t)p->nw * ((p->nz + 6) + 2 * (size_t)p->nz + 2)) * sizeof(double);
+  int64_t ch = (int64_t)std::max<size_t>(1, c->budget_bytes / per_col);
+  return std::min(ch, ncol);
+}
+
+/* One chunk: pillars + persistent solve. Outputs described by the strides in a. */
+static int run_chunk(oco_ctx *c, const oco_params *p, const double *rho, const double *T, int64_t nb,
+                     SolveArgs a, cudaStream_t s) {
+  const int grey = p->lgrey ? 1 : 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
+  if (c->prof) {
+    e0 = c->take_event();
+    e1 = c->take_event();
+    e2 = c->take_event();
+    e3 = c->take_event();
+    CU(cudaEventRecord(e0, s));
+  }
+  CU(launch_pillars(rho, T, nb, p->nz, p->fully_ionized_T, grey, c->pil.as<double>(), s));
+  if (c->prof) {
+    CU(cudaEventRecord(e1, s));
+    c->ev_pil.emplace_back(e0, e1);
+  }
+  int blocks = 0;
+  int rc = prepare_solve(c, p->form, grey, nb * p->nw, p->nz, &blocks);
+  if (rc) return rc;
+  size_t slots = (size_t)blocks * kSolveThreads;
+  a.pil = c->pil.as<double>();
+  a.lam = grey ? nullptr : c->lam.as<double>();
+  a.ncol = nb;
+  a.gam = c->scratch.as<double>();
+  a.uu = a.gam + slots * p->nz;
+  a.o1 = a.uu + slots * p->nz;
+  a.slot_stride = (int64_t)slots;
+  a.work = c->work.as<unsigned long long>();
+  a.status = c->status.as<unsigned long long>();
+  CU(cudaMemsetAsync(a.work, 0, sizeof(unsigned long long), s));
+  if (c->prof) CU(cudaEventRecord(e2, s));
+  CU(launch_solve_fp64(a, p->form == OCO_FORM_STABLE ? 1 : 0, grey, blocks, kSolveThreads, s));
+  if (c->prof) {
+    CU(cudaEventRecord(e3, s));
+    c->ev_solve.emplace_back(e2, e3);
+  }
+  c->launches += 2;
+  return OCO_OK;
+}
+
+/* status[0] = number of items with a zero pivot, status[1] = smallest such item index. */
+static int reset_status(oco_ctx *c, cudaStream_t s) {
+  if (c->status_pending) return OCO_OK; /* accumulate until the pending status is read */
+  CU(cudaMemsetAsync(c->status.p, 0, sizeof(unsigned long long), s));
+  CU(cudaMemsetAsync(c->status.as<unsigned long long>() + 1, 0xff, sizeof(unsigned long long), s));
+  return OCO_OK;
+}
+
+static int read_status(oco_ctx *c, cudaStream_t s, const oco_params *p) {
+  unsigned long long st[2];
+  c->status_pending = false;
+  CU(cudaMemcpyAsync(st, c->status.p, sizeof st, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  if (st[0]) {
+    unsigned long long item = st[1];
+    long long col = (long long)(item / (unsigned long long)p->nw), iw = (long long)(item % p->nw);
+    return set_err(c, OCO_EZEROPIVOT,
+                   "ERROR tridiag: bet == 0 in %llu (column, wavelength) items; first: ix=%lld iy=%lld iw=%lld",
+                   st[0], col / p->ny + 1, col % p->ny + 1, iw + 1);
+  }
+  return OCO_OK;
+}
+
+static void fill_strides(SolveArgs &a, const oco_params *p, int layout, int64_t ld_col) {
+  const int64_t mz = p->nz + 6, nz = p->nz;
+  a.layout = layout;
+  a.ld_col = ld_col;
+  if (layout == OCO_LAYOUT_REFERENCE) {
+    a.U_zs = 1;
+    a.U_is = mz;
+    a.K_zs = 1;
+    a.K_is = nz;
+    a.V_zs = 1;
+    a.V_is = nz;
+  } else {
+    const int64_t items = ld_col * p->nw;
+    a.U_zs = items;
+    a.U_is = 1;
+    a.K_zs = items;
+    a.K_is = 1;
+    a.V_zs = items;
+    a.V_is = 1;
+  }
+}
+
+extern "C" int oco_solve_block_device(oco_ctx *c, const oco_params *p, const double *rho, const double *T,
+                                      double *U, double *kappa, double *V, double *Vtop, double *Vbot,
+                                      void *stream) {
+  int rc = check_params(c, p);
+  if (rc) return rc;
+  if (p->form == OCO_FORM_MIXED) return set_err(c, OCO_EINVAL, "mixed form not available in this build");
+  if (!rho || !T || !U) return set_err(c, OCO_EINVAL, "rho, T and U are required");
+  CU(cudaSetDevice(c->device));
+  cudaStream_t s = (cudaStream_t)stream; /* NULL is the CUDA default stream */
+  const int64_t ncol = (int64_t)p->nx * p->ny;
+  const int64_t ch = chunk_columns(c, p, false);
+  CU(c->pil.ensure((size_t)ch * p->nz * NF * sizeof(double)));
+  if ((rc = reset_status(c, s))) return rc;
+  SolveArgs a{};
+  fill_strides(a, p, p->layout, ncol);
+  a.nz = p->nz;
+  a.nw = p->nw;
+  a.dz = p->dz;
+  a.dz1 = 1.0 / p->dz;
+  a.dz2 = p->dz * p->dz;
+  a.sigma_grey = p->sigma_grey;
+  for (int64_t c0 = 0; c0 < ncol; c0 += ch) {
+    const int64_t nb = std::min(ch, ncol - c0);
+    a.U = U;
+    a.K = kappa;
+    a.V = V;
+    a.Vtop = Vtop;
+    a.Vbot = Vbot;
+    a.c_off = c0;
+    if ((rc = run_chunk(c, p, rho + c0 * p->nz, T + c0 * p->nz, nb, a, s))) return rc;
+  }
+  c->status_pending = true;
+  c->status_stream = s;
+  c->status_params = *p;
+  return OCO_OK;
+}
+
+extern "C" int oco_solve_block(oco_ctx *c, const oco_params *p, const double *rho, const double *T, double *U,
+                               double *kappa, double *V, double *Vtop, double *Vbot) {
+  int rc = check_params(c, p);
+  if (rc) return rc;
+  if (p->form == OCO_FORM_MIXED) return set_err(c, OCO_EINVAL, "mixed form not available in this build");
+  if (!rho || !T || !U) return set_err(c, OCO_EINVAL, "rho, T and U are required");
+  CU(cudaSetDevice(c->device));
+  const int64_t ncol = (int64_t)p->nx * p->ny;
+  const int nz = p->nz, nw = p->nw, mz = nz + 6;
+  const int64_t ch = chunk_columns(c, p, true);
+  CU(c->pil.ensure((size_t)ch * nz * NF * sizeof(double)));
+  for (auto &st : c->stage) {
+    CU(st.rho.ensure((size_t)ch * nz * sizeof(double)));
+    CU(st.T.ensure((size_t)ch * nz * sizeof(double)));
+    CU(st.U.ensure((size_t)ch * mz * nw * sizeof(double)));
+    if (kappa) CU(st.K.ensure((size_t)ch * nz * nw * sizeof(double)));
+    if (V) CU(st.V.ensure((size_t)ch * nz * nw * sizeof(double)));
+    if (Vtop) CU(st.top.ensure((size_t)ch * nw * sizeof(double)));
+    if (Vbot) CU(st.bot.ensure((size_t)ch * nw * sizeof(double)));
+  }
+  if (c->status_pending && (rc = oco_synchronize(c))) return rc;
+  if ((rc = reset_status(c, c->stream))) return rc;
+  SolveArgs a{};
+  a.nz = nz;
+  a.nw = nw;
+  a.dz = p->dz;
+  a.dz1 = 1.0 / p->dz;
+  a.dz2 = p->dz * p->dz;
+  a.sigma_grey = p->sigma_grey;
+  int k = 0;
+  for (int64_t c0 = 0; c0 < ncol; c0 += ch, k ^= 1) {
+    const int64_t nb = std::min(ch, ncol - c0);
+    Stage &st = c->stage[k];
+    /* the previous copy-back from this staging set must be done before reuse */
+    CU(cudaStreamWaitEvent(c->stream, st.done, 0));
+    CU(cudaMemcpyAsync(st.rho.p, rho + c0 * nz, (size_t)nb * nz * sizeof(double), cudaMemcpyHostToDevice,
+                       c->stream));
+    CU(cudaMemcpyAsync(st.T.p, T + c0 * nz, (size_t)nb * nz * sizeof(double), cudaMemcpyHostToDevice,
+                       c->stream));
+    fill_strides(a, p, OCO_LAYOUT_REFERENCE, nb);
+    a.U = st.U.as<double>();
+    a.K = kappa ? st.K.as<double>() : nullptr;
+    a.V = V ? st.V.as<double>() : nullptr;
+    a.Vtop = Vtop ? st.top.as<double>() : nullptr;
+    a.Vbot = Vbot ? st.bot.as<double>() : nullptr;
+    a.c_off = 0;
+    if ((rc = run_chunk(c, p, st.rho.as<double>(), st.T.as<double>(), nb, a, c->stream))) return rc;
+    /* copy-back on the copy stream, after the kernels */
+    cudaEvent_t ready;
+    CU(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+    CU(cudaEventRecord(ready, c->stream));
+    CU(cudaStreamWaitEvent(c->copy, ready, 0));
+    CU(cudaEventDestroy(ready));
+    const size_t dp_u = (size_t)ncol * mz * sizeof(double), sp_u = (size_t)nb * mz * sizeof(double);
+    CU(cudaMemcpy2DAsync(U + c0 * mz, dp_u, st.U.p, sp_u, sp_u, nw, cudaMemcpyDeviceToHost, c->copy));
+    const size_t dp_k = (size_t)ncol * nz * sizeof(double), sp_k = (size_t)nb * nz * sizeof(double);
+    if (kappa) CU(cudaMemcpy2DAsync(kappa + c0 * nz, dp_k, st.K.p, sp_k, sp_k, nw, cudaMemcpyDeviceToHost, c->copy));
+    if (V) CU(cudaMemcpy2DAsync(V + c0 * nz, dp_k, st.V.p, sp_k, sp_k, nw, cudaMemcpyDeviceToHost, c->copy));
+    const size_t dp_p = (size_t)ncol * sizeof(double), sp_p = (size_t)nb * sizeof(double);
+    if (Vtop) CU(cudaMemcpy2DAsync(Vtop + c0, dp_p, st.top.p, sp_p, sp_p, nw, cudaMemcpyDeviceToHost, c->copy));
+    if (Vbot) CU(cudaMemcpy2DAsync(Vbot + c0, dp_p, st.bot.p, sp_p, sp_p, nw, cudaMemcpyDeviceToHost, c->copy));
+    CU(cudaEventRecord(st.done, c->copy));
+  }
+  CU(cudaStreamSynchronize(c->copy));
+  return read_status(c, c->stream, p);
+}
+
+extern "C" int oco_synchronize(oco_ctx *c) {
+  if (!c) return set_err(nullptr, OCO_EINVAL, "NULL context");
+  CU(cudaSetDevice(c->device));
+  if (c->status_pending) {
+    oco_params p = c->status_params;
+    int rc = read_status(c, c->status_stream, &p);
+    if (rc) return rc;
+  }
+  CU(cudaStreamSynchronize(c->stream));
+  CU(cudaStreamSynchronize(c->copy));
+  return OCO_OK;
+}
+
+extern "C" int64_t oco_kernel_launches(const oco_ctx *c) { return c ? c->launches : 0; }
+
+extern "C" int oco_set_profiling(oco_ctx *c, int enable) {
+  if (!c) return set_err(nullptr, OCO_EINVAL, "NULL context");
+  c->prof = enable != 0;
+  return OCO_OK;
+}
+
+extern "C" int oco_kernel_times(oco_ctx *c, double *solve_ms, double *pillars_ms, int64_t *solve_launches) {
+  if (!c) return set_err(nullptr, OCO_EINVAL, "NULL context");
+  CU(cudaSetDevice(c->device));
+  double ts = 0.0, tp = 0.0;
+  int64_t n = (int64_t)c->ev_solve.size();
+  for (auto *v : {&c->ev_solve, &c->ev_pil}) {
+    for (auto &pr : *v) {
+      CU(cudaEventSynchronize(pr.second));
+      float ms = 0.f;
+      CU(cudaEventElapsedTime(&ms, pr.first, pr.second));
+      (v == &c->ev_solve ? ts : tp) += ms;
+      c->ev_pool.push_back(pr.first);
+      c->ev_pool.push_back(pr.second);
+    }
+    v->clear();
+  }
+  if (solve_ms) *solve_ms = ts;
+  if (pillars_ms) *pillars_ms = tp;
+  if (solve_launches) *solve_launches = n;
+  return OCO_OK;
+}

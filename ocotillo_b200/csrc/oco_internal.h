@@ -1,0 +1,106 @@
+/*
+ * oco_internal.h -- device data layouts and kernel entry points shared by the runtime
+ * (oco_api.cu) and the kernel translation units.
+ */
+#ifndef OCO_INTERNAL_H
+#define OCO_INTERNAL_H
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace oco {
+
+/* Per-(column, z) quantities written by the pillar kernel and read by the solve kernels:
+ * the wavelength-independent part of the reference's per-(z, lambda) work
+ * (gas_state.f90:30-110 plus every factor of continuous_opacity.f90 that depends on z
+ * only).  Layout [col][z][NF] doubles. */
+enum PillarField {
+  F_RHO = 0,   /* rho */
+  F_RHO1,      /* 1/rho */
+  F_T1,        /* 1/T */
+  F_DFT1,      /* damping_factor_const*T1 (source function, c_o :399) */
+  F_THETA,     /* 5040/T */
+  F_TH1L,      /* theta1*log10e (H free-free Gaunt factor, c_o :264) */
+  F_LGT,       /* log10(theta) */
+  F_LGT2,      /* log10(theta)**2 */
+  F_IONF,      /* nHI/(nHI+nHII) */
+  F_ESCAT,     /* Thomson cross-section per H (c_o :149) */
+  F_ESCM,      /* e_scatter*mp1 (albedo numerator, c_o :195) */
+  F_HMBF,      /* H- bound-free factor (c_o :161) */
+  F_NEUTRAL,   /* 1 if (1 - NHII/N) > switch_ionfraction else 0 (c_o :262) */
+  F_E1,        /* exp(-chi_n(n)*k1*T1), n = 1..6 (c_o :238) */
+  F_E2,
+  F_E3,
+  F_E4,
+  F_E5,
+  F_E6,
+  F_UNSOLD,    /* Unsold integral (c_o :242) */
+  F_AFF,       /* ionf*ne*k*T (H- free-free prefactor, c_o :339) */
+  F_EF,        /* H free-free energy factor (c_o :265) */
+  F_TPOW,      /* (T*1e-4)**(-1.5) (bremsstrahlung Gaunt factor, c_o :290) */
+  F_LZ,        /* log(ne*(nHI+nHII)) + 2*log(1) - 0.5*log(T) (c_o :292-294) */
+  F_LNRHO,     /* log(rho) (mixed form) */
+  F_PAD,
+  NF
+};
+/* Grey RT re-uses the slots (continuous_opacity.f90:377-390). */
+enum GreyField { G_RHO = F_RHO, G_S = F_RHO1, G_ALPHA = F_T1 };
+
+/* Per-wavelength quantities: continuous_opacity.f90:64-141 plus every factor of the hot
+ * loop that depends on lambda only.  Layout [NL][nw]. */
+enum LambdaField {
+  L_CHI = 0,   /* chi = 1.2398e4/wa */
+  L_CHI1,      /* 1/chi */
+  L_GFF,       /* gff_factor */
+  L_WA3,       /* wa**3 */
+  L_SCOEF,     /* H- bound-free fit s_coeff */
+  L_HMON,      /* 1 if wa < 16000 (H- bound-free active) else 0 */
+  L_F1, L_F2, L_F3,  /* H- free-free fit f_coeff(iw, 1..3) */
+  L_GN1, L_GN2, L_GN3, L_GN4, L_GN5, L_GN6, /* g(iw,n)*n1_array(n)**3 */
+  L_NU9,       /* nu*1e-9 */
+  L_L3NU,      /* 3*log(nu) */
+  L_HNUK,      /* h*nu*k1 */
+  L_WCM1,      /* 1/wcm */
+  L_SW5,       /* source_function_const*w1cm5 */
+  L_LNSW5,     /* log(source_function_const*w1cm5) (mixed form) */
+  NL
+};
+
+/* Arguments of the FP64 solve kernels (plain and stable forms, grey or not). */
+struct SolveArgs {
+  const double *pil; /* [ncol][nz][NF] pillars of this chunk */
+  const double *lam; /* [NL][nw] */
+  int64_t ncol;      /* columns in this chunk */
+  int nz, nw;
+  double dz, dz1, dz2, sigma_grey;
+  /* Outputs: element (z, item) lives at base + z*zs + idx*is, where idx is the column-major
+   * item index of the destination:
+   *   layout REFERENCE:       idx = iw*ld_col + c_off + cl
+   *   layout LAMBDA_FASTEST:  idx = (c_off + cl)*nw + iw                              */
+  double *U;
+  int64_t U_zs, U_is;
+  double *K;
+  int64_t K_zs, K_is;
+  double *V;
+  int64_t V_zs, V_is;
+  double *Vtop, *Vbot; /* [iw*ld_col + c_off + cl] */
+  int64_t ld_col, c_off;
+  int layout;
+  /* Scratch [nz][nslot*32]: forward-sweep gamma, u and 1/kappa of each warp slot. */
+  double *gam, *uu, *o1;
+  int64_t slot_stride; /* = nslot*32 */
+  unsigned long long *work;   /* persistent-kernel work counter (warp tasks) */
+  unsigned long long *status; /* [0] zero-pivot count, [1] first bad item (min) */
+};
+
+/* Kernel launchers (defined in kernels_fp64.cu). Return cudaGetLastError(). */
+cudaError_t launch_pillars(const double *rho, const double *T, int64_t ncol, int nz,
+                           double fully_ionized_T, int grey, double *pil, cudaStream_t s);
+cudaError_t launch_solve_fp64(const SolveArgs &a, int form, int grey, int nslot_blocks,
+                              int threads, cudaStream_t s);
+int solve_fp64_max_blocks_per_sm(int form, int grey, int threads);
+
+}  // namespace oco
+
+#endif

@@ -1,0 +1,67 @@
+"""Seeded synthetic inputs with the shapes and value distributions of the benchmark configs.
+
+No public dataset is involved: every config is a synthetic AGN-disk column set built the
+way the reference's synthetic disk is (calc_grid, calc_density, calc_temperature in
+source/disk.f90:42-129), plus seeded lognormal density perturbations.  All arrays are
+float64 in the reference layout (nx, ny, nz) == Fortran (nz, ny, nx).
+"""
+import math
+
+import numpy as np
+
+Z0, Z1 = -5e15, 5e15
+RHO0, H, RHO_FLOOR = 1e-9, 1.496e14, 1e-24
+T_MID, SIGMA_T, T_FLOOR = 6.1e4, 2.5e14, 2000.0
+FULLY_IONIZED_T = 2e4
+
+
+def grid(nz, z0=Z0, z1=Z1):
+    """calc_grid (disk.f90:48-51): z_i = z0 + (i-1)*dz, dz = (z1-z0)/(nz-1)."""
+    dz = (z1 - z0) / (nz - 1)
+    return z0 + np.arange(nz, dtype=np.float64) * dz, dz
+
+
+def log_wavelengths(nw, w0=100.0, w1=1e5):
+    """nw log-spaced wavelengths in Angstrom from w0 to w1 (100 A .. 10 um by default)."""
+    if nw == 1:
+        return np.array([w0])
+    return np.logspace(math.log10(w0), math.log10(w1), nw)
+
+
+def temperature(z, t_mid=T_MID, sigma_t=SIGMA_T, t_floor=T_FLOOR):
+    """Gaussian midplane temperature with a floor (calc_temperature semantics with
+    isoTemp > midTemp: T = max(midTemp*exp(-z^2/2 sigma^2), floorTemp))."""
+    tg = t_mid * np.exp(-0.5 * z * z / (sigma_t * sigma_t))
+    return np.where(tg > t_floor, tg, t_floor)
+
+
+def agn_block(nx, ny, nz, seed=2, rho0=RHO0, sigma_dex=0.3, rho_floor=RHO_FLOOR):
+    """Config 'plain FP64 non-grey AGN grid': Gaussian density with a floor times a seeded
+    lognormal perturbation of sigma_dex per cell; Gaussian temperature with a 2000 K floor.
+    Returns rho, T (nx, ny, nz) and dz."""
+    z, dz = grid(nz)
+    base = rho0 * np.exp(-0.5 * z * z / (H * H))
+    base = np.where(base < rho_floor, rho_floor, base)
+    rng = np.random.default_rng(seed)
+    pert = 10.0 ** (sigma_dex * rng.standard_normal((nx, ny, nz)))
+    rho = base[None, None, :] * pert
+    T = np.broadcast_to(temperature(z), (nx, ny, nz)).copy()
+    return rho, T, dz
+
+
+def precision_block(nx, ny, nz, seed=3):
+    """Config 'precision form': as agn_block with rho0 drawn log-uniform in [1e-11, 1e-7]."""
+    rng = np.random.default_rng(seed)
+    rho0 = 10.0 ** rng.uniform(-11.0, -7.0)
+    rho, T, dz = agn_block(nx, ny, nz, seed=seed + 1000, rho0=rho0)
+    return rho, T, dz, rho0
+
+
+def grey_isothermal():
+    """Config 'plain method, small' == samples/GreyIsothermal: nx=ny=1, nz=10, grey
+    sigma=0.4, isothermal 2000 K (isoTemp=midTemp=1 is below the 2000 K floor)."""
+    z, dz = grid(10)
+    rho = RHO0 * np.exp(-((0.5 * (z * z)) / (H * H)))
+    rho = np.where(rho < RHO_FLOOR, RHO_FLOOR, rho)
+    T = np.full(10, 2000.0)
+    return rho.reshape(1, 1, 10), T.reshape(1, 1, 10), dz

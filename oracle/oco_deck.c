@@ -511,6 +511,26 @@ int oracle_run_deck(const char *deck, const char *outdir, char *msg, int msglen)
         rc = src;
         break;
       }
+      if (lroot) { /* block inputs, for feeding the same bytes to the GPU engine in tests */
+        snprintf(path, sizeof path, "%s/inputs_meta.txt", outdir);
+        FILE *fm = fopen(path, "w");
+        if (fm) {
+          fprintf(fm, "%d %d %d %d %.17g %d %.17g %.17g\n", nxloc, nyloc, nz, nw, dz, lgrey, sigma_grey,
+                  fully_ionized_T);
+          fclose(fm);
+        }
+        const char *names[3] = {"inputs_rho.bin", "inputs_T.bin", "inputs_wa.bin"};
+        const double *arrs[3] = {rho3d, temp3d, wa};
+        size_t counts[3] = {ncol * nz, ncol * nz, (size_t)nw};
+        for (int q = 0; q < 3; q++) {
+          snprintf(path, sizeof path, "%s/%s", outdir, names[q]);
+          FILE *fb = fopen(path, "wb");
+          if (fb) {
+            fwrite(arrs[q], sizeof(double), counts[q], fb);
+            fclose(fb);
+          }
+        }
+      }
       if (lroot) { /* output_ascii of the last column of the root block, io.f90:31-46 */
         snprintf(path, sizeof path, "%s/diagnostics.txt", outdir);
         FILE *fo = fopen(path, "w");

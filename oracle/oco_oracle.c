@@ -40,12 +40,10 @@ static const double log_overflow_limit = 308.0;             /* :28 floor(log10(h
 static const double mp = 1.67262192369e-24;                 /* :31 */
 static const double mp1 = 1.0 / 1.67262192369e-24;          /* :32 */
 static const double h_planck = 6.62607015e-27;              /* :39 */
-static const double pi = 0x1.921fb54442d18p+1;              /* :43 4*atan(1d0) */
-static const double pi1 = 1.0 / 0x1.921fb54442d18p+1;       /* :44 */
+static const double pi1 = 1.0 / 0x1.921fb54442d18p+1;       /* :43-44, pi = 4*atan(1d0) */
 static const double sqrt3 = 0x1.bb67ae8584caap+0;           /* :45 sqrt(3d0) */
 static const double exp1 = 0x1.5bf0a8b145769p+1;            /* :46 exp(1d0) */
 static const double k_cgs = 1.380649e-16;                   /* :49 */
-static const double k_eV = 8.617333262145179e-05;           /* :50 */
 static const double k1_cgs = 1.0 / 1.380649e-16;            /* :51 */
 static const double k1_eV = 1.0 / 8.617333262145179e-05;    /* :52 */
 static const double hydrogen_ionization_eV = 13.6;          /* :55 */
