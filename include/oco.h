@@ -133,6 +133,28 @@ int64_t oco_kernel_launches(const oco_ctx *ctx);
 int oco_set_profiling(oco_ctx *ctx, int enable);
 int oco_kernel_times(oco_ctx *ctx, double *solve_ms, double *pillars_ms, int64_t *solve_launches);
 
+/* ---- Solve without device allocation ----------------------------------------------------
+ * No counterpart in the reference (whose loop allocates nothing on a GPU): this entry point
+ * serves callers that cannot call cudaMalloc -- hosts that own the device heap, plugins not
+ * allowed to allocate after start-up, drivers with a fixed GPU-memory budget.  It runs the
+ * same kernels as oco_solve_block_device, on the calling thread's current device, with all
+ * intermediate data (pillars, Thomas scratch, wavelength table, counters) in one static
+ * device array of OCO_NOALLOC_WORKSPACE_BYTES that every GPU loading the library holds until
+ * the process exits.  The caller passes the wavelengths (Angstrom), the device inputs and
+ * the device outputs (layout p->layout).  No context, no cudaMalloc/cudaFree, no allocating
+ * library call.  The first call on a device looks up the array's device address (do it
+ * before any stream capture).  Calls share the array; calls whose GPU work overlaps race.
+ * The call returns when its work on `stream` is done.  Limits: nz <= OCO_NOALLOC_MAX_NZ,
+ * nw <= OCO_NOALLOC_MAX_NW, forms PLAIN and STABLE; larger sizes return OCO_EINVAL.
+ * Errors: oco_noalloc_last_error(). */
+#define OCO_NOALLOC_WORKSPACE_BYTES (32u << 20)
+#define OCO_NOALLOC_MAX_NZ 4096
+#define OCO_NOALLOC_MAX_NW 4096
+int oco_solve_block_noalloc(const oco_params *p, const double *wa_angstrom, const double *rho,
+                            const double *T, double *U, double *kappa, double *V, double *Vtop,
+                            double *Vbot, void *stream);
+const char *oco_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

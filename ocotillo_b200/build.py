@@ -28,6 +28,7 @@ UNITS = [
     ("kernels_fp64.cu", ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
     ("kernels_mixed.cu", []),
     ("oco_api.cu", []),
+    ("oco_noalloc.cu", []),
     ("oco_server.cu", []),
 ]
 HOST_UNITS = [("oco_deck.cpp", [])]

@@ -217,13 +217,12 @@ static double gaunt_bf(int n, double wave_cm) {
 /* pre_calc_opacity_quantities (continuous_opacity.f90:64-141) with the C library's pow and
  * log10, as the reference; then the hot loop's lambda-only factors (ocomath, as the
  * device computes everything inside the loop). */
-static void build_lambda_table(const double *waves, int nw, std::vector<double> &tab) {
+void oco::fill_lambda_table(const double *waves, int nw, double *tab) {
   static const double a_coeff[7] = {+1.99654,     -1.18267e-6,  +2.62423e-7, -4.40524e-11,
                                     +3.23992e-15, -1.39568e-19, +2.78701e-24};
   static const double b_coeff[3][5] = {{-2.276300, -1.685000, +0.766610, -0.053356, +0.000000},
                                        {+15.28270, -9.284600, +1.993810, -0.142631, +0.000000},
                                        {-197.789, +190.266, -67.9775, +10.6913, -0.62515}};
-  tab.assign((size_t)NL * nw, 0.0);
   auto T = [&](int f, int iw) -> double & { return tab[(size_t)f * nw + iw]; };
   for (int iw = 0; iw < nw; iw++) {
     const double wa = waves[iw];
@@ -267,8 +266,8 @@ extern "C" int oco_set_wavelengths(oco_ctx *c, const double *wa, int32_t nw) {
     if (!(wa[i] > 0.0) || !std::isfinite(wa[i]))
       return set_err(c, OCO_EINVAL, "oco_set_wavelengths: wavelength %d is not positive", i);
   CU(cudaSetDevice(c->device));
-  std::vector<double> tab;
-  build_lambda_table(wa, nw, tab);
+  std::vector<double> tab((size_t)NL * nw, 0.0);
+  fill_lambda_table(wa, nw, tab.data());
   CU(cudaStreamSynchronize(c->stream));
   CU(c->lam.ensure(tab.size() * sizeof(double)));
   CU(cudaMemcpy(c->lam.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));

@@ -94,6 +94,11 @@ struct SolveArgs {
   unsigned long long *status; /* [0] zero-pivot count, [1] first bad item (min) */
 };
 
+/* Fills tab[NL*nw] (layout [field][iw]) with the wavelength table of waves[nw] (Angstrom):
+ * pre_calc_opacity_quantities' arithmetic plus the hot loop's lambda-only factors
+ * (defined in oco_api.cu). */
+void fill_lambda_table(const double *waves, int nw, double *tab);
+
 /* Kernel launchers (defined in kernels_fp64.cu). Return cudaGetLastError(). */
 cudaError_t launch_pillars(const double *rho, const double *T, int64_t ncol, int nz,
                            double fully_ionized_T, int grey, double *pil, cudaStream_t s);

@@ -1,0 +1,172 @@
+/*
+ * oco_noalloc.cu -- oco_solve_block_noalloc: the device-array block solve for callers that
+ * cannot allocate GPU memory.
+ *
+ * Who needs it: code that runs where cudaMalloc is not allowed or not wanted -- inside an
+ * allocator-free host application (a Fortran driver linked against a runtime that owns the
+ * device heap), a plugin whose host forbids device allocation after start-up, or a caller
+ * that budgets GPU memory up front and must not see a call grow it.  The regular entry
+ * points allocate their workspace (pillars, Thomas scratch, wavelength table) on first use;
+ * this one uses a fixed workspace compiled into the library instead.
+ *
+ * The workspace is the file-scope array g_noalloc_ws below (OCO_NOALLOC_WORKSPACE_BYTES,
+ * 32 MiB): every GPU that loads the library holds it until the process exits.  Host code
+ * cannot use the array's name as a device address; the first call on each device, with that
+ * device current, asks the runtime for the address (cudaGetSymbolAddress) and caches it.
+ * That first call should therefore come before any stream capture.
+ *
+ * All calls share the one workspace and it keeps the previous call's contents: the work
+ * counter and the status words are cleared at the start of every call, everything else is
+ * fully rewritten before it is read.  Calls whose GPU work overlaps (different streams or
+ * threads at the same time) race on the workspace; serialise them.
+ */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "../../include/oco.h"
+#include "oco_internal.h"
+
+using namespace oco;
+
+static __device__ __align__(256) unsigned char g_noalloc_ws[OCO_NOALLOC_WORKSPACE_BYTES];
+
+namespace {
+
+const int kMaxDevices = 64;
+const int kThreads = 128;
+
+std::mutex g_mu;
+void *g_ws_addr[kMaxDevices];                       /* device address of g_noalloc_ws, per device */
+double g_host_table[NL * OCO_NOALLOC_MAX_NW];       /* host staging of the wavelength table */
+thread_local char g_msg[512];
+
+int fail(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_msg, sizeof g_msg, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CUN(call)                                                                             \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess)                                                                    \
+      return fail(OCO_ECUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+size_t round256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+}  // namespace
+
+extern "C" const char *oco_noalloc_last_error(void) { return g_msg; }
+
+extern "C" int oco_solve_block_noalloc(const oco_params *p, const double *wa_angstrom, const double *rho,
+                                       const double *T, double *U, double *kappa, double *V, double *Vtop,
+                                       double *Vbot, void *stream) {
+  g_msg[0] = 0;
+  if (!p || !rho || !T || !U) return fail(OCO_EINVAL, "params, rho, T and U are required");
+  if (p->nx < 1 || p->ny < 1 || p->nz < 2 || p->nw < 1)
+    return fail(OCO_EINVAL, "bad dimensions nx=%d ny=%d nz=%d nw=%d (need nz >= 2)", p->nx, p->ny, p->nz, p->nw);
+  if (p->lgrey && p->nw != 1) return fail(OCO_EGREY, "For Grey RT use only one wavelength");
+  if (p->form != OCO_FORM_PLAIN && p->form != OCO_FORM_STABLE)
+    return fail(OCO_EINVAL, "oco_solve_block_noalloc supports the plain and stable FP64 forms only");
+  if (p->layout != OCO_LAYOUT_REFERENCE && p->layout != OCO_LAYOUT_LAMBDA_FASTEST)
+    return fail(OCO_EINVAL, "unknown layout %d", p->layout);
+  if (!(p->dz > 0.0)) return fail(OCO_EINVAL, "dz must be positive");
+  if (!p->lgrey && !wa_angstrom) return fail(OCO_ENOWAVES, "wavelengths are required");
+  if (p->nz > OCO_NOALLOC_MAX_NZ || p->nw > OCO_NOALLOC_MAX_NW)
+    return fail(OCO_EINVAL, "oco_solve_block_noalloc: nz=%d nw=%d exceed the static workspace limits nz <= %d, nw <= %d",
+                p->nz, p->nw, OCO_NOALLOC_MAX_NZ, OCO_NOALLOC_MAX_NW);
+  const int grey = p->lgrey ? 1 : 0;
+  const int nz = p->nz, nw = p->nw;
+  cudaStream_t s = (cudaStream_t)stream;
+
+  std::lock_guard<std::mutex> lock(g_mu);
+  int dev = 0;
+  CUN(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return fail(OCO_EINVAL, "device %d out of range", dev);
+  if (!g_ws_addr[dev]) { /* once per device, with that device current */
+    void *ptr = nullptr;
+    CUN(cudaGetSymbolAddress(&ptr, g_noalloc_ws));
+    g_ws_addr[dev] = ptr;
+  }
+  unsigned char *ws = (unsigned char *)g_ws_addr[dev];
+
+  /* workspace layout: [counters 256 B][wavelength table][Thomas scratch][pillars] */
+  const size_t tab_bytes = grey ? 0 : round256((size_t)NL * nw * sizeof(double));
+  const size_t avail = OCO_NOALLOC_WORKSPACE_BYTES - 256 - tab_bytes;
+  int nsm = 0, bps = solve_fp64_max_blocks_per_sm(p->form == OCO_FORM_STABLE ? 1 : 0, grey, kThreads);
+  CUN(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const size_t per_slot = (size_t)nz * 3 * sizeof(double);
+  const int64_t ncol = (int64_t)p->nx * p->ny;
+  const int64_t need_blocks = (ncol * nw + kThreads - 1) / kThreads;
+  int64_t blocks = std::min<int64_t>({(int64_t)nsm * bps, need_blocks, (int64_t)(avail / 2 / (per_slot * kThreads))});
+  if (blocks < 1) return fail(OCO_EINVAL, "nz=%d does not fit the static workspace", nz);
+  const size_t scratch_bytes = round256((size_t)blocks * kThreads * per_slot);
+  const size_t per_col = (size_t)nz * NF * sizeof(double);
+  const int64_t chunk = std::min<int64_t>(ncol, (int64_t)((avail - scratch_bytes) / per_col));
+  if (chunk < 1) return fail(OCO_EINVAL, "nz=%d does not fit the static workspace", nz);
+
+  unsigned long long *ctr = (unsigned long long *)ws; /* [0] work, [1] zero-pivot count, [2] first bad item */
+  double *lam = (double *)(ws + 256);
+  double *scr = (double *)(ws + 256 + tab_bytes);
+  double *pil = (double *)(ws + 256 + tab_bytes + scratch_bytes);
+
+  if (!grey) { /* stage the table; a pageable-source copy has consumed the buffer when it returns */
+    fill_lambda_table(wa_angstrom, nw, g_host_table);
+    CUN(cudaMemcpyAsync(lam, g_host_table, (size_t)NL * nw * sizeof(double), cudaMemcpyHostToDevice, s));
+  }
+  CUN(cudaMemsetAsync(ctr + 1, 0, sizeof(unsigned long long), s));
+  CUN(cudaMemsetAsync(ctr + 2, 0xff, sizeof(unsigned long long), s));
+
+  SolveArgs a{};
+  a.nz = nz;
+  a.nw = nw;
+  a.dz = p->dz;
+  a.dz1 = 1.0 / p->dz;
+  a.dz2 = p->dz * p->dz;
+  a.sigma_grey = p->sigma_grey;
+  a.layout = p->layout;
+  a.ld_col = ncol;
+  const int64_t mz = nz + 6;
+  if (p->layout == OCO_LAYOUT_REFERENCE) {
+    a.U_zs = 1, a.U_is = mz, a.K_zs = 1, a.K_is = nz, a.V_zs = 1, a.V_is = nz;
+  } else {
+    const int64_t items = ncol * nw;
+    a.U_zs = items, a.U_is = 1, a.K_zs = items, a.K_is = 1, a.V_zs = items, a.V_is = 1;
+  }
+  a.U = U, a.K = kappa, a.V = V, a.Vtop = Vtop, a.Vbot = Vbot;
+  a.pil = pil;
+  a.lam = grey ? nullptr : lam;
+  const size_t slots = (size_t)blocks * kThreads;
+  a.gam = scr;
+  a.uu = scr + slots * nz;
+  a.o1 = scr + 2 * slots * nz;
+  a.slot_stride = (int64_t)slots;
+  a.work = ctr;
+  a.status = ctr + 1;
+  for (int64_t c0 = 0; c0 < ncol; c0 += chunk) {
+    const int64_t nb = std::min(chunk, ncol - c0);
+    a.ncol = nb;
+    a.c_off = c0;
+    CUN(launch_pillars(rho + c0 * nz, T + c0 * nz, nb, nz, p->fully_ionized_T, grey, pil, s));
+    CUN(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long), s));
+    const int64_t nblk = std::min<int64_t>(blocks, (nb * nw + kThreads - 1) / kThreads);
+    CUN(launch_solve_fp64(a, p->form == OCO_FORM_STABLE ? 1 : 0, grey, (int)nblk, kThreads, s));
+  }
+  unsigned long long st[2] = {0, 0};
+  CUN(cudaMemcpyAsync(st, ctr + 1, sizeof st, cudaMemcpyDeviceToHost, s));
+  CUN(cudaStreamSynchronize(s));
+  if (st[0]) {
+    long long col = (long long)(st[1] / (unsigned long long)nw), iw = (long long)(st[1] % nw);
+    return fail(OCO_EZEROPIVOT, "ERROR tridiag: bet == 0 in %llu items; first: ix=%lld iy=%lld iw=%lld", st[0],
+                col / p->ny + 1, col % p->ny + 1, iw + 1);
+  }
+  return OCO_OK;
+}

@@ -69,6 +69,8 @@ def load_library(path=None):
         "oco_kernel_launches": (ctypes.c_int64, [V]),
         "oco_set_profiling": (I, [V, I]),
         "oco_kernel_times": (I, [V, _DP, _DP, ctypes.POINTER(ctypes.c_int64)]),
+        "oco_solve_block_noalloc": (I, [P, _DP, V, V, V, V, V, V, V, V]),
+        "oco_noalloc_last_error": (ctypes.c_char_p, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
