@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(256) k_pillars(const double *__restrict__ rho,
   double theta = 5040.0 * T1;                      /* gas_state.f90:40-43 */
   double theta1 = 1.0 / theta;
   double lgt = oco_log10(theta);
-  double hmbf = ((4.158e-10 * Pe) * oco_pow(theta, 2.5)) * oco_pow(10.0, 0.754 * theta); /* c_o :161 */
+  double hmbf = ((4.158e-10 * Pe) * oco_pow(theta, 2.5)) * oco_pow10(0.754 * theta); /* c_o :161 */
   /* z-only factors of get_kappa_H_bf, c_o :234-242.  chi_n(n) = Ry*(1 - 1*(1/n)**2) as
    * in pre_calc_opacity_quantities :121-129; chi_m equals chi_n(6). */
   double ktemp = k_cgs * t, ktemp1 = k1_cgs * T1;
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(256) k_pillars(const double *__restrict__ rho,
   for (int q = 0; q < 6; q++) o[F_E1 + q] = E[q];
   o[F_UNSOLD] = unsold;
   o[F_AFF] = ((ionf * ne) * k_cgs) * t;                                             /* c_o :339 */
-  o[F_EF] = (((0.5 * log10e) * theta1) * Iev1) * oco_pow(10.0, -(theta * Iev));   /* c_o :265 */
+  o[F_EF] = (((0.5 * log10e) * theta1) * Iev1) * oco_pow10(-(theta * Iev));   /* c_o :265 */
   o[F_TPOW] = oco_pow(t * 1e-4, -1.5);                                              /* c_o :290 */
   o[F_LZ] = (oco_log(ne * (nHI + nHII)) + 2.0 * oco_log(1.0)) - 0.5 * oco_log(t);   /* c_o :292-294 */
   o[F_LNRHO] = oco_log(r);
@@ -143,14 +143,14 @@ struct Opac {
 __device__ __forceinline__ Opac opacity_at(const double *__restrict__ P, const Lam &L) {
   const double theta = __ldg(P + F_THETA);
   const double ionf = __ldg(P + F_IONF);
-  const double stim = 1.0 - oco_pow(10.0, -(L.chi * theta));
+  const double stim = 1.0 - oco_pow10(-(L.chi * theta));
   double sm = 0.0;
 #pragma unroll
   for (int q = 0; q < 6; q++) sm = sm + L.gn[q] * __ldg(P + F_E1 + q);
   double kHbf = (((AHbf * stim) * ionf) * L.wa3) * (__ldg(P + F_UNSOLD) + sm);
   double kHmbf = (L.hmon != 0.0) ? ((__ldg(P + F_HMBF) * stim) * ionf) * L.s : 0.0;
   double flam = ((L.f1 + L.f2 * __ldg(P + F_LGT)) + L.f3 * __ldg(P + F_LGT2)) - 26.0;
-  double kHmff = __ldg(P + F_AFF) * oco_pow(10.0, flam);
+  double kHmff = __ldg(P + F_AFF) * oco_pow10(flam);
   double kr = (((kHbf + kHmbf) + kHmff) + __ldg(P + F_ESCAT)) * mp1;
   const double rho = __ldg(P + F_RHO);
   double op = kr * rho;

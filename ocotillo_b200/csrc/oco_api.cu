@@ -363,14 +363,17 @@ static int reset_status(oco_ctx *c, cudaStream_t s) {
   if (c->status_pending) return OCO_OK; /* accumulate until the pending status is read */
   CU(cudaMemsetAsync(c->status.p, 0, sizeof(unsigned long long), s));
   CU(cudaMemsetAsync(c->status.as<unsigned long long>() + 1, 0xff, sizeof(unsigned long long), s));
+  CU(cudaMemsetAsync(c->status.as<unsigned long long>() + 2, 0, sizeof(unsigned long long), s));
   return OCO_OK;
 }
 
 static int read_status(oco_ctx *c, cudaStream_t s, const oco_params *p) {
-  unsigned long long st[2];
+  unsigned long long st[3];
   c->status_pending = false;
   CU(cudaMemcpyAsync(st, c->status.p, sizeof st, cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
+  if (st[2])
+    return set_err(c, OCO_ETIMEDOUT, "a bounded wait for a pillar copy ran out; results are incomplete");
   if (st[0]) {
     unsigned long long item = st[1];
     long long col = (long long)(item / (unsigned long long)p->nw), iw = (long long)(item % p->nw);

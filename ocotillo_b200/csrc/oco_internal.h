@@ -91,7 +91,7 @@ struct SolveArgs {
   double *gam, *uu, *o1;
   int64_t slot_stride; /* = nslot*32 */
   unsigned long long *work;   /* persistent-kernel work counter (warp tasks) */
-  unsigned long long *status; /* [0] zero-pivot count, [1] first bad item (min) */
+  unsigned long long *status; /* [0] zero-pivot count, [1] first bad item (min), [2] timeout flag */
 };
 
 /* Fills tab[NL*nw] (layout [field][iw]) with the wavelength table of waves[nw] (Angstrom):

@@ -113,7 +113,7 @@ extern "C" int oco_solve_block_noalloc(const oco_params *p, const double *wa_ang
   const int64_t chunk = std::min<int64_t>(ncol, (int64_t)((avail - scratch_bytes) / per_col));
   if (chunk < 1) return fail(OCO_EINVAL, "nz=%d does not fit the static workspace", nz);
 
-  unsigned long long *ctr = (unsigned long long *)ws; /* [0] work, [1] zero-pivot count, [2] first bad item */
+  unsigned long long *ctr = (unsigned long long *)ws; /* [0] work, [1] zero-pivot count, [2] first bad item, [3] timeout */
   double *lam = (double *)(ws + 256);
   double *scr = (double *)(ws + 256 + tab_bytes);
   double *pil = (double *)(ws + 256 + tab_bytes + scratch_bytes);
@@ -124,6 +124,7 @@ extern "C" int oco_solve_block_noalloc(const oco_params *p, const double *wa_ang
   }
   CUN(cudaMemsetAsync(ctr + 1, 0, sizeof(unsigned long long), s));
   CUN(cudaMemsetAsync(ctr + 2, 0xff, sizeof(unsigned long long), s));
+  CUN(cudaMemsetAsync(ctr + 3, 0, sizeof(unsigned long long), s));
 
   SolveArgs a{};
   a.nz = nz;
@@ -160,9 +161,10 @@ extern "C" int oco_solve_block_noalloc(const oco_params *p, const double *wa_ang
     const int64_t nblk = std::min<int64_t>(blocks, (nb * nw + kThreads - 1) / kThreads);
     CUN(launch_solve_fp64(a, p->form == OCO_FORM_STABLE ? 1 : 0, grey, (int)nblk, kThreads, s));
   }
-  unsigned long long st[2] = {0, 0};
+  unsigned long long st[3] = {0, 0, 0};
   CUN(cudaMemcpyAsync(st, ctr + 1, sizeof st, cudaMemcpyDeviceToHost, s));
   CUN(cudaStreamSynchronize(s));
+  if (st[2]) return fail(OCO_ETIMEDOUT, "a bounded wait for a pillar copy ran out; results are incomplete");
   if (st[0]) {
     long long col = (long long)(st[1] / (unsigned long long)nw), iw = (long long)(st[1] % nw);
     return fail(OCO_EZEROPIVOT, "ERROR tridiag: bet == 0 in %llu items; first: ix=%lld iy=%lld iw=%lld", st[0],

@@ -100,12 +100,14 @@ OCO_HD double oco_exp_dd(double xh, double xl) {
   if (oco_isnan(xh)) return OCO_A(xh, xh);
   if (xh > 709.8) return oco_inf();
   if (xh < -746.0) return 0.0;
-  /* kd = nearest integer to x * 128/ln2. */
+  /* kd = nearest integer to x * 128/ln2; its value also sits in the low bits of the
+   * shifted sum (|kd| < 2^18), which gives j and k without a conversion. */
   const double shift = 0x1.8p52;
-  double kd = OCO_S(OCO_A(OCO_M(xh, OCO_EXP_INVLN2N), shift), shift);
-  int64_t ki = (int64_t)kd;
-  int j = (int)(ki & (OCO_EXP_N - 1));
-  int k = (int)((ki - j) / OCO_EXP_N);
+  double ks = OCO_A(OCO_M(xh, OCO_EXP_INVLN2N), shift);
+  double kd = OCO_S(ks, shift);
+  int ki = (int)(uint32_t)oco_d2u(ks);
+  int j = ki & (OCO_EXP_N - 1);
+  int k = ki >> 7; /* floor(ki / 128) */
   /* r = x - kd ln2/128 as a double-double.  kd*L1 is exact (35 + 18 bits) and the
    * subtraction is exact by Sterbenz's lemma. */
   double d = OCO_S(xh, OCO_M(kd, OCO_EXP_L1));
@@ -115,7 +117,7 @@ OCO_HD double oco_exp_dd(double xh, double xl) {
   double bb = OCO_S(rh, d);
   double t = OCO_A(OCO_S(d, OCO_S(rh, bb)), OCO_S(-p2, bb));
   double rl = OCO_A(OCO_S(OCO_S(t, p2e), OCO_M(kd, OCO_EXP_L3)), xl);
-  double r0 = OCO_A(rh, rl); /* TwoSum renormalisation */
+  double r0 = OCO_A(rh, rl); /* TwoSum renormalisation (needed when xl is not 0) */
   bb = OCO_S(r0, rh);
   rl = OCO_A(OCO_S(rh, OCO_S(r0, bb)), OCO_S(rl, bb));
   rh = r0;
@@ -249,6 +251,15 @@ OCO_HD int oco_int_class(double y) {
   if (y != trunc(y)) return -1;
   if (fabs(y) >= 0x1p53) return 0;
   return (int)((int64_t)y & 1);
+}
+
+/* 10^y: exactly the x == 10 path of oco_pow below (same operations, same result), without
+ * the special-case ladder: y = +-0 gives 1, NaN gives NaN, +-inf give inf and 0 through
+ * oco_exp_dd itself. */
+OCO_HD double oco_pow10(double y) {
+  double ph = OCO_M(y, OCO_LN10_HI);
+  double pl = OCO_A(OCO_FMA(y, OCO_LN10_HI, -ph), OCO_M(y, OCO_LN10_LO));
+  return OCO_M(1.0, oco_exp_dd(ph, pl));
 }
 
 /* x^y with the C99 Annex F special cases. */

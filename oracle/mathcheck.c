@@ -3,7 +3,7 @@
  * Evaluates exp/log/log10/pow element-wise with (a) glibc, (b) quad precision (libquadmath,
  * 113-bit significand) rounded to double -- a correctly rounded reference except within
  * 2^-113 of a rounding boundary -- and (c) the host build of ocomath.
- * fn: 0 exp(x), 1 log(x), 2 log10(x), 3 pow(x, y).
+ * fn: 0 exp(x), 1 log(x), 2 log10(x), 3 pow(x, y), 4 10^y (ocomath's dedicated oco_pow10).
  */
 #include <math.h>
 #include <quadmath.h>
@@ -26,5 +26,6 @@ void mc_quad(int fn, const double *x, const double *y, double *out, int64_t n) {
 
 void mc_ocomath(int fn, const double *x, const double *y, double *out, int64_t n) {
   for (int64_t i = 0; i < n; i++)
-    out[i] = fn == 0 ? oco_exp(x[i]) : fn == 1 ? oco_log(x[i]) : fn == 2 ? oco_log10(x[i]) : oco_pow(x[i], y[i]);
+    out[i] = fn == 0 ? oco_exp(x[i]) : fn == 1 ? oco_log(x[i]) : fn == 2 ? oco_log10(x[i])
+             : fn == 3 ? oco_pow(x[i], y[i]) : oco_pow10(y[i]);
 }

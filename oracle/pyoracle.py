@@ -102,7 +102,7 @@ _MC = None
 
 def mathcheck(kind, fn, x, y=None):
     """Element-wise reference math: kind in {'glibc', 'quad', 'ocomath'};
-    fn in {'exp', 'log', 'log10', 'pow'}."""
+    fn in {'exp', 'log', 'log10', 'pow', 'pow10'} ('pow10': ocomath only)."""
     global _MC
     if _MC is None:
         path = os.path.join(BUILD, "libmathcheck.so")
@@ -116,6 +116,6 @@ def mathcheck(kind, fn, x, y=None):
     x = np.ascontiguousarray(x, dtype=np.float64)
     y = np.ascontiguousarray(y if y is not None else np.zeros_like(x), dtype=np.float64)
     out = np.empty_like(x)
-    code = {"exp": 0, "log": 1, "log10": 2, "pow": 3}[fn]
+    code = {"exp": 0, "log": 1, "log10": 2, "pow": 3, "pow10": 4}[fn]
     getattr(_MC, "mc_" + kind)(code, _ptr(x), _ptr(y), _ptr(out), x.size)
     return out

@@ -83,3 +83,16 @@ def test_exp_log_special_cases(oracle):
         a, q = oracle.mathcheck("ocomath", fn, x), oracle.mathcheck("quad", fn, x)
         assert (((a == q) | (np.isnan(a) & np.isnan(q)))).all(), fn
     assert oracle.mathcheck("ocomath", "log", np.array([1.0]))[0] == 0.0
+
+
+def test_pow10_fast_path_is_pow_of_ten(oracle):
+    # The kernels call oco_pow10(y); the oracle calls oco_pow(10.0, y).  They must agree
+    # bit for bit everywhere, including the special values.
+    rng = np.random.default_rng(15)
+    y = np.concatenate([rng.uniform(-330, 310, N), [0.0, -0.0, np.inf, -np.inf, 1e-300, -1e-300, 308.2547,
+                                                    308.26, -323.3, -324.5, 400.0, -400.0]])
+    a = oracle.mathcheck("ocomath", "pow10", y, y)
+    b = oracle.mathcheck("ocomath", "pow", np.full_like(y, 10.0), y)
+    assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+    nan = oracle.mathcheck("ocomath", "pow10", np.array([np.nan]), np.array([np.nan]))
+    assert np.isnan(nan).all()
