@@ -134,80 +134,185 @@ __device__ __forceinline__ void load_lam(Lam &L, const double *__restrict__ lam,
 #undef LD
 }
 
+/* One pillar record, read through the read-only cache (global) or from shared memory. */
+struct GlobalRec {
+  const double *p;
+  __device__ __forceinline__ double operator[](int f) const { return __ldg(p + f); }
+};
+struct SharedRec {
+  const double *p;
+  __device__ __forceinline__ double operator[](int f) const { return p[f]; }
+};
+
 struct Opac {
   double op, alb, S;
+  double oma; /* stable form: 1 - albedo from the absorption terms (no cancellation) */
 };
 
 /* calc_opacity_and_albedo for one (z, lambda), continuous_opacity.f90:175-201 with
  * :171, :233-244, :318-322, :337-339, :261-277, :290-298, :399-407. */
-__device__ __forceinline__ Opac opacity_at(const double *__restrict__ P, const Lam &L) {
-  const double theta = __ldg(P + F_THETA);
-  const double ionf = __ldg(P + F_IONF);
+template <bool STABLE, class R>
+__device__ __forceinline__ Opac opacity_at(const R P, const Lam &L) {
+  const double theta = P[F_THETA];
+  const double ionf = P[F_IONF];
   const double stim = 1.0 - oco_pow10(-(L.chi * theta));
   double sm = 0.0;
 #pragma unroll
-  for (int q = 0; q < 6; q++) sm = sm + L.gn[q] * __ldg(P + F_E1 + q);
-  double kHbf = (((AHbf * stim) * ionf) * L.wa3) * (__ldg(P + F_UNSOLD) + sm);
-  double kHmbf = (L.hmon != 0.0) ? ((__ldg(P + F_HMBF) * stim) * ionf) * L.s : 0.0;
-  double flam = ((L.f1 + L.f2 * __ldg(P + F_LGT)) + L.f3 * __ldg(P + F_LGT2)) - 26.0;
-  double kHmff = __ldg(P + F_AFF) * oco_pow10(flam);
-  double kr = (((kHbf + kHmbf) + kHmff) + __ldg(P + F_ESCAT)) * mp1;
-  const double rho = __ldg(P + F_RHO);
+  for (int q = 0; q < 6; q++) sm = sm + L.gn[q] * P[F_E1 + q];
+  double kHbf = (((AHbf * stim) * ionf) * L.wa3) * (P[F_UNSOLD] + sm);
+  double kHmbf = (L.hmon != 0.0) ? ((P[F_HMBF] * stim) * ionf) * L.s : 0.0;
+  double flam = ((L.f1 + L.f2 * P[F_LGT]) + L.f3 * P[F_LGT2]) - 26.0;
+  double kHmff = P[F_AFF] * oco_pow10(flam);
+  double kr = (((kHbf + kHmbf) + kHmff) + P[F_ESCAT]) * mp1;
+  double kabs = STABLE ? ((kHbf + kHmbf) + kHmff) * mp1 : 0.0;
+  const double rho = P[F_RHO];
   double op = kr * rho;
-  if (__ldg(P + F_NEUTRAL) != 0.0) {
-    double g_ff = 1.0 + L.gff * ((__ldg(P + F_TH1L) * L.chi1) + 0.5);
-    double kHff = ((((stim * ionf) * alpha0) * L.wa3) * g_ff) * __ldg(P + F_EF);
+  if (P[F_NEUTRAL] != 0.0) {
+    double g_ff = 1.0 + L.gff * ((P[F_TH1L] * L.chi1) + 0.5);
+    double kHff = ((((stim * ionf) * alpha0) * L.wa3) * g_ff) * P[F_EF];
     kr = kr + kHff * mp1;
     op = op + kr * rho;
+    if (STABLE) kabs = kabs + kHff * mp1;
   } else {
-    double gaunt = oco_log(oco_exp(5.960 - (sqrt3 * pi1) * oco_log(L.nu9 * __ldg(P + F_TPOW))) + exp1);
-    double lnq = (__ldg(P + F_LZ) - L.l3nu) + oco_log(1.0 - oco_exp(-(L.hnuk * __ldg(P + F_T1))));
+    double gaunt = oco_log(oco_exp(5.960 - (sqrt3 * pi1) * oco_log(L.nu9 * P[F_TPOW])) + exp1);
+    double lnq = (P[F_LZ] - L.l3nu) + oco_log(1.0 - oco_exp(-(L.hnuk * P[F_T1])));
     double krho = (bremsstrahlung_constant * oco_exp(lnq)) * gaunt;
     op = op + krho;
-    kr = kr + op * __ldg(P + F_RHO1);
+    kr = kr + op * P[F_RHO1];
+    if (STABLE) kabs = kabs + op * P[F_RHO1];
   }
   Opac o;
   o.op = op;
-  o.alb = __ldg(P + F_ESCM) / kr;
-  double damping = __ldg(P + F_DFT1) * L.wcm1;
+  o.alb = P[F_ESCM] / kr;
+  o.oma = STABLE ? kabs / kr : 0.0;
+  double damping = P[F_DFT1] * L.wcm1;
   if (damping > log_overflow_limit) damping = log_overflow_limit;
   o.S = L.sw5 / (oco_exp(damping) - 1.0);
   return o;
 }
 
 /* grey_parameters, continuous_opacity.f90:377-390 */
-__device__ __forceinline__ Opac opacity_grey(const double *__restrict__ P, double sg) {
-  double alpha = __ldg(P + G_ALPHA);
+template <class R>
+__device__ __forceinline__ Opac opacity_grey(const R P, double sg) {
+  double alpha = P[G_ALPHA];
   Opac o;
-  o.op = (alpha + sg) * __ldg(P + G_RHO);
+  o.op = (alpha + sg) * P[G_RHO];
   o.alb = sg / (alpha + sg);
-  o.S = __ldg(P + G_S);
+  o.oma = alpha / (alpha + sg);
+  o.S = P[G_S];
   return o;
 }
 
+/* ---- pillar access ------------------------------------------------------------------- */
+/* Generic path: each lane reads its own column's records through the read-only cache. */
+struct DirectPillars {
+  const double *base;
+  __device__ __forceinline__ GlobalRec at(int z) { return GlobalRec{base + (int64_t)z * NF}; }
+};
+
+constexpr int ZC = 16;            /* z records per staged chunk */
+constexpr int WARPS_PER_BLOCK = 4; /* k_solve runs 128-thread blocks */
+constexpr long long kSpinLimit = 1ll << 26;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+/* Staged path: all 32 lanes of the warp work on one column.  Lane 0 streams the column's
+ * pillar records in chunks of ZC z with a bulk (TMA) copy into one of two shared-memory
+ * buffers per warp; an mbarrier per buffer signals arrival.  Records are read in increasing
+ * z, one at a time: entering chunk c frees the buffer of chunk c-1, which then receives
+ * chunk c+1.  Waits are bounded; on timeout the warp records the failure and stops. */
+struct StagedPillars {
+  double *buf;    /* shared: [2][ZC*NF] */
+  uint32_t bar0;  /* shared address of two mbarriers (8 B each) */
+  const double *src;
+  int nz, nchunks, cur;
+  uint32_t waits;    /* bit b: parity of the next wait on buffer b */
+  uint32_t inflight; /* bit b: a copy into buffer b has been issued and not yet waited for */
+  bool failed;
+
+  __device__ __forceinline__ void issue(int c) {
+    const int rows = min(ZC, nz - c * ZC);
+    const uint32_t bytes = (uint32_t)(rows * NF * sizeof(double));
+    const uint32_t bar = bar0 + 8u * (c & 1);
+    const uint32_t dst = smem_addr(buf + (c & 1) * (ZC * NF));
+    const size_t g = __cvta_generic_to_global(src + (int64_t)c * ZC * NF);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(g), "r"(bytes), "r"(bar)
+                 : "memory");
+  }
+  /* Waits (bounded) for the copy into buffer b.  Every lane tracks the same state. */
+  __device__ __forceinline__ bool wait(int b) {
+    if (!((inflight >> b) & 1u)) return true;
+    const uint32_t bar = bar0 + 8u * b;
+    const uint32_t parity = (waits >> b) & 1u;
+    long long spins = 0;
+    while (!mbar_try_wait(bar, parity))
+      if (++spins > kSpinLimit) return false;
+    waits ^= 1u << b;
+    inflight &= ~(1u << b);
+    return true;
+  }
+  __device__ __forceinline__ void note_issue(int c) { inflight |= 1u << (c & 1); }
+  __device__ __forceinline__ void begin(const double *column, int lane) {
+    src = column;
+    cur = -1;
+    nchunks = (nz + ZC - 1) / ZC;
+    __syncwarp();
+    if (lane == 0) issue(0);
+    note_issue(0);
+  }
+  __device__ __forceinline__ SharedRec at(int z) {
+    const int c = z / ZC;
+    if (c != cur) { /* c == cur + 1 */
+      __syncwarp();
+      if (!failed && c + 1 < nchunks) {
+        if ((threadIdx.x & 31) == 0) issue(c + 1);
+        note_issue(c + 1);
+      }
+      if (!failed && !wait(c & 1)) failed = true;
+      cur = c;
+    }
+    return SharedRec{buf + (c & 1) * (ZC * NF) + (z - c * ZC) * NF};
+  }
+};
+
 /* ---- the solve ----------------------------------------------------------------------- */
-template <int FORM, bool GREY>
-__device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int iw,
+/* Solves one (column, wavelength) item.  `active` false: the lane only keeps the warp's
+ * shared pipeline in step (staged path, wavelength index beyond nw) and stores nothing. */
+template <int FORM, bool GREY, class PA>
+__device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int iw, bool active, PA &pa,
                                            double *__restrict__ gam, double *__restrict__ uu,
-                                           double *__restrict__ o1s) {
+                                           double *__restrict__ o1s, double *__restrict__ qs) {
   const int nz = a.nz;
   const int64_t ss = a.slot_stride;
-  const double *__restrict__ P = a.pil + cl * (int64_t)nz * NF;
   Lam L;
   if (!GREY) load_lam(L, a.lam, iw, a.nw);
-  const int64_t idx = (a.layout == 0) ? (int64_t)iw * a.ld_col + a.c_off + cl
-                                      : (a.c_off + cl) * a.nw + iw;
+  const int64_t idx = (a.layout == 0) ? (int64_t)iw * a.ld_col + a.c_off + cl : (a.c_off + cl) * a.nw + iw;
   double *Ub = a.U + idx * a.U_is;
-  double *Kb = a.K ? a.K + idx * a.K_is : nullptr;
-  double *Vb = a.V ? a.V + idx * a.V_is : nullptr;
+  double *Kb = (a.K && active) ? a.K + idx * a.K_is : nullptr;
+  double *Vb = (a.V && active) ? a.V + idx * a.V_is : nullptr;
   const double dz = a.dz, dz2 = a.dz2;
   bool bad = false;
 
   /* forward sweep: row 0 (fill_boundary_coeffs :187-191) */
-  Opac cur = GREY ? opacity_grey(P, a.sigma_grey) : opacity_at(P, L);
-  Opac nxt = GREY ? opacity_grey(P + NF, a.sigma_grey) : opacity_at(P + NF, L);
+  Opac cur = GREY ? opacity_grey(pa.at(0), a.sigma_grey) : opacity_at<FORM == 1>(pa.at(0), L);
+  Opac nxt = GREY ? opacity_grey(pa.at(1), a.sigma_grey) : opacity_at<FORM == 1>(pa.at(1), L);
   double o1 = 1.0 / cur.op, o2 = cur.op * cur.op;
-  double zeta = ((cur.op * dz2) * (1.0 - cur.alb)) * 0.25;
+  double zeta = ((cur.op * dz2) * (FORM == 1 ? cur.oma : (1.0 - cur.alb))) * 0.25;
   double bet, h = 0.0;
   if (FORM == 0) {
     bet = -(((o1 + dz) + zeta) * o2);
@@ -229,19 +334,18 @@ __device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int i
     o2 = op * op;
     double aa, bb, cc, dd, ee;
     if (j < nz - 1) { /* fill_center_coeffs :159-165 */
-      nxt = GREY ? opacity_grey(P + (int64_t)(j + 1) * NF, a.sigma_grey)
-                 : opacity_at(P + (int64_t)(j + 1) * NF, L);
+      nxt = GREY ? opacity_grey(pa.at(j + 1), a.sigma_grey) : opacity_at<FORM == 1>(pa.at(j + 1), L);
       aa = o2 / kh_prev;
       double kh = 0.5 * (nxt.op + op);
       cc = o2 / kh;
-      double z3 = (dz2 * (op * (op * op))) * (1.0 - cur.alb);
+      double z3 = (dz2 * (op * (op * op))) * (FORM == 1 ? cur.oma : (1.0 - cur.alb));
       bb = -((aa + cc) + z3);
       dd = -(cur.S * z3);
       ee = z3;
       kh_prev = kh;
     } else { /* fill_boundary_coeffs :193-197 */
       aa = op;
-      double zt = ((op * dz2) * (1.0 - cur.alb)) * 0.25;
+      double zt = ((op * dz2) * (FORM == 1 ? cur.oma : (1.0 - cur.alb))) * 0.25;
       bb = -(((o1 + dz) + zt) * o2);
       cc = 0.0;
       dd = -((cur.S * zt) * o2);
@@ -254,6 +358,7 @@ __device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int i
     } else { /* difference form: bet = -(c + h), h = e + a*h_prev/(c_prev + h_prev) */
       double den = c_prev + h;
       g = -(c_prev / den);
+      qs[(j - 1) * ss] = h / den; /* q_{j-1} = h_{j-1}/(c_{j-1} + h_{j-1}) */
       h = ee + (aa * h) / den;
       bet = -(cc + h);
       (void)bb;
@@ -267,6 +372,7 @@ __device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int i
     c_prev = cc;
     cur = nxt;
   }
+  if (!active) return;
   if (bad) {
     atomicAdd(&a.status[0], 1ull);
     atomicMin(&a.status[1], (unsigned long long)((a.c_off + cl) * a.nw + iw));
@@ -276,11 +382,74 @@ __device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int i
   const double dz1 = a.dz1;
   const int64_t uz = a.U_zs;
   double vtop = 0.0, vbot = 0.0;
-  if (nz >= 4) {
-    auto emitV = [&](int j, double w0, double w1, double w2, double w3, double w4, double w5,
-                     double w6) -> double {
+  if (FORM == 1 && nz >= 4) {
+    /* Stable form: the differences D_k = U_k - U_{k+1} = u_k - q_k U_{k+1} come out of the
+     * back-substitution directly, and the flux is the 6th-order stencil written in them
+     * (ghost differences mirror the interior ones); exact in the same arithmetic as the
+     * stencil on U, accurate where U's differences are below its resolution. */
+    const int n = nz;
+    double Un = u; /* U_{n-1} */
+    Ub[(3 + n - 1) * uz] = Un;
+    double Uk[3], Dt[3];
+    for (int t = 0; t < 3; t++) {
+      const int k = n - 2 - t;
+      const double uf = uu[k * ss];
+      Dt[t] = uf - qs[k * ss] * Un;
+      Un = uf - gam[(k + 1) * ss] * Un;
+      Uk[t] = Un;
+      Ub[(3 + k) * uz] = Un;
+    }
+    const double fn = u;
+    Ub[(n + 3) * uz] = 2.0 * fn - Uk[0];
+    Ub[(n + 4) * uz] = 2.0 * fn - Uk[1];
+    Ub[(n + 5) * uz] = 2.0 * fn - Uk[2];
+    double d0 = Dt[2], d1 = Dt[1], d2 = Dt[0], d3 = Dt[0], d4 = Dt[1], d5 = Dt[2];
+    auto emitD = [&](int j) -> double {
+      const double s1 = d2 + d3;
+      const double s2 = (s1 + d1) + d4;
+      const double s3 = (s2 + d0) + d5;
+      const double df = -((1.0 / 60.0) * (((45.0 * s1) - 9.0 * s2) + s3));
+      const double v = ((-1.0 * o1s[j * ss]) * df) * dz1;
+      if (Vb) Vb[j * a.V_zs] = v;
+      return v;
+    };
+    vtop = emitD(n - 1);
+    double U0 = Uk[2], U1 = Uk[1], U2 = Uk[0], U3 = u; /* the four lowest U seen so far */
+    auto stepD = [&](int k, double uf, double qk, double gk1) {
+      const double Dk = uf - qk * Un;
+      Un = uf - gk1 * Un;
+      Ub[(3 + k) * uz] = Un;
+      U3 = U2; U2 = U1; U1 = U0; U0 = Un;
+      d5 = d4; d4 = d3; d3 = d2; d2 = d1; d1 = d0; d0 = Dk;
+      emitD(k + 3);
+    };
+    int k = n - 5;
+    for (; k >= 7; k -= 8) { /* scratch loads of 8 steps hoisted off the serial chain */
+      double ub[8], qb[8], gb[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        ub[q] = uu[(k - q) * ss];
+        qb[q] = qs[(k - q) * ss];
+        gb[q] = gam[(k - q + 1) * ss];
+      }
+#pragma unroll
+      for (int q = 0; q < 8; q++) stepD(k - q, ub[q], qb[q], gb[q]);
+    }
+    for (; k >= 0; k--) stepD(k, uu[k * ss], qs[k * ss], gam[(k + 1) * ss]);
+    Ub[2 * uz] = 2.0 * U0 - U1;
+    Ub[1 * uz] = 2.0 * U0 - U2;
+    Ub[0] = 2.0 * U0 - U3;
+    const double D0 = d0, D1 = d1, D2 = d2;
+    d5 = d4; d4 = d3; d3 = d2; d2 = d1; d1 = d0; d0 = D0;
+    emitD(2);
+    d5 = d4; d4 = d3; d3 = d2; d2 = d1; d1 = d0; d0 = D1;
+    emitD(1);
+    d5 = d4; d4 = d3; d3 = d2; d2 = d1; d1 = d0; d0 = D2;
+    vbot = emitD(0);
+  } else if (nz >= 4) {
+    auto emitV = [&](int j, double o1j, double w0, double w1, double w2, double w4, double w5, double w6) -> double {
       double df = (1.0 / 60.0) * (((45.0 * (w4 - w2)) - 9.0 * (w5 - w1)) + (w6 - w0));
-      double v = ((-1.0 * o1s[j * ss]) * df) * dz1;
+      double v = ((-1.0 * o1j) * df) * dz1;
       if (Vb) Vb[j * a.V_zs] = v;
       return v;
     };
@@ -298,23 +467,41 @@ __device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int i
     Ub[(n + 4) * uz] = g2;
     Ub[(n + 5) * uz] = g3;
     double w0 = u4, w1 = u3, w2 = u2, w3 = u1, w4 = g1, w5 = g2, w6 = g3;
-    vtop = emitV(n - 1, w0, w1, w2, w3, w4, w5, w6);
-    for (int kk = n - 5; kk >= 0; kk--) {
+    vtop = emitV(n - 1, o1s[(n - 1) * ss], w0, w1, w2, w4, w5, w6);
+    int kk = n - 5;
+    /* blocks of 8 steps with the scratch loads hoisted off the serial U chain */
+    for (; kk >= 7; kk -= 8) {
+      double ub[8], gb[8], ob[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        ub[q] = uu[(kk - q) * ss];
+        gb[q] = gam[(kk - q + 1) * ss];
+        ob[q] = o1s[(kk - q + 3) * ss];
+      }
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        double Uk = ub[q] - gb[q] * w0;
+        Ub[(3 + kk - q) * uz] = Uk;
+        w6 = w5; w5 = w4; w4 = w3; w3 = w2; w2 = w1; w1 = w0; w0 = Uk;
+        emitV(kk - q + 3, ob[q], w0, w1, w2, w4, w5, w6);
+      }
+    }
+    for (; kk >= 0; kk--) {
       double Uk = uu[kk * ss] - gam[(kk + 1) * ss] * w0;
       Ub[(3 + kk) * uz] = Uk;
       w6 = w5; w5 = w4; w4 = w3; w3 = w2; w2 = w1; w1 = w0; w0 = Uk;
-      emitV(kk + 3, w0, w1, w2, w3, w4, w5, w6);
+      emitV(kk + 3, o1s[(kk + 3) * ss], w0, w1, w2, w4, w5, w6);
     }
     double b1 = 2.0 * w0 - w1, b2 = 2.0 * w0 - w2, b3 = 2.0 * w0 - w3;
     Ub[2 * uz] = b1;
     Ub[1 * uz] = b2;
     Ub[0] = b3;
     w6 = w5; w5 = w4; w4 = w3; w3 = w2; w2 = w1; w1 = w0; w0 = b1;
-    emitV(2, w0, w1, w2, w3, w4, w5, w6);
+    emitV(2, o1s[2 * ss], w0, w1, w2, w4, w5, w6);
     w6 = w5; w5 = w4; w4 = w3; w3 = w2; w2 = w1; w1 = w0; w0 = b2;
-    emitV(1, w0, w1, w2, w3, w4, w5, w6);
+    emitV(1, o1s[1 * ss], w0, w1, w2, w4, w5, w6);
     w6 = w5; w5 = w4; w4 = w3; w3 = w2; w2 = w1; w1 = w0; w0 = b3;
-    vbot = emitV(0, w0, w1, w2, w3, w4, w5, w6);
+    vbot = emitV(0, o1s[0], w0, w1, w2, w4, w5, w6);
   } else { /* nz = 2 or 3: the reference's ghost update order matters (ghosts feed ghosts) */
     double f[9];
     const int n1 = 3, n2 = nz + 2;
@@ -340,6 +527,7 @@ __device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int i
   if (a.Vbot) a.Vbot[pidx] = vbot;
 }
 
+/* Generic path: warp tasks are 32 consecutive items of the flattened (column, lambda) index. */
 template <int FORM, bool GREY>
 __global__ void __launch_bounds__(128) k_solve(const SolveArgs a) {
   const int lane = threadIdx.x & 31;
@@ -349,6 +537,7 @@ __global__ void __launch_bounds__(128) k_solve(const SolveArgs a) {
   double *gam = a.gam + slot * 32 + lane;
   double *uu = a.uu + slot * 32 + lane;
   double *o1 = a.o1 + slot * 32 + lane;
+  double *qs = a.q + slot * 32 + lane;
   for (;;) {
     unsigned long long task = 0;
     if (lane == 0) task = atomicAdd(a.work, 1ull);
@@ -358,7 +547,57 @@ __global__ void __launch_bounds__(128) k_solve(const SolveArgs a) {
     if (item < nitems) {
       const int64_t cl = item / a.nw;
       const int iw = (int)(item - cl * a.nw);
-      solve_item<FORM, GREY>(a, cl, iw, gam, uu, o1);
+      DirectPillars pa{a.pil + cl * (int64_t)a.nz * NF};
+      solve_item<FORM, GREY>(a, cl, iw, true, pa, gam, uu, o1, qs);
+    }
+  }
+}
+
+/* Staged path: warp tasks are (column, tile of 32 wavelengths); the column's pillar records
+ * are streamed into shared memory by bulk copies (see StagedPillars). */
+template <int FORM, bool GREY>
+__global__ void __launch_bounds__(128) k_solve_staged(const SolveArgs a) {
+  __shared__ __align__(128) double s_pil[WARPS_PER_BLOCK][2 * ZC * NF];
+  __shared__ __align__(8) unsigned long long s_bar[WARPS_PER_BLOCK][2];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int ntiles = (a.nw + 31) / 32;
+  const unsigned long long ntasks = (unsigned long long)a.ncol * ntiles;
+  double *gam = a.gam + slot * 32 + lane;
+  double *uu = a.uu + slot * 32 + lane;
+  double *o1 = a.o1 + slot * 32 + lane;
+  double *qs = a.q + slot * 32 + lane;
+  StagedPillars pa;
+  pa.buf = s_pil[wib];
+  pa.bar0 = smem_addr(&s_bar[wib][0]);
+  pa.nz = a.nz;
+  pa.waits = 0;
+  pa.inflight = 0;
+  pa.failed = false;
+  if (lane == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(pa.bar0) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(pa.bar0 + 8u) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  for (;;) {
+    unsigned long long task = 0;
+    if (lane == 0) task = atomicAdd(a.work, 1ull);
+    task = __shfl_sync(0xffffffffu, task, 0);
+    if (task >= ntasks) break;
+    const int64_t cl = (int64_t)(task / ntiles);
+    const int tile = (int)(task - (unsigned long long)cl * ntiles);
+    const int iw_raw = tile * 32 + lane;
+    const bool active = iw_raw < a.nw;
+    const int iw = active ? iw_raw : a.nw - 1;
+    pa.begin(a.pil + cl * (int64_t)a.nz * NF, lane);
+    solve_item<FORM, GREY>(a, cl, iw, active, pa, gam, uu, o1, qs);
+    if (__any_sync(0xffffffffu, pa.failed)) {
+      if (lane == 0) atomicOr(&a.status[2], 1ull);
+      /* let copies still in flight land (bounded) before the block's shared memory is released */
+      pa.wait(0);
+      pa.wait(1);
+      return;
     }
   }
 }
@@ -373,32 +612,31 @@ cudaError_t launch_pillars(const double *rho, const double *T, int64_t ncol, int
   return cudaGetLastError();
 }
 
-static const void *solve_fn(int form, int grey) {
+bool solve_uses_staging(int nw) { return nw >= 64 || (nw % 32) == 0; }
+
+static const void *solve_fn(int form, int grey, bool staged) {
+  if (staged) {
+    if (form == 0) return grey ? (const void *)k_solve_staged<0, true> : (const void *)k_solve_staged<0, false>;
+    return grey ? (const void *)k_solve_staged<1, true> : (const void *)k_solve_staged<1, false>;
+  }
   if (form == 0) return grey ? (const void *)k_solve<0, true> : (const void *)k_solve<0, false>;
   return grey ? (const void *)k_solve<1, true> : (const void *)k_solve<1, false>;
 }
 
 int solve_fp64_max_blocks_per_sm(int form, int grey, int threads) {
-  int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, solve_fn(form, grey), threads, 0) != cudaSuccess)
-    return 1;
+  int nb = 0, nb2 = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, solve_fn(form, grey, false), threads, 0) != cudaSuccess)
+    nb = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, solve_fn(form, grey, true), threads, 0) != cudaSuccess)
+    nb2 = 1;
+  nb = nb > nb2 ? nb : nb2;
   return nb > 0 ? nb : 1;
 }
 
-cudaError_t launch_solve_fp64(const SolveArgs &a, int form, int grey, int blocks, int threads,
-                              cudaStream_t s) {
-  if (form == 0) {
-    if (grey)
-      k_solve<0, true><<<blocks, threads, 0, s>>>(a);
-    else
-      k_solve<0, false><<<blocks, threads, 0, s>>>(a);
-  } else {
-    if (grey)
-      k_solve<1, true><<<blocks, threads, 0, s>>>(a);
-    else
-      k_solve<1, false><<<blocks, threads, 0, s>>>(a);
-  }
-  return cudaGetLastError();
+cudaError_t launch_solve_fp64(const SolveArgs &a, int form, int grey, int blocks, int threads, cudaStream_t s) {
+  const bool staged = !grey && solve_uses_staging(a.nw);
+  void *args[] = {(void *)&a};
+  return cudaLaunchKernel(solve_fn(form, grey, staged), dim3(blocks), dim3(threads), args, 0, s);
 }
 
 }  // namespace oco

@@ -1,0 +1,388 @@
+/*
+ * kernels_mixed.cu -- the mixed-precision form (OCO_FORM_MIXED) on sm_100a.
+ *
+ *   k_solve_mixed     persistent kernel, one thread per (column, wavelength); warp tasks are
+ *                     (column, 32 wavelengths) with the column's records streamed into shared
+ *                     memory by bulk copies (TMA, mbarrier, bounded waits), or 32 consecutive
+ *                     items with direct loads when nw is small.  Forward sweep: log2-space
+ *                     opacity, scaled rows and the difference-form Thomas elimination in FP32
+ *                     (the source function's exponent as integer + FP32 fraction),
+ *                     writing kappa and a 16-byte scratch record per z (|gamma| or q, 1/kappa, u
+ *                     mantissa and exponent); reverse sweep: extended-range FP32
+ *                     back-substitution, the differences D_j, and the flux from a 6-value
+ *                     window of differences, with FP64 outputs.
+ * See mixed_core.h for the arithmetic and its relation to the reference.
+ */
+#include <cuda_runtime.h>
+
+#include "mixed_core.h"
+#include "oco_internal.h"
+
+namespace oco {
+using namespace oco::mx;
+
+constexpr int MZC = 32;            /* z records per staged chunk (32 x 160 B) */
+constexpr int MWARPS = 4;          /* warps per 128-thread block */
+constexpr long long kMSpinLimit = 1ll << 26;
+#ifndef OCO_MIXED_PREFETCH
+#define OCO_MIXED_PREFETCH 4 /* reverse-sweep steps whose scratch loads are issued together */
+#endif
+
+/* Shared-memory record accessor. */
+struct MRec {
+  const float *p;
+  __device__ __forceinline__ float operator[](int f) const { return p[f]; }
+};
+struct MGRec {
+  const float *p;
+  __device__ __forceinline__ float operator[](int f) const { return __ldg(p + f); }
+};
+
+__device__ __forceinline__ uint32_t msmem(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mtry_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+/* Per-warp double-buffered stream of one column's records (see StagedPillars in
+ * kernels_fp64.cu for the protocol). */
+struct MStaged {
+  float *buf;
+  uint32_t bar0;
+  const float *src;
+  int nz, nchunks, cur;
+  uint32_t waits, inflight;
+  bool failed;
+  __device__ __forceinline__ void issue(int c) {
+    const int rows = min(MZC, nz - c * MZC);
+    const uint32_t bytes = (uint32_t)(rows * MZN * sizeof(float));
+    const uint32_t bar = bar0 + 8u * (c & 1);
+    const uint32_t dst = msmem(buf + (c & 1) * (MZC * MZN));
+    const size_t g = __cvta_generic_to_global(src + (int64_t)c * MZC * MZN);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(g), "r"(bytes), "r"(bar)
+                 : "memory");
+  }
+  __device__ __forceinline__ bool wait(int b) {
+    if (!((inflight >> b) & 1u)) return true;
+    const uint32_t bar = bar0 + 8u * b;
+    const uint32_t parity = (waits >> b) & 1u;
+    long long spins = 0;
+    while (!mtry_wait(bar, parity))
+      if (++spins > kMSpinLimit) return false;
+    waits ^= 1u << b;
+    inflight &= ~(1u << b);
+    return true;
+  }
+  __device__ __forceinline__ void begin(const float *column) {
+    src = column;
+    cur = -1;
+    nchunks = (nz + MZC - 1) / MZC;
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) issue(0);
+    inflight |= 1u;
+  }
+  __device__ __forceinline__ MRec at(int z) {
+    const int c = z / MZC;
+    if (c != cur) {
+      __syncwarp();
+      if (!failed && c + 1 < nchunks) {
+        if ((threadIdx.x & 31) == 0) issue(c + 1);
+        inflight |= 1u << ((c + 1) & 1);
+      }
+      if (!failed && !wait(c & 1)) failed = true;
+      cur = c;
+    }
+    return MRec{buf + (c & 1) * (MZC * MZN) + (z - c * MZC) * MZN};
+  }
+};
+
+struct MDirect {
+  const float *base;
+  __device__ __forceinline__ MGRec at(int z) { return MGRec{base + (int64_t)z * MZN}; }
+};
+
+__device__ __forceinline__ void load_lam32(Lam32 &L, const float *__restrict__ t, int iw, int nw) {
+#define LF(f) __ldg(t + (int64_t)(f) * nw + iw)
+  L.cl2 = LF(ML_CL2);
+  L.law = LF(ML_LAW);
+#pragma unroll
+  for (int q = 0; q < 6; q++) L.g[q] = LF(ML_G1 + q);
+  L.n0 = (int)LF(ML_N0);
+  L.ls = LF(ML_LS);
+  L.f1 = LF(ML_F1);
+  L.f2 = LF(ML_F2);
+  L.f3 = LF(ML_F3);
+  L.lal0w = LF(ML_LAL0W);
+  L.gff = LF(ML_GFF);
+  L.chi1 = LF(ML_CHI1);
+  L.lnnu9 = LF(ML_LNNU9);
+  L.hnuk = LF(ML_HNUK);
+  L.l3nu = LF(ML_L3NU);
+  L.ch = LF(ML_CH);
+  L.cl = LF(ML_CL);
+  L.lsi = LF(ML_LSI);
+  L.lsf = LF(ML_LSF);
+#undef LF
+}
+
+/* One (column, wavelength) item.  Scratch: one float4 per z (see the forward sweep). */
+template <class PA>
+__device__ __forceinline__ void msolve_item(const MixedArgs &a, int64_t cl, int iw, bool active, PA &pa,
+                                            float4 *__restrict__ s4) {
+  const int nz = a.nz;
+  const int64_t ss = a.slot_stride;
+  Lam32 L;
+  load_lam32(L, a.lam, iw, a.nw);
+  const int64_t idx = (a.layout == 0) ? (int64_t)iw * a.ld_col + a.c_off + cl : (a.c_off + cl) * a.nw + iw;
+  double *Ub = a.U + idx * a.U_is;
+  double *Kb = (a.K && active) ? a.K + idx * a.K_is : nullptr;
+  double *Vb = (a.V && active) ? a.V + idx * a.V_is : nullptr;
+  const float dzf = (float)a.dz, ldz2 = a.ldz2;
+
+  Opac32 cur = opacity(pa.at(0), L);
+  Opac32 nxt = opacity(pa.at(1), L);
+  float kc = kappa_lin(cur.lk), kn = kappa_lin(nxt.lk), kprev = 0.0f;
+  Row32 r = row_boundary(kc, cur, dzf, ldz2, false);
+  float h = r.e, cprev = r.c;
+  XF u = xexp2(r.ldi, r.ldf);
+  u = xnorm(u.m * rcp(r.c + h), u.e);
+  float o1 = rcp(kc);
+  if (Kb) Kb[0] = (double)kc;
+  /* scratch record of z = j: {v_j, 1/kappa_j, u_j mantissa, u_j exponent} where v_j holds the
+   * smaller of q_j = h_j/(c_j+h_j) and |gamma_{j+1}| = c_j/(c_j+h_j) (they sum to 1; a negative
+   * v_j stores -|gamma_{j+1}|), written once row j+1 is known */
+  float4 pend = make_float4(0.0f, o1, u.m, (float)u.e);
+  for (int j = 1; j < nz; j++) {
+    kprev = kc;
+    cur = nxt;
+    kc = kn;
+    if (j < nz - 1) {
+      nxt = opacity(pa.at(j + 1), L);
+      kn = kappa_lin(nxt.lk);
+      r = row_center(kprev, kc, kn, cur, ldz2);
+    } else {
+      r = row_boundary(kc, cur, dzf, ldz2, true);
+    }
+    const float rr = rcp(cprev + h);
+    const float qv = h * rr, gv = cprev * rr;
+    pend.x = (qv < gv) ? qv : -gv;
+    s4[(int64_t)(j - 1) * ss] = pend;
+    h = r.e + (r.a * rr) * h; /* a'/(c'+h) is O(1); a' h alone can overflow */
+    const float rb = rcp(r.c + h);
+    u = xaxpy(xexp2(r.ldi, r.ldf), rb, u, r.a * rb);
+    o1 = rcp(kc);
+    if (Kb) Kb[(int64_t)j * a.K_zs] = (double)kc;
+    pend = make_float4(0.0f, o1, u.m, (float)u.e);
+    cprev = r.c;
+  }
+  s4[(int64_t)(nz - 1) * ss] = pend;
+  if (!active) return;
+
+  /* reverse sweep */
+  const int n = nz;
+  const double dz1 = 1.0 / a.dz;
+  const int64_t uz = a.U_zs;
+  XF Un = u; /* U_{n-1} */
+  Ub[(int64_t)(3 + n - 1) * uz] = xtod(Un);
+  double vtop = 0.0, vbot = 0.0;
+  if (nz >= 4) {
+    /* window of differences d0..d5 = D_k..D_{k+5}; V_{k+3} from it */
+    double d0, d1, d2, d3, d4, d5;
+    double Uk[3];
+    /* D_{n-2}, D_{n-3}, D_{n-4} first (top ghosts mirror them) */
+    double Dt[3];
+    const float nx4_top_o1 = s4[(int64_t)(n - 1) * ss].y; /* 1/kappa_{n-1} */
+    float o1t[3];
+#pragma unroll
+    for (int t = 0; t < 3; t++) {
+      const int k = n - 2 - t;
+      const float4 w = s4[(int64_t)k * ss];
+      o1t[t] = w.y;
+      const float g1 = (w.x >= 0.0f) ? 1.0f - w.x : -w.x;
+      const float qk = (w.x >= 0.0f) ? w.x : 1.0f + w.x;
+      XF uj;
+      uj.m = w.z;
+      uj.e = (int)w.w;
+      XF Dj = xaxpy(uj, 1.0f, Un, -qk);
+      Un = xaxpy(uj, 1.0f, Un, g1);
+      Uk[t] = xtod(Un);
+      Ub[(int64_t)(3 + k) * uz] = Uk[t];
+      Dt[t] = xtod(Dj);
+    }
+    const float o1_nm2 = o1t[0], o1_nm3 = o1t[1], o1_nm4 = o1t[2];
+    /* top ghosts f(n2+i) = 2 f(n2) - f(n2-i) */
+    const double fn = xtod(u);
+    Ub[(int64_t)(n + 3) * uz] = 2.0 * fn - Uk[0];
+    Ub[(int64_t)(n + 4) * uz] = 2.0 * fn - Uk[1];
+    Ub[(int64_t)(n + 5) * uz] = 2.0 * fn - Uk[2];
+    /* window for V_{n-1}: D_{n-4} .. D_{n+1} = Dt[2], Dt[1], Dt[0], D_{n-1}=Dt[0], D_n=Dt[1], D_{n+1}=Dt[2] */
+    d0 = Dt[2]; d1 = Dt[1]; d2 = Dt[0]; d3 = Dt[0]; d4 = Dt[1]; d5 = Dt[2];
+    auto emit = [&](int j, float o1j) -> double {
+      const double s1 = d2 + d3;
+      const double s2 = (s1 + d1) + d4;
+      const double s3 = (s2 + d0) + d5;
+      const double df = -((1.0 / 60.0) * (((45.0 * s1) - 9.0 * s2) + s3));
+      const double v = ((-(double)o1j) * df) * dz1;
+      if (Vb) Vb[(int64_t)j * a.V_zs] = v;
+      return v;
+    };
+    vtop = emit(n - 1, nx4_top_o1);
+    /* o1 ring: r1, r2, r3 = 1/kappa of k+1, k+2, k+3 before step k */
+    float r1 = o1_nm4, r2 = o1_nm3, r3 = o1_nm2;
+    auto step = [&](int k, const float4 &w) {
+      const float g1 = (w.x >= 0.0f) ? 1.0f - w.x : -w.x; /* |gamma_{k+1}| */
+      const float qk = (w.x >= 0.0f) ? w.x : 1.0f + w.x;  /* q_k */
+      XF uj;
+      uj.m = w.z;
+      uj.e = (int)w.w;
+      XF Dj = xaxpy(uj, 1.0f, Un, -qk);
+      Un = xaxpy(uj, 1.0f, Un, g1);
+      Ub[(int64_t)(3 + k) * uz] = xtod(Un);
+      d5 = d4; d4 = d3; d3 = d2; d2 = d1; d1 = d0; d0 = xtod(Dj);
+      emit(k + 3, r3);
+      r3 = r2; r2 = r1; r1 = w.y;
+    };
+    int k = n - 5;
+    constexpr int PF = OCO_MIXED_PREFETCH;
+    for (; k >= PF - 1; k -= PF) { /* scratch loads of PF steps hoisted off the serial chain */
+      float4 w[PF];
+#pragma unroll
+      for (int q = 0; q < PF; q++) w[q] = s4[(int64_t)(k - q) * ss];
+#pragma unroll
+      for (int q = 0; q < PF; q++) step(k - q, w[q]);
+    }
+    for (; k >= 0; k--) step(k, s4[(int64_t)k * ss]);
+    /* bottom ghosts f(n1-i) = 2 f(n1) - f(n1+i); ghost differences mirror D_0, D_1, D_2 */
+    const double f0 = Ub[(int64_t)3 * uz], f1 = Ub[(int64_t)4 * uz], f2 = Ub[(int64_t)5 * uz], f3 = Ub[(int64_t)6 * uz];
+    Ub[(int64_t)2 * uz] = 2.0 * f0 - f1;
+    Ub[(int64_t)1 * uz] = 2.0 * f0 - f2;
+    Ub[0] = 2.0 * f0 - f3;
+    const double D0 = d0, D1 = d1, D2 = d2;
+    d5 = d4; d4 = d3; d3 = d2; d2 = d1; d1 = d0; d0 = D0; /* D_{-1} = D_0 */
+    emit(2, r3);
+    d5 = d4; d4 = d3; d3 = d2; d2 = d1; d1 = d0; d0 = D1; /* D_{-2} = D_1 */
+    emit(1, r2);
+    d5 = d4; d4 = d3; d3 = d2; d2 = d1; d1 = d0; d0 = D2; /* D_{-3} = D_2 */
+    vbot = emit(0, r1);
+  } else { /* nz = 2 or 3: U stencil on the ghosted array (the reference's update order) */
+    double f[9];
+    const int n1 = 3, n2 = nz + 2;
+    f[n1 + nz - 1] = xtod(Un);
+    for (int j = nz - 2; j >= 0; j--) {
+      const float4 w = s4[(int64_t)j * ss];
+      const float g1 = (w.x >= 0.0f) ? 1.0f - w.x : -w.x;
+      XF uj;
+      uj.m = w.z;
+      uj.e = (int)w.w;
+      Un = xaxpy(uj, 1.0f, Un, g1);
+      f[n1 + j] = xtod(Un);
+    }
+    for (int i = 1; i <= 3; i++) {
+      f[n1 - i] = 2.0 * f[n1] - f[n1 + i];
+      f[n2 + i] = 2.0 * f[n2] - f[n2 - i];
+    }
+    for (int m = 0; m < nz + 6; m++) Ub[(int64_t)m * uz] = f[m];
+    for (int j = 0; j < nz; j++) {
+      const int c = n1 + j;
+      const double df = (1.0 / 60.0) * (((45.0 * (f[c + 1] - f[c - 1])) - 9.0 * (f[c + 2] - f[c - 2])) + (f[c + 3] - f[c - 3]));
+      const double v = ((-(double)s4[(int64_t)j * ss].y) * df) * dz1;
+      if (Vb) Vb[(int64_t)j * a.V_zs] = v;
+      if (j == 0) vbot = v;
+      if (j == nz - 1) vtop = v;
+    }
+  }
+  const int64_t pidx = (int64_t)iw * a.ld_col + a.c_off + cl;
+  if (a.Vtop) a.Vtop[pidx] = vtop;
+  if (a.Vbot) a.Vbot[pidx] = vbot;
+}
+
+__global__ void __launch_bounds__(128) k_solve_mixed_staged(const MixedArgs a) {
+  __shared__ __align__(128) float s_rec[MWARPS][2 * MZC * MZN];
+  __shared__ __align__(8) unsigned long long s_bar[MWARPS][2];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int ntiles = (a.nw + 31) / 32;
+  const unsigned long long ntasks = (unsigned long long)a.ncol * ntiles;
+  float4 *s4 = a.s4 + slot * 32 + lane;
+  MStaged pa;
+  pa.buf = s_rec[wib];
+  pa.bar0 = msmem(&s_bar[wib][0]);
+  pa.nz = a.nz;
+  pa.waits = 0;
+  pa.inflight = 0;
+  pa.failed = false;
+  if (lane == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(pa.bar0) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(pa.bar0 + 8u) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  for (;;) {
+    unsigned long long task = 0;
+    if (lane == 0) task = atomicAdd(a.work, 1ull);
+    task = __shfl_sync(0xffffffffu, task, 0);
+    if (task >= ntasks) break;
+    const int64_t cl = (int64_t)(task / ntiles);
+    const int tile = (int)(task - (unsigned long long)cl * ntiles);
+    const int iw_raw = tile * 32 + lane;
+    const bool active = iw_raw < a.nw;
+    const int iw = active ? iw_raw : a.nw - 1;
+    pa.begin(a.rec + cl * (int64_t)a.nz * MZN);
+    msolve_item(a, cl, iw, active, pa, s4);
+    if (__any_sync(0xffffffffu, pa.failed)) {
+      if (lane == 0) atomicOr(&a.status[2], 1ull);
+      pa.wait(0);
+      pa.wait(1);
+      return;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128) k_solve_mixed(const MixedArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nitems = a.ncol * a.nw;
+  const unsigned long long ntasks = (unsigned long long)((nitems + 31) / 32);
+  float4 *s4 = a.s4 + slot * 32 + lane;
+  for (;;) {
+    unsigned long long task = 0;
+    if (lane == 0) task = atomicAdd(a.work, 1ull);
+    task = __shfl_sync(0xffffffffu, task, 0);
+    if (task >= ntasks) break;
+    const int64_t item = (int64_t)task * 32 + lane;
+    if (item < nitems) {
+      const int64_t cl = item / a.nw;
+      const int iw = (int)(item - cl * a.nw);
+      MDirect pa{a.rec + cl * (int64_t)a.nz * MZN};
+      msolve_item(a, cl, iw, true, pa, s4);
+    }
+  }
+}
+
+int solve_mixed_max_blocks_per_sm(int threads) {
+  int a = 0, b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_solve_mixed, threads, 0) != cudaSuccess) a = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_solve_mixed_staged, threads, 0) != cudaSuccess) b = 1;
+  a = a > b ? a : b;
+  return a > 0 ? a : 1;
+}
+
+cudaError_t launch_solve_mixed(const MixedArgs &a, int blocks, int threads, cudaStream_t s) {
+  const bool staged = (a.nw >= 64) || (a.nw % 32) == 0;
+  if (staged)
+    k_solve_mixed_staged<<<blocks, threads, 0, s>>>(a);
+  else
+    k_solve_mixed<<<blocks, threads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace oco

@@ -1,0 +1,42 @@
+/*
+ * kernels_mixed_pillars.cu -- per-(column, z) records of the mixed-precision form.
+ *
+ *   k_pillars_mixed   one thread per (column, z): Saha ionization and the z-only factors in
+ *                     FP64, written as the FP32 log2 record of mixed_core.h (MixedZ, 160 B).
+ *
+ * Compiled with -fmad=false like the FP64 kernels: the Saha quadratic
+ * 0.5*(sqrt(C^2 + 4C) - C) (gas_state.f90:63) cancels as the gas approaches full ionization
+ * (1 - x ~ 1e-7 carries ~1% rounding error in FP64, as the reference's own comment notes), so
+ * the FP64 form of this arithmetic must be the reference's, operation for operation, for the
+ * mixed form to agree with the FP64 forms there.
+ */
+#include <cuda_runtime.h>
+
+#include "mixed_core.h"
+#include "oco_internal.h"
+
+namespace oco {
+using namespace oco::mx;
+
+__global__ void __launch_bounds__(256) k_pillars_mixed(const double *__restrict__ rho, const double *__restrict__ T,
+                                                       int64_t n, double fully_ionized_T, float *__restrict__ rec) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float r[MZN];
+  pillar(rho[i], T[i], fully_ionized_T, r);
+  float4 *o = reinterpret_cast<float4 *>(rec + i * MZN);
+#pragma unroll
+  for (int k = 0; k < MZN / 4; k++) o[k] = make_float4(r[4 * k], r[4 * k + 1], r[4 * k + 2], r[4 * k + 3]);
+}
+
+static_assert(MZN == MIXED_ZN, "mixed record size");
+
+cudaError_t launch_pillars_mixed(const double *rho, const double *T, int64_t ncol, int nz, double fully_ionized_T,
+                                 float *rec, cudaStream_t s) {
+  const int64_t n = ncol * nz;
+  if (n == 0) return cudaSuccess;
+  k_pillars_mixed<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(rho, T, n, fully_ionized_T, rec);
+  return cudaGetLastError();
+}
+
+}  // namespace oco

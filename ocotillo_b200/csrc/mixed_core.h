@@ -1,0 +1,535 @@
+/*
+ * mixed_core.h -- the mixed-precision form of the per-(column, wavelength) solve, shared by
+ * the CUDA kernels (kernels_mixed.cu) and a host build used for accuracy studies.
+ *
+ * Same physics and the same linear system as the reference loop
+ * (source/flux_feautrier.f90:160-228), evaluated as follows:
+ *   - per (column, z), in FP64: Saha ionization and every z-only factor, as in the FP64
+ *     pillar kernel, stored as a record of base-2 logarithms (MixedZ) so that nothing
+ *     underflows (opacity terms per H atom span ~1e-60..1e-17);
+ *   - per (z, lambda), in FP32 log2 space: every opacity term of calc_opacity_and_albedo
+ *     (continuous_opacity.f90:175-201) is a sum of log2 factors; terms are added with a
+ *     log-sum-exp on the SFU (ex2/lg2).  The source function is the one quantity that needs
+ *     more: in optically thick cells U ~ S and the flux is a ~1% difference of U, so S (and
+ *     the right-hand side S*e') must be good to ~1e-7, while log2 S reaches ~100 (an FP32
+ *     logarithm of that size resolves only ~5e-6).  The Planck exponent x*log2(e) is
+ *     therefore formed as a double-float product (hi + lo, FMA two-product of split FP32
+ *     factors), and log2 S and log2(S e') are carried as an exact integer plus an FP32
+ *     fraction.  The H bound-free level sum
+ *     sum_n g(lambda,n) n^-3 exp(-chi_n/kT) (:237-239) is factored by its first non-zero
+ *     level n0(lambda): E_n0 * (g_n0 + sum_{n>n0} g_n * E_n/E_n0), with the ratios E_n/E_n0
+ *     precomputed per z.  The albedo enters only as log2(1 - omega), computed from the
+ *     absorption terms themselves (no cancellation when scattering dominates).  The
+ *     reference's double addition of the H free-free opacity (:267-268, :274-275) is kept:
+ *     neutral cells get kappa = rho (2 kr0 + kHff/mp), kappa_rad = kr0 + kHff/mp; ionized
+ *     cells kappa = rho kr0 + k_brems, kappa_rad = 2 kr0 + k_brems/rho.
+ *   - the tridiagonal system of auxiliary.f90:111-201 with every row divided by kappa_i^2
+ *     (a' = 1/kappa_{i-1/2}, c' = 1/kappa_{i+1/2}, diagonal excess dz^2 kappa (1-omega)) and
+ *     the Thomas recursion in difference form (all terms non-negative), in FP32, with the
+ *     right-hand side and u carried as extended-exponent FP32 (XF) values;
+ *   - back-substitution in extended FP32 for U_j and for the differences
+ *     D_j = U_j - U_{j+1} = u_j - q_j U_{j+1} (q_j = h_j/(c_j+h_j)), so the flux never
+ *     subtracts two nearly equal U; ghost zones and the 6th-order flux in FP64 from the D_j;
+ *     outputs U, kappa, V in FP64.
+ */
+#ifndef OCO_MIXED_CORE_H
+#define OCO_MIXED_CORE_H
+
+#include <math.h>
+#include <stdint.h>
+
+#include "ocomath.h"
+#include "oco_consts.h"
+
+#ifdef __CUDACC__
+#define MX_HD static __host__ __device__ __forceinline__
+#else
+#define MX_HD static inline
+#endif
+
+namespace oco {
+namespace mx {
+
+/* Per-(column, z) FP32 record: base-2 logarithms of the z-only factors, a few linear values,
+ * and damping_factor_const/T split into hi + lo (the Planck exponent needs it to ~1e-12). */
+enum MixedZ {
+  MZ_TH = 0,     /* theta = 5040/T */
+  MZ_LIONF,      /* log2(ionization_factor) */
+  MZ_LE2,        /* log2 exp(-chi_n k1 T1), n = 2..6 (n = 1 is 0) */
+  MZ_LE3,
+  MZ_LE4,
+  MZ_LE5,
+  MZ_LE6,
+  MZ_R,          /* 15 ratios E_n/E_n0 for n0 = 1..5, n = n0+1..6 (linear) */
+  MZ_LU = MZ_R + 15, /* log2(Unsold integral) */
+  MZ_LHM,        /* log2(hm_bf_factor * ionf) */
+  MZ_LAFF,       /* log2(ionf ne k T) */
+  MZ_LGT,        /* log10(theta) */
+  MZ_LGT2,       /* log10(theta)^2 */
+  MZ_LESC,       /* log2(e_scatter) */
+  MZ_LRHO,       /* log2(rho) */
+  MZ_NEUTRAL,    /* 1 if (1 - NHII/N) > switch_ionfraction */
+  MZ_LIONFEF,    /* log2(ionf * energyfactor) */
+  MZ_TH1L,       /* theta1 * log10e */
+  MZ_LNTPOW,     /* ln((T*1e-4)^-1.5) */
+  MZ_LZ,         /* ln(ne (nHI+nHII)) - 0.5 ln T */
+  MZ_T1,         /* 1/T */
+  MZ_DFT1,       /* damping_factor_const / T, high part */
+  MZ_DFT1L,      /* low part */
+  MZN = 40       /* 160 B (padded) */
+};
+
+/* Per-wavelength FP32 record (device layout [field][nw]). */
+enum MixedL {
+  ML_CL2 = 0,  /* chi * log2(10) */
+  ML_LAW,      /* log2(AHbf * wa^3) */
+  ML_G1,       /* g(lambda,n) * n^-3, n = 1..6 */
+  ML_G2,
+  ML_G3,
+  ML_G4,
+  ML_G5,
+  ML_G6,
+  ML_N0,       /* first level with g > 0 (1..6), 7 if none */
+  ML_LS,       /* log2(s_coeff) if wa < 16000 else -1000 */
+  ML_F1,
+  ML_F2,
+  ML_F3,
+  ML_LAL0W,    /* log2(alpha0 * wa^3 * mp1) */
+  ML_GFF,
+  ML_CHI1,
+  ML_LNNU9,    /* ln(nu * 1e-9) */
+  ML_HNUK,     /* h nu / k */
+  ML_L3NU,     /* 3 ln nu */
+  ML_CH,       /* log2(e) / lambda_cm, high part */
+  ML_CL,       /* low part */
+  ML_LSI,      /* log2(2 h c^2 lambda_cm^-5) = LSI + LSF, LSI an integer */
+  ML_LSF,
+  MLN = 24
+};
+
+constexpr float kNeg = -1000.0f; /* log2 of a vanishing term */
+constexpr double kLog2e = 1.4426950408889634;
+constexpr double kLn2 = 0.6931471805599453;
+constexpr double kLog2_10 = 3.321928094887362;
+constexpr float kLog2e_f = 1.44269504f;
+constexpr float kLn2_f = 0.693147181f;
+constexpr float kLog2_10_f = 3.32192809f;
+
+/* ---- SFU helpers: MUFU on the device, libm on the host ---------------------------- */
+MX_HD float ex2(float x) {
+#ifdef __CUDA_ARCH__
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+#else
+  return exp2f(x);
+#endif
+}
+MX_HD float lg2(float x) {
+#ifdef __CUDA_ARCH__
+  float y;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+#else
+  return log2f(x);
+#endif
+}
+MX_HD float rcp(float x) {
+#ifdef __CUDA_ARCH__
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+#else
+  return 1.0f / x;
+#endif
+}
+
+MX_HD float fmaxf_(float a, float b) { return a > b ? a : b; }
+/* log2(2^a + 2^b) */
+MX_HD float lae2(float a, float b) {
+  float m = fmaxf_(a, b), d = (a > b) ? b - a : a - b;
+  return m + lg2(1.0f + ex2(d));
+}
+/* log2(1 - 2^-t) for t > 0 (accurate to a few 1e-7 relative of the result's argument
+ * for t >= 2^-6; a two-term series below that). */
+MX_HD float log2_one_minus_exp2neg(float t) {
+  if (t < 0.015625f) {
+    float x = t * kLn2_f; /* 1 - e^-x = x (1 - x/2 + x^2/6) */
+    return lg2(x * (1.0f - x * (0.5f - x * (1.0f / 6.0f))));
+  }
+  return lg2(1.0f - ex2(-t));
+}
+
+MX_HD float tolog(double v) { return v > 0.0 ? (float)(oco_log(v) * kLog2e) : kNeg; }
+/* hi + lo split of a double into two floats */
+MX_HD void split2(double v, float &hi, float &lo) {
+  hi = (float)v;
+  lo = (float)(v - (double)hi);
+}
+
+/* ---- per-(column, z) record (gas_state.f90:30-110, c_o :143-163) ------------------------ */
+MX_HD void pillar(double r, double t, double fully_ionized_T, float *o) {
+  using namespace oco::k;
+  const double rho1 = 1.0 / r, T1 = 1.0 / t;
+  double c_ion = (mp * rho1) * (saha_const * oco_pow(t, 1.5) * oco_exp(-((T1 * hydrogen_ionization_eV) * k1_eV)));
+  double x = 0.5 * (sqrt(c_ion * c_ion + 4.0 * c_ion) - c_ion);
+  if (t > fully_ionized_T) x = 1.0;
+  double nn = r * mp1, nHII = x * nn, nHI = nn - nHII, ne = nHII;
+  double ionf = (nHI != 0.0) ? nHI / (nHI + nHII) : 0.0;
+  double Pe = (ne * k_cgs) * t;
+  double escat = (alpha_e * nHII) * (rho1 * mp);
+  double theta = 5040.0 * T1, theta1 = 1.0 / theta;
+  double lgt = oco_log10(theta);
+  double ktemp1 = k1_cgs * T1;
+  double chi[7];
+  for (int n = 1; n <= 6; n++) {
+    double n1 = 1.0 / (double)n;
+    chi[n] = RydbergEnergy * (1.0 - n1 * n1);
+  }
+  o[MZ_TH] = (float)(theta);
+  o[MZ_LIONF] = tolog(ionf);
+  for (int n = 2; n <= 6; n++) o[MZ_LE2 + n - 2] = (-(chi[n] * ktemp1) * kLog2e);
+  int q = 0;
+  for (int n0 = 1; n0 <= 5; n0++)
+    for (int n = n0 + 1; n <= 6; n++) o[MZ_R + q++] = oco_exp(-((chi[n] - chi[n0]) * ktemp1));
+  /* Unsold: 0.5 kT/Ry (exp(-chi_6/kT) - exp(-Ry/kT)) = 0.5 kT/Ry e^{-chi_6/kT} (1 - e^{-(Ry-chi_6)/kT}) */
+  double lu = oco_log((0.5 * (k_cgs * t)) * RydbergEnergy1) - chi[6] * ktemp1 +
+              oco_log(1.0 - oco_exp(-((RydbergEnergy - chi[6]) * ktemp1)));
+  o[MZ_LU] = (float)((lu * kLog2e));
+  /* hm_bf_factor = 4.158e-10 Pe theta^2.5 10^(0.754 theta), in logs */
+  double lhm = (Pe > 0.0 && ionf > 0.0)
+                   ? (oco_log(4.158e-10 * Pe) + 2.5 * oco_log(theta)) * kLog2e + 0.754 * theta * kLog2_10 + oco_log(ionf) * kLog2e
+                   : (double)kNeg;
+  o[MZ_LHM] = (float)(lhm);
+  o[MZ_LAFF] = tolog(((ionf * ne) * k_cgs) * t);
+  o[MZ_LGT] = (float)(lgt);
+  o[MZ_LGT2] = (float)((lgt * lgt));
+  o[MZ_LESC] = tolog(escat);
+  o[MZ_LRHO] = (float)((oco_log(r) * kLog2e));
+  o[MZ_NEUTRAL] = (float)(((1.0 - x) > switch_ionfraction) ? 1.0 : 0.0);
+  /* energyfactor = 0.5 log10e theta1 / Iev * 10^(-theta Iev) */
+  double lef = oco_log(((0.5 * log10e) * theta1) * Iev1) * kLog2e - theta * Iev * kLog2_10;
+  o[MZ_LIONFEF] = (float)(ionf > 0.0 ? (lef + oco_log(ionf) * kLog2e) : (double)kNeg);
+  o[MZ_TH1L] = (float)((theta1 * log10e));
+  o[MZ_LNTPOW] = (float)((-1.5 * oco_log(t * 1e-4)));
+  double nprod = ne * (nHI + nHII);
+  o[MZ_LZ] = (float)(nprod > 0.0 ? (oco_log(nprod) - 0.5 * oco_log(t)) : (double)kNeg * kLn2);
+  o[MZ_T1] = (float)(T1);
+  split2(damping_factor_const * T1, o[MZ_DFT1], o[MZ_DFT1L]);
+  for (int k2 = MZ_DFT1L + 1; k2 < MZN; k2++) o[k2] = 0.0f;
+}
+
+/* ---- per-wavelength record from the FP64 table entries --------------------------------- */
+struct LamIn {
+  double chi, gff, chi1, wa3, s, hmon, f1, f2, f3, gn[6], nu9, l3nu, hnuk, wcm1, sw5;
+};
+MX_HD void lambda_record(const LamIn &L, float *o) {
+  using namespace oco::k;
+  o[ML_CL2] = (float)(L.chi * kLog2_10);
+  o[ML_LAW] = (float)(oco_log(AHbf * L.wa3) * kLog2e);
+  int n0 = 7;
+  for (int n = 6; n >= 1; n--) {
+    o[ML_G1 + n - 1] = (float)L.gn[n - 1];
+    if (L.gn[n - 1] > 0.0) n0 = n;
+  }
+  o[ML_N0] = (float)n0;
+  o[ML_LS] = (L.hmon != 0.0 && L.s > 0.0) ? (float)(oco_log(L.s) * kLog2e) : kNeg;
+  o[ML_F1] = (float)L.f1;
+  o[ML_F2] = (float)L.f2;
+  o[ML_F3] = (float)L.f3;
+  o[ML_LAL0W] = (float)(oco_log((alpha0 * L.wa3) * mp1) * kLog2e);
+  o[ML_GFF] = (float)L.gff;
+  o[ML_CHI1] = (float)L.chi1;
+  o[ML_LNNU9] = (float)oco_log(L.nu9);
+  o[ML_HNUK] = (float)L.hnuk;
+  o[ML_L3NU] = (float)L.l3nu;
+  split2(L.wcm1 * kLog2e, o[ML_CH], o[ML_CL]);
+  const double lsw5 = oco_log(L.sw5) * kLog2e;
+  const double fl = floor(lsw5);
+  o[ML_LSI] = (float)fl;
+  o[ML_LSF] = (float)(lsw5 - fl);
+}
+
+/* Wavelength constants held in registers by the solve. */
+struct Lam32 {
+  float cl2, law, g[6], ls, f1, f2, f3, lal0w, gff, chi1, lnnu9, hnuk, l3nu;
+  float ch, cl;   /* log2(e)/lambda_cm = ch + cl */
+  float lsi, lsf; /* log2(2 h c^2 lambda_cm^-5) = lsi + lsf */
+  int n0;
+};
+
+/* Opacity, absorption fraction and source function of one (z, lambda) in log2 form;
+ * log2 S = lSi + lSf with lSi an integer. */
+struct Opac32 {
+  float lk;
+  float l1mw;
+  float lSi, lSf;
+};
+
+/* 308 log2(e) as hi + lo: the reference clamps the Planck exponent x at log_overflow_limit = 308 */
+constexpr float kT2Clamp = (float)(308.0 * kLog2e);
+constexpr float kT2ClampLo = (float)(308.0 * kLog2e - (double)kT2Clamp);
+
+template <class Rec>
+MX_HD Opac32 opacity(const Rec &Z, const Lam32 &L) {
+  const float log2mp1 = 78.9841629f; /* log2(1/mp) */
+  /* stim = 1 - 10^(-chi theta) (c_o :171) */
+  const float t10 = L.cl2 * Z[MZ_TH];
+  const float ls = (t10 > 40.0f) ? 0.0f : log2_one_minus_exp2neg(t10);
+  /* H bound-free (c_o :233-244): log2(AHbf wa^3) + ls + log2 ionf + log2(unsold + sm) */
+  float lsum = kNeg;
+  const int n0 = L.n0;
+  if (n0 <= 6) {
+    float sm = L.g[0];
+#pragma unroll
+    for (int n = 2; n <= 6; n++) sm = (n == n0) ? L.g[n - 1] : sm; /* L.g[n0-1] without local memory */
+    int q = 0;
+    const int off = (n0 == 1) ? 0 : (n0 == 2) ? 5 : (n0 == 3) ? 9 : (n0 == 4) ? 12 : 14;
+#pragma unroll
+    for (int n = 2; n <= 6; n++) {
+      if (n > n0) {
+        sm += L.g[n - 1] * Z[MZ_R + off + q];
+        q++;
+      }
+    }
+    const float le0 = (n0 >= 2) ? Z[MZ_LE2 + n0 - 2] : 0.0f;
+    lsum = le0 + lg2(sm);
+  }
+  const float lbf = lae2(Z[MZ_LU], lsum);
+  const float A = ((L.law + ls) + Z[MZ_LIONF]) + lbf;
+  /* H- bound-free (c_o :318-322) */
+  const float B = (ls + Z[MZ_LHM]) + L.ls;
+  /* H- free-free (c_o :337-339) */
+  const float C = Z[MZ_LAFF] + ((((L.f1 + L.f2 * Z[MZ_LGT]) + L.f3 * Z[MZ_LGT2]) - 26.0f) * kLog2_10_f);
+  const float D = Z[MZ_LESC];
+  const float m = fmaxf_(fmaxf_(A, B), fmaxf_(C, D));
+  const float eA = ex2(A - m), eB = ex2(B - m), eC = ex2(C - m), eD = ex2(D - m);
+  const float lsig = m + lg2((eA + eB) + (eC + eD)); /* log2 of the sum per H */
+  const float labs0 = m + lg2(fmaxf_((eA + eB) + eC, 1e-37f));
+  const float lkr0 = lsig + log2mp1; /* log2 kappa_rad before the free-free part */
+  Opac32 o;
+  float lkr, labs;
+  if (Z[MZ_NEUTRAL] != 0.0f) { /* c_o :262-268 */
+    const float gff = 1.0f + L.gff * (Z[MZ_TH1L] * L.chi1 + 0.5f);
+    const float H = ((ls + Z[MZ_LIONFEF]) + L.lal0w) + lg2(gff); /* log2(kHff * mp1) */
+    o.lk = Z[MZ_LRHO] + lae2(1.0f + lkr0, H);
+    lkr = lae2(lkr0, H);
+    labs = lae2(labs0 + log2mp1, H);
+  } else { /* c_o :270-275, bremsstrahlung :281-300 */
+    const float y = 5.960f - 0.551328895f * (L.lnnu9 + Z[MZ_LNTPOW]); /* sqrt(3)/pi */
+    const float gaunt = kLn2_f * lg2(ex2(y * kLog2e_f) + 2.71828183f);
+    const float xh = L.hnuk * Z[MZ_T1];
+    const float lnq = (Z[MZ_LZ] - L.l3nu) + ((xh > 30.0f) ? 0.0f : kLn2_f * log2_one_minus_exp2neg(xh * kLog2e_f));
+    const float lkb = 28.4599637f + lnq * kLog2e_f + lg2(gaunt); /* log2(369234910.67735046) */
+    o.lk = lae2(lkr0 + Z[MZ_LRHO], lkb);
+    lkr = lae2(1.0f + lkr0, lkb - Z[MZ_LRHO]);
+    labs = lae2(lae2(1.0f + labs0 + log2mp1, Z[MZ_LESC] + log2mp1), lkb - Z[MZ_LRHO]);
+  }
+  float l1 = labs - lkr;
+  if (l1 > 0.0f) l1 = 0.0f;
+  o.l1mw = fmaxf_(l1, -126.0f);
+  /* Planck function (c_o :399-407): S = sw5 / (e^x - 1), x = dft1/lambda_cm clamped at 308.
+   * t2 = x log2(e) = (dft1_hi + dft1_lo)(ch + cl) as hi + lo (FMA two-product). */
+  const float dh = Z[MZ_DFT1], dl = Z[MZ_DFT1L];
+  float p = dh * L.ch;
+  float lo = fmaf(dh, L.ch, -p) + (dh * L.cl + dl * L.ch);
+  if (p > kT2Clamp) {
+    p = kT2Clamp;
+    lo = kT2ClampLo;
+  }
+  const float ti = floorf(p);
+  const float tf = (p - ti) + lo; /* t2 = ti + tf */
+  const float lm = (p > 40.0f) ? 0.0f : log2_one_minus_exp2neg(p);
+  o.lSi = L.lsi - ti;
+  o.lSf = (L.lsf - tf) - lm;
+  return o;
+}
+
+/* ---- extended-exponent non-negative numbers: value = m * 2^e, m FP32, e int -------------- */
+struct XF {
+  float m;
+  int e;
+};
+/* 2^k as a float for -126 <= k <= 127; 0 below. */
+MX_HD float pow2f(int k) {
+  if (k < -126) return 0.0f;
+#ifdef __CUDA_ARCH__
+  return __int_as_float((k + 127) << 23);
+#else
+  union {
+    int i;
+    float f;
+  } u;
+  u.i = (k + 127) << 23;
+  return u.f;
+#endif
+}
+MX_HD int float_exponent(float m) {
+#ifdef __CUDA_ARCH__
+  return ((__float_as_int(m) >> 23) & 0xff) - 127;
+#else
+  union {
+    int i;
+    float f;
+  } u;
+  u.f = m;
+  return ((u.i >> 23) & 0xff) - 127;
+#endif
+}
+/* renormalise so that m is in [1, 2) (m = 0 keeps e) */
+MX_HD XF xnorm(float m, int e) {
+  XF r;
+  if (m == 0.0f) {
+    r.m = 0.0f;
+    r.e = e;
+    return r;
+  }
+  const int k = float_exponent(m);
+  r.m = m * pow2f(-k);
+  r.e = e + k;
+  return r;
+}
+/* 2^(I + F) for an integer-valued float I and a small float F */
+MX_HD XF xexp2(float I, float F) {
+  XF r;
+  const float fl = floorf(F);
+  r.e = (int)(I + fl);
+  r.m = ex2(F - fl);
+  return r;
+}
+/* x*s + y*t for non-negative x, y and FP32 factors s, t >= 0 */
+MX_HD XF xaxpy(XF x, float s, XF y, float t) {
+  const int e = x.e > y.e ? x.e : y.e;
+  const float m = x.m * s * pow2f(x.e - e) + y.m * t * pow2f(y.e - e);
+  return xnorm(m, e);
+}
+MX_HD double xtod(XF x) {
+  if (x.m == 0.0f || x.e < -1000) return 0.0;
+  return (double)x.m * oco_u2d((uint64_t)(int64_t)(x.e + 1023) << 52);
+}
+
+/* ---- scaled tridiagonal rows (auxiliary.f90:125-201 divided by kappa_i^2) ------------- */
+struct Row32 {
+  float a, c, e;  /* sub, super, diagonal excess -(a+b+c) */
+  float ldi, ldf; /* log2 of -d (right-hand side) = ldi + ldf, ldi an integer */
+};
+/* 2^L for log2 values clamped to the FP32 normal range, split exactly into 2^int * ex2(frac) */
+MX_HD float exp2_split(float L) {
+  L = L < -126.0f ? -126.0f : (L > 127.0f ? 127.0f : L);
+  const float fl = floorf(L);
+  return ex2(L - fl) * pow2f((int)fl);
+}
+MX_HD float kappa_lin(float lk) { return exp2_split(lk); }
+/* log2 d = le + log2 S with le split exactly as floor + fraction */
+MX_HD void row_rhs(Row32 &r, float le, const Opac32 &o) {
+  const float fi = floorf(le);
+  r.ldi = fi + o.lSi;
+  r.ldf = (le - fi) + o.lSf;
+}
+/* centre row: a' = 1/kappa_{i-1/2}, c' = 1/kappa_{i+1/2}, e' = dz^2 kappa (1-omega), d' = -S e' */
+MX_HD Row32 row_center(float km, float kj, float kp, const Opac32 &o, float ldz2) {
+  Row32 r;
+  r.a = 2.0f * rcp(kj + km);
+  r.c = 2.0f * rcp(kp + kj);
+  const float le = (ldz2 + o.lk) + o.l1mw;
+  r.e = exp2_split(le);
+  row_rhs(r, le, o);
+  return r;
+}
+/* boundary rows: zeta = kappa dz^2 (1-omega)/4; excess dz + zeta; d' = -S zeta;
+ * bottom: a' = 0, c' = 1/kappa; top: a' = 1/kappa, c' = 0 */
+MX_HD Row32 row_boundary(float kj, const Opac32 &o, float dz, float ldz2, bool top) {
+  Row32 r;
+  const float lz = ((ldz2 + o.lk) + o.l1mw) - 2.0f;
+  r.a = top ? rcp(kj) : 0.0f;
+  r.c = top ? 0.0f : rcp(kj);
+  r.e = dz + exp2_split(lz);
+  row_rhs(r, lz, o);
+  return r;
+}
+
+/* 6th-order flux at interior index m (auxiliary.f90:64-109) from the differences
+ * Dl[k] = f_k - f_{k+1} of the ghosted array (ghost differences mirror the interior ones). */
+MX_HD double flux_from_diffs(const double *Dl, int m, double o1, double dz1) {
+  const double s1 = Dl[m - 1] + Dl[m];
+  const double s2 = (s1 + Dl[m - 2]) + Dl[m + 1];
+  const double s3 = (s2 + Dl[m - 3]) + Dl[m + 2];
+  const double df = -((1.0 / 60.0) * (((45.0 * s1) - 9.0 * s2) + s3));
+  return ((-o1) * df) * dz1;
+}
+
+/* Reference implementation of the mixed solve for one (column, wavelength) item on the host
+ * (accuracy studies; the CUDA kernel streams the same arithmetic).  Zat(z): record of z;
+ * work: 6*nz floats; dwork: nz+6 doubles.  Outputs U[nz+6], K[nz], V[nz] in FP64. */
+template <class ZAt>
+MX_HD void solve_item_host(ZAt Zat, const Lam32 &L, int nz, double dz, float *work, double *dwork, double *U,
+                           double *K, double *V) {
+  const float dzf = (float)dz, ldz2 = (float)(2.0 * oco_log(dz) * kLog2e);
+  float *g = work, *um = work + nz, *o1 = work + 2 * nz, *kap = work + 3 * nz, *qv = work + 5 * nz;
+  int *ue = (int *)(work + 4 * nz);
+  Opac32 cur = opacity(Zat(0), L), nxt = opacity(Zat(1), L);
+  float kc = kappa_lin(cur.lk), kn = kappa_lin(nxt.lk), kprev = 0.0f;
+  Row32 r = row_boundary(kc, cur, dzf, ldz2, false);
+  float h = r.e, cprev = r.c;
+  XF u = xexp2(r.ldi, r.ldf);
+  u.m *= rcp(r.c + h);
+  u = xnorm(u.m, u.e);
+  um[0] = u.m;
+  ue[0] = u.e;
+  o1[0] = rcp(kc);
+  kap[0] = kc;
+  for (int j = 1; j < nz; j++) {
+    kprev = kc;
+    cur = nxt;
+    kc = kn;
+    if (j < nz - 1) {
+      nxt = opacity(Zat(j + 1), L);
+      kn = kappa_lin(nxt.lk);
+      r = row_center(kprev, kc, kn, cur, ldz2);
+    } else {
+      r = row_boundary(kc, cur, dzf, ldz2, true);
+    }
+    const float rr = rcp(cprev + h);
+    g[j] = cprev * rr;  /* |gamma_j| = c_{j-1}/(c_{j-1}+h_{j-1}) */
+    qv[j - 1] = h * rr; /* q_{j-1} = h_{j-1}/(c_{j-1}+h_{j-1}) */
+    h = r.e + (r.a * rr) * h; /* a'/(c'+h) is O(1); a' h alone can overflow */
+    const float rb = rcp(r.c + h); /* 1/|bet_j| */
+    u = xaxpy(xexp2(r.ldi, r.ldf), rb, u, r.a * rb); /* u_j = (|d_j| + a_j u_{j-1}) / |bet_j| */
+    um[j] = u.m;
+    ue[j] = u.e;
+    o1[j] = rcp(kc);
+    kap[j] = kc;
+    cprev = r.c;
+  }
+  /* back-substitution: U_j = u_j + |gamma_{j+1}| U_{j+1} (all terms >= 0) and the differences
+   * D_j = U_j - U_{j+1} = u_j - q_j U_{j+1}, in extended FP32; flux in FP64 from the D_j */
+  XF Un = u;
+  const int n1 = 3, n2 = nz + 2;
+  double *Dl = dwork;
+  U[n1 + nz - 1] = xtod(Un);
+  for (int j = nz - 2; j >= 0; j--) {
+    XF uj;
+    uj.m = um[j];
+    uj.e = ue[j];
+    XF Dj = xaxpy(uj, 1.0f, Un, -qv[j]);
+    Un = xaxpy(uj, 1.0f, Un, g[j + 1]);
+    U[n1 + j] = xtod(Un);
+    Dl[n1 + j] = xtod(Dj);
+  }
+  for (int i = 1; i <= 3; i++) {
+    U[n1 - i] = 2.0 * U[n1] - U[n1 + i];
+    U[n2 + i] = 2.0 * U[n2] - U[n2 - i];
+    Dl[n2 + i - 1] = Dl[n2 - i];
+    Dl[n1 - i] = Dl[n1 + i - 1];
+  }
+  const double dz1 = 1.0 / dz;
+  for (int j = 0; j < nz; j++) {
+    V[j] = flux_from_diffs(Dl, n1 + j, (double)o1[j], dz1);
+    K[j] = (double)kap[j];
+  }
+}
+
+}  // namespace mx
+}  // namespace oco
+
+#endif

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/oco.h"
+#include "mixed_core.h"
 #include "ocomath.h"
 #include "oco_consts.h"
 #include "oco_internal.h"
@@ -63,10 +64,10 @@ struct oco_ctx {
   cudaStream_t stream = nullptr; /* kernels */
   cudaStream_t copy = nullptr;   /* host<->device copies of the host-array path */
   std::string err;
-  /* wavelength tables */
+  /* wavelength tables (FP64 and the mixed form's FP32 log table) */
   int nw = 0;
   std::vector<double> wa;
-  DevBuf lam;
+  DevBuf lam, lam32;
   /* workspace */
   DevBuf pil, scratch, work, status;
   Stage stage[2];
@@ -155,6 +156,7 @@ extern "C" void oco_destroy(oco_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->copy) cudaStreamSynchronize(c->copy);
   c->lam.release();
+  c->lam32.release();
   c->pil.release();
   c->scratch.release();
   c->work.release();
@@ -259,6 +261,31 @@ void oco::fill_lambda_table(const double *waves, int nw, double *tab) {
   }
 }
 
+void oco::fill_mixed_lambda_table(const double *tab, int nw, float *tab32) {
+  for (int iw = 0; iw < nw; iw++) {
+    auto T = [&](int f) { return tab[(size_t)f * nw + iw]; };
+    mx::LamIn li;
+    li.chi = T(L_CHI);
+    li.gff = T(L_GFF);
+    li.chi1 = T(L_CHI1);
+    li.wa3 = T(L_WA3);
+    li.s = T(L_SCOEF);
+    li.hmon = T(L_HMON);
+    li.f1 = T(L_F1);
+    li.f2 = T(L_F2);
+    li.f3 = T(L_F3);
+    for (int q = 0; q < 6; q++) li.gn[q] = T(L_GN1 + q);
+    li.nu9 = T(L_NU9);
+    li.l3nu = T(L_L3NU);
+    li.hnuk = T(L_HNUK);
+    li.wcm1 = T(L_WCM1);
+    li.sw5 = T(L_SW5);
+    float rec[mx::MLN];
+    mx::lambda_record(li, rec);
+    for (int f = 0; f < mx::MLN; f++) tab32[(size_t)f * nw + iw] = rec[f];
+  }
+}
+
 extern "C" int oco_set_wavelengths(oco_ctx *c, const double *wa, int32_t nw) {
   if (!c) return set_err(nullptr, OCO_EINVAL, "oco_set_wavelengths: NULL context");
   if (!wa || nw < 1) return set_err(c, OCO_EINVAL, "oco_set_wavelengths: nw < 1 or NULL wa");
@@ -269,8 +296,12 @@ extern "C" int oco_set_wavelengths(oco_ctx *c, const double *wa, int32_t nw) {
   std::vector<double> tab((size_t)NL * nw, 0.0);
   fill_lambda_table(wa, nw, tab.data());
   CU(cudaStreamSynchronize(c->stream));
+  std::vector<float> tab32((size_t)mx::MLN * nw);
+  fill_mixed_lambda_table(tab.data(), nw, tab32.data());
   CU(c->lam.ensure(tab.size() * sizeof(double)));
   CU(cudaMemcpy(c->lam.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CU(c->lam32.ensure(tab32.size() * sizeof(float)));
+  CU(cudaMemcpy(c->lam32.p, tab32.data(), tab32.size() * sizeof(float), cudaMemcpyHostToDevice));
   c->wa.assign(wa, wa + nw);
   c->nw = nw;
   return OCO_OK;
@@ -296,21 +327,29 @@ static int check_params(oco_ctx *c, const oco_params *p) {
 
 static const int kSolveThreads = 128;
 
-/* Grid of the persistent solve kernel and its scratch (gamma, u, 1/kappa per z). */
+/* Grid of the persistent solve kernel and its scratch: per resident thread and z, FP64
+ * gamma, u, 1/kappa, q (32 B) or, for the mixed form, one float4 (16 B). */
 static int prepare_solve(oco_ctx *c, int form, int grey, int64_t nitems, int nz, int *blocks) {
-  int bps = solve_fp64_max_blocks_per_sm(form == OCO_FORM_STABLE ? 1 : 0, grey, kSolveThreads);
+  const bool mixed = form == OCO_FORM_MIXED;
+  int bps = mixed ? solve_mixed_max_blocks_per_sm(kSolveThreads)
+                  : solve_fp64_max_blocks_per_sm(form == OCO_FORM_STABLE ? 1 : 0, grey, kSolveThreads);
   int64_t maxb = (int64_t)bps * c->num_sms;
   int64_t need = (nitems + kSolveThreads - 1) / kSolveThreads;
   *blocks = (int)std::max<int64_t>(1, std::min(maxb, need));
   size_t slots = (size_t)(*blocks) * kSolveThreads;
-  CU(c->scratch.ensure(slots * (size_t)nz * 3 * sizeof(double)));
+  CU(c->scratch.ensure(slots * (size_t)nz * (mixed ? 16 : 4 * sizeof(double))));
   return OCO_OK;
+}
+
+/* Bytes of the per-(column, z) record of a form: the FP64 pillar or the mixed record. */
+static size_t record_bytes(int form) {
+  return form == OCO_FORM_MIXED ? MIXED_ZN * sizeof(float) : NF * sizeof(double);
 }
 
 /* Columns per chunk so that pillars (+ staged outputs on the host path) fit the budget. */
 static int64_t chunk_columns(oco_ctx *c, const oco_params *p, bool host_path) {
   const int64_t ncol = (int64_t)p->nx * p->ny;
-  size_t per_col = (size_t)p->nz * NF * sizeof(double);
+  size_t per_col = (size_t)p->nz * record_bytes(p->form);
   if (host_path)
     per_col += 2 * ((size_t)p->nz * 2 + (size_t)p->nw * ((p->nz + 6) + 2 * (size_t)p->nz + 2)) * sizeof(double);
   int64_t ch = (int64_t)std::max<size_t>(1, c->budget_bytes / per_col);
@@ -318,8 +357,57 @@ static int64_t chunk_columns(oco_ctx *c, const oco_params *p, bool host_path) {
 }
 
 /* One chunk: pillars + persistent solve. Outputs described by the strides in a. */
+static int run_chunk_mixed(oco_ctx *c, const oco_params *p, const double *rho, const double *T, int64_t nb,
+                           const SolveArgs &a64, cudaStream_t s) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
+  if (c->prof) {
+    e0 = c->take_event();
+    e1 = c->take_event();
+    e2 = c->take_event();
+    e3 = c->take_event();
+    CU(cudaEventRecord(e0, s));
+  }
+  float *rec = c->pil.as<float>();
+  CU(launch_pillars_mixed(rho, T, nb, p->nz, p->fully_ionized_T, rec, s));
+  if (c->prof) {
+    CU(cudaEventRecord(e1, s));
+    c->ev_pil.emplace_back(e0, e1);
+  }
+  int blocks = 0;
+  int rc = prepare_solve(c, OCO_FORM_MIXED, 0, nb * p->nw, p->nz, &blocks);
+  if (rc) return rc;
+  const size_t slots = (size_t)blocks * kSolveThreads;
+  MixedArgs a{};
+  a.rec = rec;
+  a.lam = c->lam32.as<float>();
+  a.ncol = nb;
+  a.nz = p->nz;
+  a.nw = p->nw;
+  a.dz = p->dz;
+  a.ldz2 = (float)(2.0 * std::log2(p->dz));
+  a.U = a64.U, a.U_zs = a64.U_zs, a.U_is = a64.U_is;
+  a.K = a64.K, a.K_zs = a64.K_zs, a.K_is = a64.K_is;
+  a.V = a64.V, a.V_zs = a64.V_zs, a.V_is = a64.V_is;
+  a.Vtop = a64.Vtop, a.Vbot = a64.Vbot;
+  a.ld_col = a64.ld_col, a.c_off = a64.c_off, a.layout = a64.layout;
+  a.s4 = c->scratch.as<float4>();
+  a.slot_stride = (int64_t)slots;
+  a.work = c->work.as<unsigned long long>();
+  a.status = c->status.as<unsigned long long>();
+  CU(cudaMemsetAsync(a.work, 0, sizeof(unsigned long long), s));
+  if (c->prof) CU(cudaEventRecord(e2, s));
+  CU(launch_solve_mixed(a, blocks, kSolveThreads, s));
+  if (c->prof) {
+    CU(cudaEventRecord(e3, s));
+    c->ev_solve.emplace_back(e2, e3);
+  }
+  c->launches += 2;
+  return OCO_OK;
+}
+
 static int run_chunk(oco_ctx *c, const oco_params *p, const double *rho, const double *T, int64_t nb,
                      SolveArgs a, cudaStream_t s) {
+  if (p->form == OCO_FORM_MIXED) return run_chunk_mixed(c, p, rho, T, nb, a, s);
   const int grey = p->lgrey ? 1 : 0;
   cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
   if (c->prof) {
@@ -344,6 +432,7 @@ static int run_chunk(oco_ctx *c, const oco_params *p, const double *rho, const d
   a.gam = c->scratch.as<double>();
   a.uu = a.gam + slots * p->nz;
   a.o1 = a.uu + slots * p->nz;
+  a.q = a.o1 + slots * p->nz;
   a.slot_stride = (int64_t)slots;
   a.work = c->work.as<unsigned long long>();
   a.status = c->status.as<unsigned long long>();
@@ -411,13 +500,13 @@ extern "C" int oco_solve_block_device(oco_ctx *c, const oco_params *p, const dou
                                       void *stream) {
   int rc = check_params(c, p);
   if (rc) return rc;
-  if (p->form == OCO_FORM_MIXED) return set_err(c, OCO_EINVAL, "mixed form not available in this build");
+  if (p->form == OCO_FORM_MIXED && p->lgrey) return set_err(c, OCO_EINVAL, "the mixed form has no grey variant");
   if (!rho || !T || !U) return set_err(c, OCO_EINVAL, "rho, T and U are required");
   CU(cudaSetDevice(c->device));
   cudaStream_t s = (cudaStream_t)stream; /* NULL is the CUDA default stream */
   const int64_t ncol = (int64_t)p->nx * p->ny;
   const int64_t ch = chunk_columns(c, p, false);
-  CU(c->pil.ensure((size_t)ch * p->nz * NF * sizeof(double)));
+  CU(c->pil.ensure((size_t)ch * p->nz * record_bytes(p->form)));
   if ((rc = reset_status(c, s))) return rc;
   SolveArgs a{};
   fill_strides(a, p, p->layout, ncol);
@@ -447,13 +536,13 @@ extern "C" int oco_solve_block(oco_ctx *c, const oco_params *p, const double *rh
                                double *kappa, double *V, double *Vtop, double *Vbot) {
   int rc = check_params(c, p);
   if (rc) return rc;
-  if (p->form == OCO_FORM_MIXED) return set_err(c, OCO_EINVAL, "mixed form not available in this build");
+  if (p->form == OCO_FORM_MIXED && p->lgrey) return set_err(c, OCO_EINVAL, "the mixed form has no grey variant");
   if (!rho || !T || !U) return set_err(c, OCO_EINVAL, "rho, T and U are required");
   CU(cudaSetDevice(c->device));
   const int64_t ncol = (int64_t)p->nx * p->ny;
   const int nz = p->nz, nw = p->nw, mz = nz + 6;
   const int64_t ch = chunk_columns(c, p, true);
-  CU(c->pil.ensure((size_t)ch * nz * NF * sizeof(double)));
+  CU(c->pil.ensure((size_t)ch * nz * record_bytes(p->form)));
   for (auto &st : c->stage) {
     CU(st.rho.ensure((size_t)ch * nz * sizeof(double)));
     CU(st.T.ensure((size_t)ch * nz * sizeof(double)));

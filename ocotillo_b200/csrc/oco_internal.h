@@ -87,11 +87,35 @@ struct SolveArgs {
   double *Vtop, *Vbot; /* [iw*ld_col + c_off + cl] */
   int64_t ld_col, c_off;
   int layout;
-  /* Scratch [nz][nslot*32]: forward-sweep gamma, u and 1/kappa of each warp slot. */
-  double *gam, *uu, *o1;
+  /* Scratch [nz][nslot*32]: forward-sweep gamma, u, 1/kappa and (stable form) q of each
+   * warp slot. */
+  double *gam, *uu, *o1, *q;
   int64_t slot_stride; /* = nslot*32 */
   unsigned long long *work;   /* persistent-kernel work counter (warp tasks) */
   unsigned long long *status; /* [0] zero-pivot count, [1] first bad item (min), [2] timeout flag */
+};
+
+/* Arguments of the mixed-precision solve kernels. */
+struct MixedArgs {
+  const float *rec; /* [ncol][nz][MIXED_ZN] mixed records of this chunk */
+  const float *lam; /* [MIXED_LN][nw] */
+  int64_t ncol;
+  int nz, nw;
+  double dz;
+  float ldz2; /* log2(dz^2) */
+  double *U;
+  int64_t U_zs, U_is;
+  double *K;
+  int64_t K_zs, K_is;
+  double *V;
+  int64_t V_zs, V_is;
+  double *Vtop, *Vbot;
+  int64_t ld_col, c_off;
+  int layout;
+  float4 *s4; /* scratch [nz][slots]: |gamma| or q, 1/kappa, u mantissa, u exponent */
+  int64_t slot_stride;
+  unsigned long long *work;
+  unsigned long long *status;
 };
 
 /* Fills tab[NL*nw] (layout [field][iw]) with the wavelength table of waves[nw] (Angstrom):
@@ -105,6 +129,16 @@ cudaError_t launch_pillars(const double *rho, const double *T, int64_t ncol, int
 cudaError_t launch_solve_fp64(const SolveArgs &a, int form, int grey, int nslot_blocks,
                               int threads, cudaStream_t s);
 int solve_fp64_max_blocks_per_sm(int form, int grey, int threads);
+
+/* Mixed-precision kernels (kernels_mixed.cu). */
+constexpr int MIXED_ZN = 40; /* floats per mixed record */
+constexpr int MIXED_LN = 24; /* fields of the mixed wavelength table */
+cudaError_t launch_pillars_mixed(const double *rho, const double *T, int64_t ncol, int nz, double fully_ionized_T,
+                                 float *rec, cudaStream_t s);
+cudaError_t launch_solve_mixed(const MixedArgs &a, int blocks, int threads, cudaStream_t s);
+int solve_mixed_max_blocks_per_sm(int threads);
+/* Fills tab32[MIXED_LN*nw] from the FP64 table tab[NL*nw]. */
+void fill_mixed_lambda_table(const double *tab, int nw, float *tab32);
 
 }  // namespace oco
 

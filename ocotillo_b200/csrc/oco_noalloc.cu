@@ -103,7 +103,7 @@ extern "C" int oco_solve_block_noalloc(const oco_params *p, const double *wa_ang
   const size_t avail = OCO_NOALLOC_WORKSPACE_BYTES - 256 - tab_bytes;
   int nsm = 0, bps = solve_fp64_max_blocks_per_sm(p->form == OCO_FORM_STABLE ? 1 : 0, grey, kThreads);
   CUN(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  const size_t per_slot = (size_t)nz * 3 * sizeof(double);
+  const size_t per_slot = (size_t)nz * 4 * sizeof(double);
   const int64_t ncol = (int64_t)p->nx * p->ny;
   const int64_t need_blocks = (ncol * nw + kThreads - 1) / kThreads;
   int64_t blocks = std::min<int64_t>({(int64_t)nsm * bps, need_blocks, (int64_t)(avail / 2 / (per_slot * kThreads))});
@@ -149,6 +149,7 @@ extern "C" int oco_solve_block_noalloc(const oco_params *p, const double *wa_ang
   a.gam = scr;
   a.uu = scr + slots * nz;
   a.o1 = scr + 2 * slots * nz;
+  a.q = scr + 3 * slots * nz;
   a.slot_stride = (int64_t)slots;
   a.work = ctr;
   a.status = ctr + 1;

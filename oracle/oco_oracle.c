@@ -181,6 +181,7 @@ void oracle_calc_wavelength(double w1, double w0, int32_t nw, double *wa) {
 enum {
   P_RHO, P_RHO1, P_T, P_T1, P_X, P_N, P_INVN, P_NHI, P_NHII, P_NE, P_IONF, P_PE, P_ESCAT,
   P_THETA, P_THETA1, P_LGT, P_LGT2, P_HMBF, P_STIM, P_S, P_ALB, P_OP, P_OP1, P_OP2, P_FLUX,
+  P_OMA, /* 1 - albedo from the absorption terms (stable form) */
   P_NFIELDS
 };
 typedef struct {
@@ -277,6 +278,7 @@ static void opacity_and_albedo(opillar *p, const otab *t, int iw, double *kr) {
                    t->f_coeff[iw * 3 + 2] * f[P_LGT2][i]) - 26.0;
     double kHmff = (((f[P_IONF][i] * f[P_NE][i]) * k_cgs) * f[P_T][i]) * MPOW(10.0, flam);
     kr[i] = (((kHbf + kHmbf) + kHmff) + f[P_ESCAT][i]) * mp1; /* :188 */
+    f[P_OMA][i] = ((kHbf + kHmbf) + kHmff) * mp1; /* absorption part of kr, stable form */
     f[P_OP][i] = kr[i] * f[P_RHO][i];                          /* :189 */
   }
   for (int i = 0; i < nz; i++) { /* calc_kappa_H_ff :261-277 */
@@ -285,15 +287,18 @@ static void opacity_and_albedo(opillar *p, const otab *t, int iw, double *kr) {
       double energyfactor = (((0.5 * log10e) * f[P_THETA1][i]) * Iev1) * MPOW(10.0, -(f[P_THETA][i] * Iev));
       double kHff = ((((f[P_STIM][i] * f[P_IONF][i]) * alpha0) * wa3) * g_ff) * energyfactor;
       kr[i] = kr[i] + kHff * mp1;
+      f[P_OMA][i] = f[P_OMA][i] + kHff * mp1;
       f[P_OP][i] = f[P_OP][i] + kr[i] * f[P_RHO][i];
     } else {
       double ob = bremsstrahlung(p, i, t->nu[iw]);
       f[P_OP][i] = f[P_OP][i] + ob;
       kr[i] = kr[i] + f[P_OP][i] * f[P_RHO1][i];
+      f[P_OMA][i] = f[P_OMA][i] + f[P_OP][i] * f[P_RHO1][i];
     }
   }
   for (int i = 0; i < nz; i++) {
     f[P_ALB][i] = (f[P_ESCAT][i] * mp1) / kr[i]; /* :195 */
+    f[P_OMA][i] = f[P_OMA][i] / kr[i];             /* = 1 - albedo without cancellation */
     f[P_OP1][i] = 1.0 / f[P_OP][i];              /* :196 */
     f[P_OP2][i] = f[P_OP][i] * f[P_OP][i];       /* :197 */
   }
@@ -313,6 +318,7 @@ static void grey_parameters(opillar *p, double sigma_grey) {
     double alpha_grey = (3.68e22 * MPOW(T, -3.5)) * f[P_RHO][i];
     f[P_OP][i] = (alpha_grey + sigma_grey) * f[P_RHO][i];
     f[P_ALB][i] = sigma_grey / (alpha_grey + sigma_grey);
+    f[P_OMA][i] = alpha_grey / (alpha_grey + sigma_grey);
     f[P_OP1][i] = 1.0 / f[P_OP][i];
     f[P_OP2][i] = f[P_OP][i] * f[P_OP][i];
   }
@@ -322,7 +328,7 @@ static void grey_parameters(opillar *p, double sigma_grey) {
  * auxiliary.f90:111-201.  ex receives the diagonal excess -(a+b+c) computed directly
  * (used only by the stable form). */
 static void tridag_coefficients(double *aa, double *bb, double *cc, double *dd, double *ex,
-                                const opillar *p, double dz, double dz2, double *kp) {
+                                const opillar *p, double dz, double dz2, double *kp, int stable) {
   const int nz = p->nz;
   double *const *f = p->f;
   for (int iz = 0; iz < nz - 1; iz++) kp[iz] = 0.5 * (f[P_OP][iz + 1] + f[P_OP][iz]); /* :147-149 */
@@ -330,20 +336,21 @@ static void tridag_coefficients(double *aa, double *bb, double *cc, double *dd, 
     double op = f[P_OP][iz];
     aa[iz] = f[P_OP2][iz] / kp[iz - 1];
     cc[iz] = f[P_OP2][iz] / kp[iz];
-    double zeta = (dz2 * (op * (op * op))) * (1.0 - f[P_ALB][iz]);
+    double oma = stable ? f[P_OMA][iz] : (1.0 - f[P_ALB][iz]);
+    double zeta = (dz2 * (op * (op * op))) * oma;
     bb[iz] = -((aa[iz] + cc[iz]) + zeta);
     dd[iz] = -(f[P_S][iz] * zeta);
     ex[iz] = zeta;
   }
   /* :187-197 */
-  double zeta = ((f[P_OP][0] * dz2) * (1.0 - f[P_ALB][0])) * 0.25;
+  double zeta = ((f[P_OP][0] * dz2) * (stable ? f[P_OMA][0] : (1.0 - f[P_ALB][0]))) * 0.25;
   aa[0] = 0.0;
   bb[0] = -(((f[P_OP1][0] + dz) + zeta) * f[P_OP2][0]);
   cc[0] = f[P_OP][0];
   dd[0] = -((f[P_S][0] * zeta) * f[P_OP2][0]);
   ex[0] = (dz + zeta) * f[P_OP2][0];
   int n = nz - 1;
-  zeta = ((f[P_OP][n] * dz2) * (1.0 - f[P_ALB][n])) * 0.25;
+  zeta = ((f[P_OP][n] * dz2) * (stable ? f[P_OMA][n] : (1.0 - f[P_ALB][n]))) * 0.25;
   aa[n] = f[P_OP][n];
   bb[n] = -(((f[P_OP1][n] + dz) + zeta) * f[P_OP2][n]);
   cc[n] = 0.0;
@@ -370,9 +377,12 @@ static int tridag(const double *a, const double *b, const double *c, const doubl
 }
 
 /* Same system, difference-form pivots: bet_j = -(c_j + h_j) with
- * h_j = e_j + a_j h_{j-1} / (c_{j-1} + h_{j-1}), all terms non-negative. */
+ * h_j = e_j + a_j h_{j-1} / (c_{j-1} + h_{j-1}), all terms non-negative.  The back-substitution
+ * also returns the differences D_j = U_j - U_{j+1} = u_j - q_j U_{j+1}, q_j = h_j/(c_j + h_j):
+ * in optically thin layers |gamma| = 1 - q rounds to 1 and U_j - U_{j+1} is below the
+ * resolution of U itself, while u_j and q_j U_{j+1} are of the size of the difference. */
 static int tridag_stable(const double *a, const double *c, const double *r, const double *e,
-                         double *u, int n, double *gam) {
+                         double *u, int n, double *gam, double *q, double *D) {
   int bad = 0;
   double h = e[0];
   double bet = -(c[0] + h);
@@ -381,13 +391,41 @@ static int tridag_stable(const double *a, const double *c, const double *r, cons
   for (int j = 1; j < n; j++) {
     double den = c[j - 1] + h;
     gam[j] = -(c[j - 1] / den);
+    q[j - 1] = h / den;
     h = e[j] + (a[j] * h) / den;
     bet = -(c[j] + h);
     if (bet == 0.0) bad = -1;
     u[j] = (r[j] - a[j] * u[j - 1]) / bet;
   }
-  for (int j = n - 2; j >= 0; j--) u[j] = u[j] - gam[j + 1] * u[j + 1];
+  for (int j = n - 2; j >= 0; j--) {
+    double uf = u[j];
+    u[j] = uf - gam[j + 1] * u[j + 1];
+    D[j] = uf - q[j] * u[j + 1];
+  }
   return bad;
+}
+
+/* 6th-order flux (auxiliary.f90:64-109, ghosts :49-62) written in the differences
+ * Delta_m = f_m - f_{m+1}: f_{m+k} - f_{m-k} = -(Delta_{m-k} + ... + Delta_{m+k-1}), and the
+ * ghost zones mirror the differences next to each boundary.  Same value as the stencil on
+ * f in exact arithmetic; used by the stable form (nz >= 4), whose D_j are accurate where
+ * the differences of U are not resolved. */
+static void calc_flux_diff(const double *D, opillar *p, double dz1, double *Dl) {
+  const int nz = p->nz, n1 = 3;
+  double **pf = p->f;
+  for (int m = n1; m <= nz + 1; m++) Dl[m] = D[m - n1];
+  for (int i = 1; i <= 3; i++) {
+    Dl[nz + 2 + i - 1] = Dl[nz + 2 - i];
+    Dl[n1 - i] = Dl[n1 + i - 1];
+  }
+  for (int j = 0; j < nz; j++) {
+    int m = n1 + j;
+    double s1 = Dl[m - 1] + Dl[m];
+    double s2 = (s1 + Dl[m - 2]) + Dl[m + 1];
+    double s3 = (s2 + Dl[m - 3]) + Dl[m + 2];
+    double df = -((1.0 / 60.0) * (((45.0 * s1) - 9.0 * s2) + s3));
+    pf[P_FLUX][j] = ((-1.0 * pf[P_OP1][j]) * df) * dz1;
+  }
 }
 
 /* update_ghosts, auxiliary.f90:49-62 (f has nz+6 entries, n1 = 3, n2 = nz+2 0-based) */
@@ -431,7 +469,7 @@ int oracle_solve_columns(const oracle_params *prm, const double *wa, const doubl
     otab_free(&t);
     return ORACLE_ENOMEM;
   }
-  double *work = (double *)calloc((size_t)nz * 8 + mz, sizeof(double));
+  double *work = (double *)calloc((size_t)nz * 10 + 2 * mz, sizeof(double));
   if (!work) {
     free(p.mem);
     otab_free(&t);
@@ -439,6 +477,7 @@ int oracle_solve_columns(const oracle_params *prm, const double *wa, const doubl
   }
   double *a = work, *b = work + nz, *c = work + 2 * nz, *d = work + 3 * nz, *ex = work + 4 * nz;
   double *kr = work + 5 * nz, *gam = work + 6 * nz, *kp = work + 7 * nz, *u = work + 8 * nz;
+  double *qv = work + 8 * nz + mz, *Dv = work + 9 * nz + mz, *Dl = work + 10 * nz + mz;
   const double dz = prm->dz, dz1 = 1.0 / prm->dz, dz2 = prm->dz * prm->dz;
   for (int64_t col = col0; col < col1; col++) {
     memcpy(p.f[P_RHO], rho + col * nz, (size_t)nz * sizeof(double));
@@ -449,15 +488,18 @@ int oracle_solve_columns(const oracle_params *prm, const double *wa, const doubl
         grey_parameters(&p, prm->sigma_grey);
       else
         opacity_and_albedo(&p, &t, iw, kr);
-      tridag_coefficients(a, b, c, d, ex, &p, dz, dz2, kp);
-      int bad = (prm->form == ORACLE_FORM_STABLE) ? tridag_stable(a, c, d, ex, u + 3, nz, gam)
-                                                   : tridag(a, b, c, d, u + 3, nz, gam);
+      tridag_coefficients(a, b, c, d, ex, &p, dz, dz2, kp, prm->form == ORACLE_FORM_STABLE);
+      const int stable = prm->form == ORACLE_FORM_STABLE;
+      int bad = stable ? tridag_stable(a, c, d, ex, u + 3, nz, gam, qv, Dv) : tridag(a, b, c, d, u + 3, nz, gam);
       if (bad && rc == ORACLE_OK) {
         rc = ORACLE_EZEROPIVOT;
         if (bad_item) *bad_item = col * nw + iw;
       }
       update_ghosts(u, nz);
-      calc_flux(u, &p, dz1);
+      if (stable && nz >= 4)
+        calc_flux_diff(Dv, &p, dz1, Dl);
+      else
+        calc_flux(u, &p, dz1);
       size_t item = (size_t)iw * (size_t)ncol + (size_t)col;
       if (U) memcpy(U + item * mz, u, (size_t)mz * sizeof(double));
       if (kappa) memcpy(kappa + item * nz, p.f[P_OP], (size_t)nz * sizeof(double));

@@ -31,7 +31,8 @@ extern "C" {
 
 /* Solver forms. */
 #define ORACLE_FORM_REFERENCE 0 /* the reference's Thomas recursion, auxiliary.f90:14-47 */
-#define ORACLE_FORM_STABLE 1    /* difference-form pivots (no cancellation), same system */
+#define ORACLE_FORM_STABLE 1    /* same system: difference-form pivots, 1 - albedo from the absorption
+                                 * terms, flux from the differences of U (no cancellation) */
 
 /* Error codes (same values as the product's include/oco.h). */
 #define ORACLE_OK 0
