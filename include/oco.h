@@ -155,6 +155,89 @@ int oco_solve_block_noalloc(const oco_params *p, const double *wa_angstrom, cons
                             double *Vbot, void *stream);
 const char *oco_noalloc_last_error(void);
 
+/* ---- Ragged batches ---------------------------------------------------------------------
+ * No counterpart in the reference, whose loop runs one block with one nz and one wavelength
+ * grid: a batch is a set of independent columns, each with its own nz, dz and wavelength
+ * grid (for instance columns of several snapshots), solved by one persistent launch fed from
+ * a device work queue and replayed as a CUDA graph.  Mixed form only.  Per column the
+ * arithmetic is that of oco_solve_block_device with p->form = OCO_FORM_MIXED.
+ *
+ * Array layout (device arrays, element offsets given per column):
+ *   rho, T      nz values from in_off (z fastest), read-only
+ *   U           from u_off: (nz+6) x nw values, [lambda][z] (z fastest) for
+ *               OCO_LAYOUT_REFERENCE, [z][lambda] for OCO_LAYOUT_LAMBDA_FASTEST
+ *   kappa, V    from kv_off: nz x nw values, same order as U
+ *   Vtop, Vbot  from flux_off: nw values (V at z index nz and 1)
+ * Output ranges of different columns must not overlap. */
+typedef struct oco_batch oco_batch;
+
+typedef struct oco_batch_column {
+  int64_t in_off;   /* first element (z = 1) of the column's rho and T profiles */
+  int64_t u_off;    /* first element of the column's U block */
+  int64_t kv_off;   /* first element of the column's kappa and V blocks */
+  int64_t flux_off; /* first element of the column's Vtop and Vbot entries */
+  int64_t wave_off; /* first wavelength (Angstrom) of the column's grid in `waves` */
+  int32_t nz;       /* >= 2 */
+  int32_t nw;       /* >= 1 */
+  double dz;        /* grid spacing, cm */
+} oco_batch_column;
+
+/* Tilings (oco_batch_info.tiling). */
+#define OCO_TILING_WARP_COLUMN 0 /* a warp solves 32 wavelengths of one column */
+#define OCO_TILING_PACKED 1      /* a warp solves 32 consecutive items of the nz-sorted item list */
+
+typedef struct oco_batch_info {
+  int64_t ncol;          /* columns */
+  int64_t npoints;       /* sum of nz * nw */
+  int32_t max_nz, max_nw;
+  int32_t tiling;        /* OCO_TILING_* in use */
+  int32_t blocks_per_sm; /* resident 128-thread blocks per SM of the persistent launch */
+  int32_t tuned;         /* 1 after oco_batch_tune */
+  int32_t ncandidates;   /* tilings timed by oco_batch_tune */
+  int32_t cand_tiling[16];
+  int32_t cand_blocks_per_sm[16];
+  double cand_ms[16];    /* one timed run of each candidate */
+  int64_t graph_launches; /* oco_batch_run calls so far */
+} oco_batch_info;
+
+/* Describes a batch of ncol columns on the context's device: validates the descriptors,
+ * builds one wavelength table per distinct (wave_off, nw) grid from waves[nwaves] (Angstrom,
+ * host memory), sorts the work longest column first and reserves the device workspace.
+ * form must be OCO_FORM_MIXED; layout is OCO_LAYOUT_*. */
+int oco_batch_create(oco_ctx *ctx, const oco_batch_column *cols, int64_t ncol, const double *waves,
+                     int64_t nwaves, int32_t form, int32_t layout, double fully_ionized_T,
+                     oco_batch **batch);
+
+/* Binds the device arrays (element counts for the bounds check of every column's ranges)
+ * and captures the batch's launches into a CUDA graph.  kappa, V, Vtop, Vbot may be NULL
+ * (then their count is ignored).  Rebinding recaptures. */
+int oco_batch_bind(oco_batch *batch, const double *rho, const double *T, int64_t n_in, double *U,
+                   int64_t n_u, double *kappa, double *V, int64_t n_kv, double *Vtop, double *Vbot,
+                   int64_t n_flux);
+
+/* Autotuner: runs the bound batch once per candidate tiling (tiling x resident blocks per
+ * SM), keeps the fastest and recaptures the graph with it.  Writes the outputs as a run
+ * does.  Synchronous. */
+int oco_batch_tune(oco_batch *batch);
+
+/* Sets the tiling by hand (instead of oco_batch_tune): tiling OCO_TILING_*, blocks_per_sm
+ * from 1 to the kernel's occupancy limit (0 = that limit).  Recaptures the graph if bound. */
+int oco_batch_set_tiling(oco_batch *batch, int32_t tiling, int32_t blocks_per_sm);
+
+/* Replays the batch's graph on `stream` (a cudaStream_t; NULL is the CUDA default stream):
+ * records, then every (column, wavelength) item.  Returns after enqueueing; the bound inputs
+ * must stay valid and the outputs untouched until the stream reaches this work. */
+int oco_batch_run(oco_batch *batch, void *stream);
+
+/* Waits for the last oco_batch_run; returns OCO_ETIMEDOUT if a bounded wait in the kernel
+ * ran out (its results are then incomplete). */
+int oco_batch_wait(oco_batch *batch);
+
+int oco_batch_get_info(const oco_batch *batch, oco_batch_info *info);
+
+/* Releases the batch (waits for its work first). */
+void oco_batch_destroy(oco_batch *batch);
+
 #ifdef __cplusplus
 }
 #endif

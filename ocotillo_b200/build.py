@@ -30,11 +30,12 @@ UNITS = [
     ("kernels_mixed_pillars.cu", ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
     ("oco_api.cu", []),
     ("oco_noalloc.cu", []),
+    ("oco_batch.cu", []),
     ("oco_server.cu", []),
 ]
 HOST_UNITS = [("oco_deck.cpp", [])]
 
-HEADERS = ["ocomath.h", "ocomath_tables.h", "oco_consts.h", "oco_internal.h"]
+HEADERS = ["ocomath.h", "ocomath_tables.h", "oco_consts.h", "oco_internal.h", "oco_ctx.h", "mixed_core.h"]
 
 
 def _newer(target, deps):

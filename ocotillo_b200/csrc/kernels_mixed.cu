@@ -134,19 +134,54 @@ __device__ __forceinline__ void load_lam32(Lam32 &L, const float *__restrict__ t
 #undef LF
 }
 
-/* One (column, wavelength) item.  Scratch: one float4 per z (see the forward sweep). */
-template <class PA>
-__device__ __forceinline__ void msolve_item(const MixedArgs &a, int64_t cl, int iw, bool active, PA &pa,
-                                            float4 *__restrict__ s4) {
-  const int nz = a.nz;
-  const int64_t ss = a.slot_stride;
-  Lam32 L;
-  load_lam32(L, a.lam, iw, a.nw);
+/* Everything one (column, wavelength) item needs besides its records. */
+struct MItem {
+  const float *lam; /* wavelength table [MLN][nw] of the item's grid */
+  int nz, nw, iw;
+  float dzf, ldz2;  /* dz and log2(dz^2) */
+  double dz1;       /* 1/dz */
+  double *U;        /* U of z = 0 (ghost zone 0), stride uz; written only when active */
+  double *K, *V;    /* kappa and V of z = 0 or NULL, strides kz, vz */
+  int64_t uz, kz, vz;
+  double *vtop, *vbot; /* emergent-flux destinations or NULL */
+};
+
+/* Item of the block kernels: column cl of the chunk, wavelength iw. */
+__device__ __forceinline__ MItem block_item(const MixedArgs &a, int64_t cl, int iw) {
+  MItem it;
+  it.lam = a.lam;
+  it.nz = a.nz;
+  it.nw = a.nw;
+  it.iw = iw;
+  it.dzf = (float)a.dz;
+  it.ldz2 = a.ldz2;
+  it.dz1 = 1.0 / a.dz;
   const int64_t idx = (a.layout == 0) ? (int64_t)iw * a.ld_col + a.c_off + cl : (a.c_off + cl) * a.nw + iw;
-  double *Ub = a.U + idx * a.U_is;
-  double *Kb = (a.K && active) ? a.K + idx * a.K_is : nullptr;
-  double *Vb = (a.V && active) ? a.V + idx * a.V_is : nullptr;
-  const float dzf = (float)a.dz, ldz2 = a.ldz2;
+  it.U = a.U + idx * a.U_is;
+  it.K = a.K ? a.K + idx * a.K_is : nullptr;
+  it.V = a.V ? a.V + idx * a.V_is : nullptr;
+  it.uz = a.U_zs;
+  it.kz = a.K_zs;
+  it.vz = a.V_zs;
+  const int64_t pidx = (int64_t)iw * a.ld_col + a.c_off + cl;
+  it.vtop = a.Vtop ? a.Vtop + pidx : nullptr;
+  it.vbot = a.Vbot ? a.Vbot + pidx : nullptr;
+  return it;
+}
+
+/* One (column, wavelength) item.  Scratch: one float4 per z at s4[z * ss] (see the forward
+ * sweep).  An inactive lane runs the forward sweep (to keep a staged warp in step) and writes
+ * nothing. */
+template <class PA>
+__device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa, float4 *__restrict__ s4,
+                                            int64_t ss) {
+  const int nz = it.nz;
+  Lam32 L;
+  load_lam32(L, it.lam, it.iw, it.nw);
+  double *Ub = it.U;
+  double *Kb = active ? it.K : nullptr;
+  double *Vb = active ? it.V : nullptr;
+  const float dzf = it.dzf, ldz2 = it.ldz2;
 
   Opac32 cur = opacity(pa.at(0), L);
   Opac32 nxt = opacity(pa.at(1), L);
@@ -180,7 +215,7 @@ __device__ __forceinline__ void msolve_item(const MixedArgs &a, int64_t cl, int 
     const float rb = rcp(r.c + h);
     u = xaxpy(xexp2(r.ldi, r.ldf), rb, u, r.a * rb);
     o1 = rcp(kc);
-    if (Kb) Kb[(int64_t)j * a.K_zs] = (double)kc;
+    if (Kb) Kb[(int64_t)j * it.kz] = (double)kc;
     pend = make_float4(0.0f, o1, u.m, (float)u.e);
     cprev = r.c;
   }
@@ -189,8 +224,8 @@ __device__ __forceinline__ void msolve_item(const MixedArgs &a, int64_t cl, int 
 
   /* reverse sweep */
   const int n = nz;
-  const double dz1 = 1.0 / a.dz;
-  const int64_t uz = a.U_zs;
+  const double dz1 = it.dz1;
+  const int64_t uz = it.uz;
   XF Un = u; /* U_{n-1} */
   Ub[(int64_t)(3 + n - 1) * uz] = xtod(Un);
   double vtop = 0.0, vbot = 0.0;
@@ -232,7 +267,7 @@ __device__ __forceinline__ void msolve_item(const MixedArgs &a, int64_t cl, int 
       const double s3 = (s2 + d0) + d5;
       const double df = -((1.0 / 60.0) * (((45.0 * s1) - 9.0 * s2) + s3));
       const double v = ((-(double)o1j) * df) * dz1;
-      if (Vb) Vb[(int64_t)j * a.V_zs] = v;
+      if (Vb) Vb[(int64_t)j * it.vz] = v;
       return v;
     };
     vtop = emit(n - 1, nx4_top_o1);
@@ -295,14 +330,13 @@ __device__ __forceinline__ void msolve_item(const MixedArgs &a, int64_t cl, int 
       const int c = n1 + j;
       const double df = (1.0 / 60.0) * (((45.0 * (f[c + 1] - f[c - 1])) - 9.0 * (f[c + 2] - f[c - 2])) + (f[c + 3] - f[c - 3]));
       const double v = ((-(double)s4[(int64_t)j * ss].y) * df) * dz1;
-      if (Vb) Vb[(int64_t)j * a.V_zs] = v;
+      if (Vb) Vb[(int64_t)j * it.vz] = v;
       if (j == 0) vbot = v;
       if (j == nz - 1) vtop = v;
     }
   }
-  const int64_t pidx = (int64_t)iw * a.ld_col + a.c_off + cl;
-  if (a.Vtop) a.Vtop[pidx] = vtop;
-  if (a.Vbot) a.Vbot[pidx] = vbot;
+  if (it.vtop) *it.vtop = vtop;
+  if (it.vbot) *it.vbot = vbot;
 }
 
 __global__ void __launch_bounds__(128) k_solve_mixed_staged(const MixedArgs a) {
@@ -337,7 +371,7 @@ __global__ void __launch_bounds__(128) k_solve_mixed_staged(const MixedArgs a) {
     const bool active = iw_raw < a.nw;
     const int iw = active ? iw_raw : a.nw - 1;
     pa.begin(a.rec + cl * (int64_t)a.nz * MZN);
-    msolve_item(a, cl, iw, active, pa, s4);
+    msolve_item(block_item(a, cl, iw), active, pa, s4, a.slot_stride);
     if (__any_sync(0xffffffffu, pa.failed)) {
       if (lane == 0) atomicOr(&a.status[2], 1ull);
       pa.wait(0);
@@ -363,7 +397,7 @@ __global__ void __launch_bounds__(128) k_solve_mixed(const MixedArgs a) {
       const int64_t cl = item / a.nw;
       const int iw = (int)(item - cl * a.nw);
       MDirect pa{a.rec + cl * (int64_t)a.nz * MZN};
-      msolve_item(a, cl, iw, true, pa, s4);
+      msolve_item(block_item(a, cl, iw), true, pa, s4, a.slot_stride);
     }
   }
 }
@@ -382,6 +416,123 @@ cudaError_t launch_solve_mixed(const MixedArgs &a, int blocks, int threads, cuda
     k_solve_mixed_staged<<<blocks, threads, 0, s>>>(a);
   else
     k_solve_mixed<<<blocks, threads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+/* ---- ragged batches ---------------------------------------------------------------------- */
+
+/* Item of a batch: wavelength iw of column c. */
+__device__ __forceinline__ MItem batch_item(const MixedBatchArgs &b, const MBatchCol &c, int iw) {
+  MItem it;
+  it.lam = b.lam + c.lam_off;
+  it.nz = c.nz;
+  it.nw = c.nw;
+  it.iw = iw;
+  it.dzf = c.dzf;
+  it.ldz2 = c.ldz2;
+  it.dz1 = c.dz1;
+  if (b.layout == 0) { /* per column [lambda][z] (z fastest) */
+    it.U = b.U + c.u_off + (int64_t)iw * (c.nz + 6);
+    it.K = b.K ? b.K + c.kv_off + (int64_t)iw * c.nz : nullptr;
+    it.V = b.V ? b.V + c.kv_off + (int64_t)iw * c.nz : nullptr;
+    it.uz = it.kz = it.vz = 1;
+  } else { /* per column [z][lambda] */
+    it.U = b.U + c.u_off + iw;
+    it.K = b.K ? b.K + c.kv_off + iw : nullptr;
+    it.V = b.V ? b.V + c.kv_off + iw : nullptr;
+    it.uz = it.kz = it.vz = c.nw;
+  }
+  it.vtop = b.Vtop ? b.Vtop + c.flux_off + iw : nullptr;
+  it.vbot = b.Vbot ? b.Vbot + c.flux_off + iw : nullptr;
+  return it;
+}
+
+/* Warp-column tiling: tasks (column, 32-wavelength tile) from the device queue, longest
+ * columns first; the column's records stream through the warp's shared-memory buffers. */
+__global__ void __launch_bounds__(128) k_batch_mixed_staged(const MixedBatchArgs b) {
+  __shared__ __align__(128) float s_rec[MWARPS][2 * MZC * MZN];
+  __shared__ __align__(8) unsigned long long s_bar[MWARPS][2];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  float4 *s4 = b.s4 + slot * 32 + lane;
+  MStaged pa;
+  pa.buf = s_rec[wib];
+  pa.bar0 = msmem(&s_bar[wib][0]);
+  pa.waits = 0;
+  pa.inflight = 0;
+  pa.failed = false;
+  if (lane == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(pa.bar0) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(pa.bar0 + 8u) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  for (;;) {
+    unsigned long long task = 0;
+    if (lane == 0) task = atomicAdd(b.work, 1ull);
+    task = __shfl_sync(0xffffffffu, task, 0);
+    if (task >= (unsigned long long)b.ntasks) break;
+    const uint2 t = b.tasks[task];
+    const MBatchCol c = b.cols[t.x];
+    const int iw_raw = (int)t.y * 32 + lane;
+    const bool active = iw_raw < c.nw;
+    const int iw = active ? iw_raw : c.nw - 1;
+    pa.nz = c.nz;
+    pa.begin(b.rec + c.rec_off * MZN);
+    msolve_item(batch_item(b, c, iw), active, pa, s4, b.slot_stride);
+    if (__any_sync(0xffffffffu, pa.failed)) {
+      if (lane == 0) atomicOr(&b.status[2], 1ull);
+      pa.wait(0);
+      pa.wait(1);
+      return;
+    }
+  }
+}
+
+/* Packed tiling: the (column, wavelength) items of the columns sorted by nz (longest first)
+ * form one list; a warp takes 32 consecutive items, so partial wavelength tiles of one column
+ * are filled with the next column's items (similar nz, as the list is sorted). */
+__global__ void __launch_bounds__(128) k_batch_mixed_packed(const MixedBatchArgs b) {
+  const int lane = threadIdx.x & 31;
+  const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  float4 *s4 = b.s4 + slot * 32 + lane;
+  for (;;) {
+    unsigned long long task = 0;
+    if (lane == 0) task = atomicAdd(b.work, 1ull);
+    task = __shfl_sync(0xffffffffu, task, 0);
+    if (task >= (unsigned long long)b.ntasks) break;
+    const int64_t item = (int64_t)task * 32 + lane;
+    if (item < b.nitems) {
+      int64_t lo = 0, hi = b.ncol; /* item_pre[lo] <= item < item_pre[hi] */
+      while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (__ldg(b.item_pre + mid) <= item)
+          lo = mid;
+        else
+          hi = mid;
+      }
+      const MBatchCol c = b.cols[__ldg(b.order + lo)];
+      const int iw = (int)(item - __ldg(b.item_pre + lo));
+      MDirect pa{b.rec + c.rec_off * MZN};
+      msolve_item(batch_item(b, c, iw), true, pa, s4, b.slot_stride);
+    }
+  }
+}
+
+int batch_mixed_max_blocks_per_sm(int tiling, int threads) {
+  int n = 0;
+  cudaError_t e = tiling == BATCH_TILING_PACKED
+                      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_mixed_packed, threads, 0)
+                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_mixed_staged, threads, 0);
+  if (e != cudaSuccess || n < 1) n = 1;
+  return n;
+}
+
+cudaError_t launch_batch_mixed(const MixedBatchArgs &a, int tiling, int blocks, int threads, cudaStream_t s) {
+  if (tiling == BATCH_TILING_PACKED)
+    k_batch_mixed_packed<<<blocks, threads, 0, s>>>(a);
+  else
+    k_batch_mixed_staged<<<blocks, threads, 0, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -23,77 +23,14 @@
 #include "mixed_core.h"
 #include "ocomath.h"
 #include "oco_consts.h"
+#include "oco_ctx.h"
 #include "oco_internal.h"
 
 using namespace oco;
 
 static thread_local std::string g_thread_err;
 
-struct DevBuf {
-  void *p = nullptr;
-  size_t n = 0;
-  cudaError_t ensure(size_t bytes) {
-    if (bytes <= n) return cudaSuccess;
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-    cudaError_t e = cudaMalloc(&p, bytes);
-    if (e == cudaSuccess) n = bytes;
-    return e;
-  }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-  }
-  template <class T>
-  T *as() const {
-    return (T *)p;
-  }
-};
-
-/* Per-chunk staging for the host-array path (two sets, used alternately). */
-struct Stage {
-  DevBuf rho, T, U, K, V, top, bot;
-  cudaEvent_t done = nullptr; /* copy-back of this set finished */
-};
-
-struct oco_ctx {
-  int device = 0;
-  int num_sms = 148;
-  cudaStream_t stream = nullptr; /* kernels */
-  cudaStream_t copy = nullptr;   /* host<->device copies of the host-array path */
-  std::string err;
-  /* wavelength tables (FP64 and the mixed form's FP32 log table) */
-  int nw = 0;
-  std::vector<double> wa;
-  DevBuf lam, lam32;
-  /* workspace */
-  DevBuf pil, scratch, work, status;
-  Stage stage[2];
-  int64_t launches = 0;
-  size_t budget_bytes = 8ull << 30; /* chunk budget for pillars + staged outputs */
-  /* kernel timing (oco_set_profiling) */
-  bool prof = false;
-  /* device-array calls defer the zero-pivot check to oco_synchronize */
-  bool status_pending = false;
-  cudaStream_t status_stream = nullptr;
-  oco_params status_params{};
-  std::vector<cudaEvent_t> ev_pool;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_solve, ev_pil;
-  cudaEvent_t take_event() {
-    if (!ev_pool.empty()) {
-      cudaEvent_t e = ev_pool.back();
-      ev_pool.pop_back();
-      return e;
-    }
-    cudaEvent_t e = nullptr;
-    cudaEventCreate(&e);
-    return e;
-  }
-};
-
-static int set_err(oco_ctx *c, int code, const char *fmt, ...) {
+int oco_set_err(oco_ctx *c, int code, const char *fmt, ...) {
   char buf[512];
   va_list ap;
   va_start(ap, fmt);
@@ -104,14 +41,6 @@ static int set_err(oco_ctx *c, int code, const char *fmt, ...) {
   return code;
 }
 
-#define CU(call)                                                                          \
-  do {                                                                                    \
-    cudaError_t e_ = (call);                                                              \
-    if (e_ != cudaSuccess)                                                                \
-      return set_err(c, e_ == cudaErrorMemoryAllocation ? OCO_ENOMEM : OCO_ECUDA,        \
-                     "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
-  } while (0)
-
 extern "C" int oco_abi_version(void) { return OCO_ABI_VERSION; }
 
 extern "C" const char *oco_last_error(const oco_ctx *c) {
@@ -120,14 +49,14 @@ extern "C" const char *oco_last_error(const oco_ctx *c) {
 
 extern "C" int oco_create(oco_ctx **out, int device) {
   oco_ctx *c = nullptr;
-  if (!out) return set_err(nullptr, OCO_EINVAL, "oco_create: out is NULL");
+  if (!out) return oco_set_err(nullptr, OCO_EINVAL, "oco_create: out is NULL");
   *out = nullptr;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
-    return set_err(nullptr, OCO_ECUDA, "oco_create: no CUDA device");
-  if (device < 0 || device >= ndev) return set_err(nullptr, OCO_EINVAL, "oco_create: bad device %d", device);
+    return oco_set_err(nullptr, OCO_ECUDA, "oco_create: no CUDA device");
+  if (device < 0 || device >= ndev) return oco_set_err(nullptr, OCO_EINVAL, "oco_create: bad device %d", device);
   c = new (std::nothrow) oco_ctx();
-  if (!c) return set_err(nullptr, OCO_ENOMEM, "oco_create: out of host memory");
+  if (!c) return oco_set_err(nullptr, OCO_ENOMEM, "oco_create: out of host memory");
   c->device = device;
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
@@ -138,7 +67,7 @@ extern "C" int oco_create(oco_ctx **out, int device) {
   if (e == cudaSuccess) e = c->work.ensure(64);
   if (e == cudaSuccess) e = c->status.ensure(64);
   if (e != cudaSuccess) {
-    int code = set_err(nullptr, OCO_ECUDA, "oco_create: %s", cudaGetErrorString(e));
+    int code = oco_set_err(nullptr, OCO_ECUDA, "oco_create: %s", cudaGetErrorString(e));
     oco_destroy(c);
     return code;
   }
@@ -183,7 +112,7 @@ extern "C" void oco_destroy(oco_ctx *c) {
 }
 
 extern "C" int oco_calc_wavelength(double w1, double w0, int32_t nw, double *wa) {
-  if (nw < 1 || !wa) return set_err(nullptr, OCO_EINVAL, "oco_calc_wavelength: nw < 1 or NULL wa");
+  if (nw < 1 || !wa) return oco_set_err(nullptr, OCO_EINVAL, "oco_calc_wavelength: nw < 1 or NULL wa");
   if (nw > 1) { /* continuous_opacity.f90:48-54 */
     double dw = (w1 - w0) / (double)(nw - 1);
     for (int i = 1; i <= nw; i++) wa[i - 1] = w0 + (double)(i - 1) * dw;
@@ -287,11 +216,11 @@ void oco::fill_mixed_lambda_table(const double *tab, int nw, float *tab32) {
 }
 
 extern "C" int oco_set_wavelengths(oco_ctx *c, const double *wa, int32_t nw) {
-  if (!c) return set_err(nullptr, OCO_EINVAL, "oco_set_wavelengths: NULL context");
-  if (!wa || nw < 1) return set_err(c, OCO_EINVAL, "oco_set_wavelengths: nw < 1 or NULL wa");
+  if (!c) return oco_set_err(nullptr, OCO_EINVAL, "oco_set_wavelengths: NULL context");
+  if (!wa || nw < 1) return oco_set_err(c, OCO_EINVAL, "oco_set_wavelengths: nw < 1 or NULL wa");
   for (int i = 0; i < nw; i++)
     if (!(wa[i] > 0.0) || !std::isfinite(wa[i]))
-      return set_err(c, OCO_EINVAL, "oco_set_wavelengths: wavelength %d is not positive", i);
+      return oco_set_err(c, OCO_EINVAL, "oco_set_wavelengths: wavelength %d is not positive", i);
   CU(cudaSetDevice(c->device));
   std::vector<double> tab((size_t)NL * nw, 0.0);
   fill_lambda_table(wa, nw, tab.data());
@@ -308,20 +237,20 @@ extern "C" int oco_set_wavelengths(oco_ctx *c, const double *wa, int32_t nw) {
 }
 
 static int check_params(oco_ctx *c, const oco_params *p) {
-  if (!c) return set_err(nullptr, OCO_EINVAL, "NULL context");
-  if (!p) return set_err(c, OCO_EINVAL, "NULL params");
+  if (!c) return oco_set_err(nullptr, OCO_EINVAL, "NULL context");
+  if (!p) return oco_set_err(c, OCO_EINVAL, "NULL params");
   if (p->nx < 1 || p->ny < 1 || p->nz < 2 || p->nw < 1)
-    return set_err(c, OCO_EINVAL, "bad dimensions nx=%d ny=%d nz=%d nw=%d (need nz >= 2)", p->nx, p->ny,
+    return oco_set_err(c, OCO_EINVAL, "bad dimensions nx=%d ny=%d nz=%d nw=%d (need nz >= 2)", p->nx, p->ny,
                    p->nz, p->nw);
   if (p->lgrey && p->nw != 1)
-    return set_err(c, OCO_EGREY, "For Grey RT use only one wavelength. Switch nw=1 in resolution.in");
+    return oco_set_err(c, OCO_EGREY, "For Grey RT use only one wavelength. Switch nw=1 in resolution.in");
   if (!p->lgrey && (c->nw != p->nw))
-    return set_err(c, OCO_ENOWAVES, "wavelength tables hold %d wavelengths, block has nw=%d", c->nw, p->nw);
+    return oco_set_err(c, OCO_ENOWAVES, "wavelength tables hold %d wavelengths, block has nw=%d", c->nw, p->nw);
   if (p->form != OCO_FORM_PLAIN && p->form != OCO_FORM_STABLE && p->form != OCO_FORM_MIXED)
-    return set_err(c, OCO_EINVAL, "unknown form %d", p->form);
+    return oco_set_err(c, OCO_EINVAL, "unknown form %d", p->form);
   if (p->layout != OCO_LAYOUT_REFERENCE && p->layout != OCO_LAYOUT_LAMBDA_FASTEST)
-    return set_err(c, OCO_EINVAL, "unknown layout %d", p->layout);
-  if (!(p->dz > 0.0)) return set_err(c, OCO_EINVAL, "dz must be positive");
+    return oco_set_err(c, OCO_EINVAL, "unknown layout %d", p->layout);
+  if (!(p->dz > 0.0)) return oco_set_err(c, OCO_EINVAL, "dz must be positive");
   return OCO_OK;
 }
 
@@ -462,11 +391,11 @@ static int read_status(oco_ctx *c, cudaStream_t s, const oco_params *p) {
   CU(cudaMemcpyAsync(st, c->status.p, sizeof st, cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
   if (st[2])
-    return set_err(c, OCO_ETIMEDOUT, "a bounded wait for a pillar copy ran out; results are incomplete");
+    return oco_set_err(c, OCO_ETIMEDOUT, "a bounded wait for a pillar copy ran out; results are incomplete");
   if (st[0]) {
     unsigned long long item = st[1];
     long long col = (long long)(item / (unsigned long long)p->nw), iw = (long long)(item % p->nw);
-    return set_err(c, OCO_EZEROPIVOT,
+    return oco_set_err(c, OCO_EZEROPIVOT,
                    "ERROR tridiag: bet == 0 in %llu (column, wavelength) items; first: ix=%lld iy=%lld iw=%lld",
                    st[0], col / p->ny + 1, col % p->ny + 1, iw + 1);
   }
@@ -500,8 +429,8 @@ extern "C" int oco_solve_block_device(oco_ctx *c, const oco_params *p, const dou
                                       void *stream) {
   int rc = check_params(c, p);
   if (rc) return rc;
-  if (p->form == OCO_FORM_MIXED && p->lgrey) return set_err(c, OCO_EINVAL, "the mixed form has no grey variant");
-  if (!rho || !T || !U) return set_err(c, OCO_EINVAL, "rho, T and U are required");
+  if (p->form == OCO_FORM_MIXED && p->lgrey) return oco_set_err(c, OCO_EINVAL, "the mixed form has no grey variant");
+  if (!rho || !T || !U) return oco_set_err(c, OCO_EINVAL, "rho, T and U are required");
   CU(cudaSetDevice(c->device));
   cudaStream_t s = (cudaStream_t)stream; /* NULL is the CUDA default stream */
   const int64_t ncol = (int64_t)p->nx * p->ny;
@@ -536,8 +465,8 @@ extern "C" int oco_solve_block(oco_ctx *c, const oco_params *p, const double *rh
                                double *kappa, double *V, double *Vtop, double *Vbot) {
   int rc = check_params(c, p);
   if (rc) return rc;
-  if (p->form == OCO_FORM_MIXED && p->lgrey) return set_err(c, OCO_EINVAL, "the mixed form has no grey variant");
-  if (!rho || !T || !U) return set_err(c, OCO_EINVAL, "rho, T and U are required");
+  if (p->form == OCO_FORM_MIXED && p->lgrey) return oco_set_err(c, OCO_EINVAL, "the mixed form has no grey variant");
+  if (!rho || !T || !U) return oco_set_err(c, OCO_EINVAL, "rho, T and U are required");
   CU(cudaSetDevice(c->device));
   const int64_t ncol = (int64_t)p->nx * p->ny;
   const int nz = p->nz, nw = p->nw, mz = nz + 6;
@@ -600,7 +529,7 @@ extern "C" int oco_solve_block(oco_ctx *c, const oco_params *p, const double *rh
 }
 
 extern "C" int oco_synchronize(oco_ctx *c) {
-  if (!c) return set_err(nullptr, OCO_EINVAL, "NULL context");
+  if (!c) return oco_set_err(nullptr, OCO_EINVAL, "NULL context");
   CU(cudaSetDevice(c->device));
   if (c->status_pending) {
     oco_params p = c->status_params;
@@ -615,13 +544,13 @@ extern "C" int oco_synchronize(oco_ctx *c) {
 extern "C" int64_t oco_kernel_launches(const oco_ctx *c) { return c ? c->launches : 0; }
 
 extern "C" int oco_set_profiling(oco_ctx *c, int enable) {
-  if (!c) return set_err(nullptr, OCO_EINVAL, "NULL context");
+  if (!c) return oco_set_err(nullptr, OCO_EINVAL, "NULL context");
   c->prof = enable != 0;
   return OCO_OK;
 }
 
 extern "C" int oco_kernel_times(oco_ctx *c, double *solve_ms, double *pillars_ms, int64_t *solve_launches) {
-  if (!c) return set_err(nullptr, OCO_EINVAL, "NULL context");
+  if (!c) return oco_set_err(nullptr, OCO_EINVAL, "NULL context");
   CU(cudaSetDevice(c->device));
   double ts = 0.0, tp = 0.0;
   int64_t n = (int64_t)c->ev_solve.size();

@@ -1,0 +1,397 @@
+/*
+ * oco_batch.cu -- ragged batches (include/oco.h, "Ragged batches"): many independent columns
+ * of different nz, dz and wavelength grids in one persistent launch, replayed as a CUDA graph.
+ *
+ * Work queue.  The kernels pull warp tasks from one device counter.  Tasks are ordered
+ * longest column first, so the short columns fill the tail of the launch (a greedy
+ * longest-processing-time schedule over the resident warps).  Two tilings:
+ *   OCO_TILING_WARP_COLUMN  task = (column, 32-wavelength tile); the column's records stream
+ *                           into the warp's shared memory (bulk copies); lanes past the
+ *                           column's nw idle;
+ *   OCO_TILING_PACKED       task = 32 consecutive (column, wavelength) items of the list of
+ *                           columns sorted by nz; no idle lanes, records read through L1.
+ * The autotuner (oco_batch_tune) times every (tiling, resident blocks per SM) candidate on
+ * the bound arrays and keeps the fastest.
+ *
+ * Graph.  oco_batch_bind captures: counter reset, status reset, the record kernel over all
+ * columns' z values, the solve kernel.  oco_batch_run replays it on the caller's stream.
+ */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <memory>
+#include <numeric>
+#include <utility>
+#include <vector>
+
+#include "../../include/oco.h"
+#include "mixed_core.h"
+#include "oco_ctx.h"
+#include "oco_internal.h"
+
+using namespace oco;
+
+static const int kBatchThreads = 128;
+
+struct oco_batch {
+  oco_ctx *c = nullptr;
+  int layout = OCO_LAYOUT_LAMBDA_FASTEST;
+  double fully_ionized_T = 2e4;
+  int64_t ncol = 0, npoints = 0, nrec = 0, nitems = 0, ntasks_tile = 0, ntasks_packed = 0;
+  int max_nz = 0, max_nw = 0;
+  int64_t need_in = 0, need_u = 0, need_kv = 0, need_flux = 0; /* element counts the arrays must hold */
+  DevBuf cols, rec_pre, tasks, order, item_pre, lam, rec, scratch, work, status;
+  int64_t slots = 0; /* scratch slots (threads of the largest persistent grid) */
+  int tiling = OCO_TILING_WARP_COLUMN, bps = 1, max_bps[2] = {1, 1};
+  /* bound arrays */
+  bool bound = false;
+  const double *rho = nullptr, *T = nullptr;
+  double *U = nullptr, *K = nullptr, *V = nullptr, *Vtop = nullptr, *Vbot = nullptr;
+  cudaStream_t cap = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t last = nullptr;
+  bool pending = false;
+  oco_batch_info info{};
+};
+
+static MixedBatchArgs batch_args(const oco_batch *b) {
+  MixedBatchArgs a{};
+  a.rec = b->rec.as<float>();
+  a.lam = b->lam.as<float>();
+  a.cols = b->cols.as<MBatchCol>();
+  a.tasks = b->tasks.as<uint2>();
+  a.order = b->order.as<int32_t>();
+  a.item_pre = b->item_pre.as<int64_t>();
+  a.ncol = b->ncol;
+  a.ntasks = b->tiling == OCO_TILING_PACKED ? b->ntasks_packed : b->ntasks_tile;
+  a.nitems = b->nitems;
+  a.U = b->U;
+  a.K = b->K;
+  a.V = b->V;
+  a.Vtop = b->Vtop;
+  a.Vbot = b->Vbot;
+  a.layout = b->layout;
+  a.s4 = b->scratch.as<float4>();
+  a.slot_stride = b->slots;
+  a.work = b->work.as<unsigned long long>();
+  a.status = b->status.as<unsigned long long>();
+  return a;
+}
+
+/* Enqueues one run (counter and status reset, records, solve) on s. */
+static int enqueue_run(oco_batch *b, cudaStream_t s) {
+  oco_ctx *c = b->c;
+  CU(cudaMemsetAsync(b->work.p, 0, sizeof(unsigned long long), s));
+  CU(cudaMemsetAsync(b->status.p, 0, 3 * sizeof(unsigned long long), s));
+  CU(launch_pillars_mixed_batch(b->rho, b->T, b->cols.as<MBatchCol>(), b->rec_pre.as<int64_t>(), b->ncol, b->nrec,
+                                b->fully_ionized_T, b->rec.as<float>(), s));
+  const MixedBatchArgs a = batch_args(b);
+  const int blocks = b->bps * c->num_sms;
+  CU(launch_batch_mixed(a, b->tiling == OCO_TILING_PACKED ? BATCH_TILING_PACKED : BATCH_TILING_WARP_COLUMN, blocks,
+                        kBatchThreads, s));
+  return OCO_OK;
+}
+
+static void drop_graph(oco_batch *b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+}
+
+static int capture(oco_batch *b) {
+  oco_ctx *c = b->c;
+  drop_graph(b);
+  CU(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+  int rc = enqueue_run(b, b->cap);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(b->cap, &g);
+  if (rc != OCO_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  CU(e);
+  b->graph = g;
+  CU(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  return OCO_OK;
+}
+
+static int check_status(oco_batch *b) {
+  oco_ctx *c = b->c;
+  unsigned long long st[3];
+  CU(cudaMemcpy(st, b->status.p, sizeof st, cudaMemcpyDeviceToHost));
+  if (st[2]) return oco_set_err(c, OCO_ETIMEDOUT, "batch: a bounded wait for a record copy ran out; results are incomplete");
+  return OCO_OK;
+}
+
+extern "C" int oco_batch_create(oco_ctx *c, const oco_batch_column *cols, int64_t ncol, const double *waves,
+                                int64_t nwaves, int32_t form, int32_t layout, double fully_ionized_T,
+                                oco_batch **out) {
+  if (!c) return oco_set_err(nullptr, OCO_EINVAL, "oco_batch_create: NULL context");
+  if (!out) return oco_set_err(c, OCO_EINVAL, "oco_batch_create: out is NULL");
+  *out = nullptr;
+  if (form != OCO_FORM_MIXED) return oco_set_err(c, OCO_EINVAL, "oco_batch_create: batches run the mixed form only");
+  if (layout != OCO_LAYOUT_REFERENCE && layout != OCO_LAYOUT_LAMBDA_FASTEST)
+    return oco_set_err(c, OCO_EINVAL, "oco_batch_create: bad layout %d", layout);
+  if (!cols || ncol < 1 || ncol > (int64_t)INT32_MAX)
+    return oco_set_err(c, OCO_EINVAL, "oco_batch_create: need 1 <= ncol <= 2^31-1 column descriptors");
+  if (!waves || nwaves < 1) return oco_set_err(c, OCO_EINVAL, "oco_batch_create: no wavelengths");
+  if (!std::isfinite(fully_ionized_T)) return oco_set_err(c, OCO_EINVAL, "oco_batch_create: fully_ionized_T not finite");
+  for (int64_t i = 0; i < nwaves; i++)
+    if (!(waves[i] > 0.0) || !std::isfinite(waves[i]))
+      return oco_set_err(c, OCO_EINVAL, "oco_batch_create: wavelength %lld is not positive", (long long)i);
+
+  oco_batch *b = new (std::nothrow) oco_batch();
+  if (!b) return oco_set_err(c, OCO_ENOMEM, "oco_batch_create: out of host memory");
+  std::unique_ptr<oco_batch, void (*)(oco_batch *)> guard(b, oco_batch_destroy);
+  b->c = c;
+  b->layout = layout;
+  b->fully_ionized_T = fully_ionized_T;
+  b->ncol = ncol;
+
+  /* descriptors, wavelength tables (one per distinct grid), record prefix sums */
+  std::vector<MBatchCol> dc((size_t)ncol);
+  std::vector<int64_t> rpre((size_t)ncol + 1, 0);
+  std::map<std::pair<int64_t, int32_t>, int64_t> grids;
+  std::vector<float> lam;
+  std::vector<double> tab;
+  for (int64_t i = 0; i < ncol; i++) {
+    const oco_batch_column &q = cols[i];
+    if (q.nz < 2 || q.nw < 1 || !(q.dz > 0.0) || !std::isfinite(q.dz) || q.in_off < 0 || q.u_off < 0 ||
+        q.kv_off < 0 || q.flux_off < 0 || q.wave_off < 0 || q.wave_off + q.nw > nwaves)
+      return oco_set_err(c, OCO_EINVAL,
+                         "oco_batch_create: column %lld: need nz >= 2, nw >= 1, dz > 0, offsets >= 0 and "
+                         "wave_off + nw <= nwaves",
+                         (long long)i);
+    auto key = std::make_pair(q.wave_off, q.nw);
+    auto it = grids.find(key);
+    int64_t loff;
+    if (it == grids.end()) {
+      loff = (int64_t)lam.size();
+      tab.assign((size_t)NL * q.nw, 0.0);
+      fill_lambda_table(waves + q.wave_off, q.nw, tab.data());
+      lam.resize(lam.size() + (size_t)MIXED_LN * q.nw);
+      fill_mixed_lambda_table(tab.data(), q.nw, lam.data() + loff);
+      grids.emplace(key, loff);
+    } else {
+      loff = it->second;
+    }
+    MBatchCol &d = dc[(size_t)i];
+    d.in_off = q.in_off;
+    d.rec_off = rpre[(size_t)i];
+    d.u_off = q.u_off;
+    d.kv_off = q.kv_off;
+    d.flux_off = q.flux_off;
+    d.lam_off = loff;
+    d.nz = q.nz;
+    d.nw = q.nw;
+    d.dzf = (float)q.dz;
+    d.ldz2 = (float)(2.0 * std::log2(q.dz));
+    d.dz1 = 1.0 / q.dz;
+    rpre[(size_t)i + 1] = rpre[(size_t)i] + q.nz;
+    b->npoints += (int64_t)q.nz * q.nw;
+    b->nitems += q.nw;
+    b->max_nz = std::max(b->max_nz, (int)q.nz);
+    b->max_nw = std::max(b->max_nw, (int)q.nw);
+    b->need_in = std::max(b->need_in, q.in_off + q.nz);
+    b->need_u = std::max(b->need_u, q.u_off + (int64_t)(q.nz + 6) * q.nw);
+    b->need_kv = std::max(b->need_kv, q.kv_off + (int64_t)q.nz * q.nw);
+    b->need_flux = std::max(b->need_flux, q.flux_off + q.nw);
+  }
+  b->nrec = rpre[(size_t)ncol];
+
+  /* work lists, longest column first */
+  std::vector<int32_t> order((size_t)ncol);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return cols[x].nz > cols[y].nz; });
+  std::vector<int64_t> ipre((size_t)ncol + 1, 0);
+  std::vector<uint2> tasks;
+  for (int64_t k = 0; k < ncol; k++) {
+    const int32_t i = order[(size_t)k];
+    ipre[(size_t)k + 1] = ipre[(size_t)k] + cols[i].nw;
+    const int ntile = (cols[i].nw + 31) / 32;
+    for (int t = 0; t < ntile; t++) tasks.push_back(make_uint2((unsigned)i, (unsigned)t));
+  }
+  b->ntasks_tile = (int64_t)tasks.size();
+  b->ntasks_packed = (b->nitems + 31) / 32;
+
+  /* device state */
+  CU(cudaSetDevice(c->device));
+  CU(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+  b->max_bps[0] = batch_mixed_max_blocks_per_sm(BATCH_TILING_WARP_COLUMN, kBatchThreads);
+  b->max_bps[1] = batch_mixed_max_blocks_per_sm(BATCH_TILING_PACKED, kBatchThreads);
+  b->slots = (int64_t)std::max(b->max_bps[0], b->max_bps[1]) * c->num_sms * kBatchThreads;
+  b->tiling = OCO_TILING_WARP_COLUMN;
+  b->bps = b->max_bps[0];
+  CU(b->cols.ensure(dc.size() * sizeof(MBatchCol)));
+  CU(b->rec_pre.ensure(rpre.size() * sizeof(int64_t)));
+  CU(b->tasks.ensure(tasks.size() * sizeof(uint2)));
+  CU(b->order.ensure(order.size() * sizeof(int32_t)));
+  CU(b->item_pre.ensure(ipre.size() * sizeof(int64_t)));
+  CU(b->lam.ensure(lam.size() * sizeof(float)));
+  CU(b->rec.ensure((size_t)b->nrec * MIXED_ZN * sizeof(float)));
+  CU(b->scratch.ensure((size_t)b->slots * b->max_nz * sizeof(float4)));
+  CU(b->work.ensure(64));
+  CU(b->status.ensure(64));
+  CU(cudaMemcpy(b->cols.p, dc.data(), dc.size() * sizeof(MBatchCol), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(b->rec_pre.p, rpre.data(), rpre.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(b->tasks.p, tasks.data(), tasks.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(b->order.p, order.data(), order.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(b->item_pre.p, ipre.data(), ipre.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(b->lam.p, lam.data(), lam.size() * sizeof(float), cudaMemcpyHostToDevice));
+  CU(cudaMemset(b->status.p, 0, 64));
+
+  b->info.ncol = ncol;
+  b->info.npoints = b->npoints;
+  b->info.max_nz = b->max_nz;
+  b->info.max_nw = b->max_nw;
+  *out = guard.release();
+  return OCO_OK;
+}
+
+extern "C" int oco_batch_bind(oco_batch *b, const double *rho, const double *T, int64_t n_in, double *U, int64_t n_u,
+                              double *kappa, double *V, int64_t n_kv, double *Vtop, double *Vbot, int64_t n_flux) {
+  if (!b) return oco_set_err(nullptr, OCO_EINVAL, "oco_batch_bind: NULL batch");
+  oco_ctx *c = b->c;
+  if (!rho || !T || !U) return oco_set_err(c, OCO_EINVAL, "oco_batch_bind: rho, T and U are required");
+  if (n_in < b->need_in || n_u < b->need_u)
+    return oco_set_err(c, OCO_EINVAL, "oco_batch_bind: inputs need %lld elements and U %lld",
+                       (long long)b->need_in, (long long)b->need_u);
+  if ((kappa || V) && n_kv < b->need_kv)
+    return oco_set_err(c, OCO_EINVAL, "oco_batch_bind: kappa and V need %lld elements", (long long)b->need_kv);
+  if ((Vtop || Vbot) && n_flux < b->need_flux)
+    return oco_set_err(c, OCO_EINVAL, "oco_batch_bind: Vtop and Vbot need %lld elements", (long long)b->need_flux);
+  CU(cudaSetDevice(c->device));
+  if (b->pending) CU(cudaStreamSynchronize(b->last));
+  b->rho = rho;
+  b->T = T;
+  b->U = U;
+  b->K = kappa;
+  b->V = V;
+  b->Vtop = Vtop;
+  b->Vbot = Vbot;
+  b->bound = true;
+  return capture(b);
+}
+
+extern "C" int oco_batch_tune(oco_batch *b) {
+  if (!b) return oco_set_err(nullptr, OCO_EINVAL, "oco_batch_tune: NULL batch");
+  oco_ctx *c = b->c;
+  if (!b->bound) return oco_set_err(c, OCO_EINVAL, "oco_batch_tune: bind the arrays first");
+  CU(cudaSetDevice(c->device));
+  if (b->pending) CU(cudaStreamSynchronize(b->last));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  struct Cand {
+    int tiling, bps;
+    float ms;
+  };
+  std::vector<Cand> cands;
+  for (int t = 0; t < 2; t++)
+    for (int d = 0; d < 3; d++) {
+      const int bps = b->max_bps[t] - d;
+      if (bps >= 1) cands.push_back({t, bps, 0.0f});
+    }
+  if (cands.size() > 16) cands.resize(16);
+  int rc = OCO_OK;
+  bool warm = false;
+  for (auto &k : cands) {
+    b->tiling = k.tiling;
+    b->bps = k.bps;
+    if (!warm) { /* first touch of the outputs and the code */
+      rc = enqueue_run(b, b->cap);
+      warm = true;
+      if (rc) break;
+    }
+    cudaEventRecord(e0, b->cap);
+    rc = enqueue_run(b, b->cap);
+    if (rc) break;
+    cudaEventRecord(e1, b->cap);
+    if (cudaEventSynchronize(e1) != cudaSuccess) {
+      rc = oco_set_err(c, OCO_ECUDA, "oco_batch_tune: %s", cudaGetErrorString(cudaGetLastError()));
+      break;
+    }
+    cudaEventElapsedTime(&k.ms, e0, e1);
+    if ((rc = check_status(b))) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  const Cand *best = &cands[0];
+  for (auto &k : cands)
+    if (k.ms < best->ms) best = &k;
+  b->tiling = best->tiling;
+  b->bps = best->bps;
+  b->info.ncandidates = (int32_t)cands.size();
+  for (size_t i = 0; i < cands.size(); i++) {
+    b->info.cand_tiling[i] = cands[i].tiling;
+    b->info.cand_blocks_per_sm[i] = cands[i].bps;
+    b->info.cand_ms[i] = cands[i].ms;
+  }
+  b->info.tuned = 1;
+  return capture(b);
+}
+
+extern "C" int oco_batch_set_tiling(oco_batch *b, int32_t tiling, int32_t blocks_per_sm) {
+  if (!b) return oco_set_err(nullptr, OCO_EINVAL, "oco_batch_set_tiling: NULL batch");
+  oco_ctx *c = b->c;
+  if (tiling != OCO_TILING_WARP_COLUMN && tiling != OCO_TILING_PACKED)
+    return oco_set_err(c, OCO_EINVAL, "oco_batch_set_tiling: bad tiling %d", tiling);
+  const int lim = b->max_bps[tiling];
+  if (blocks_per_sm < 0 || blocks_per_sm > lim)
+    return oco_set_err(c, OCO_EINVAL, "oco_batch_set_tiling: blocks_per_sm must be 0..%d", lim);
+  CU(cudaSetDevice(c->device));
+  if (b->pending) CU(cudaStreamSynchronize(b->last));
+  b->tiling = tiling;
+  b->bps = blocks_per_sm ? blocks_per_sm : lim;
+  return b->bound ? capture(b) : OCO_OK;
+}
+
+extern "C" int oco_batch_run(oco_batch *b, void *stream) {
+  if (!b) return oco_set_err(nullptr, OCO_EINVAL, "oco_batch_run: NULL batch");
+  oco_ctx *c = b->c;
+  if (!b->bound || !b->exec) return oco_set_err(c, OCO_EINVAL, "oco_batch_run: bind the arrays first");
+  CU(cudaSetDevice(c->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  CU(cudaGraphLaunch(b->exec, s));
+  b->last = s;
+  b->pending = true;
+  b->info.graph_launches++;
+  c->launches += 2;
+  return OCO_OK;
+}
+
+extern "C" int oco_batch_wait(oco_batch *b) {
+  if (!b) return oco_set_err(nullptr, OCO_EINVAL, "oco_batch_wait: NULL batch");
+  oco_ctx *c = b->c;
+  if (!b->pending) return OCO_OK;
+  CU(cudaSetDevice(c->device));
+  CU(cudaStreamSynchronize(b->last));
+  b->pending = false;
+  return check_status(b);
+}
+
+extern "C" int oco_batch_get_info(const oco_batch *b, oco_batch_info *info) {
+  if (!b || !info) return oco_set_err(nullptr, OCO_EINVAL, "oco_batch_get_info: NULL argument");
+  *info = b->info;
+  info->tiling = b->tiling;
+  info->blocks_per_sm = b->bps;
+  return OCO_OK;
+}
+
+extern "C" void oco_batch_destroy(oco_batch *b) {
+  if (!b) return;
+  if (b->c) cudaSetDevice(b->c->device);
+  if (b->pending && b->last) cudaStreamSynchronize(b->last);
+  if (b->cap) cudaStreamSynchronize(b->cap);
+  drop_graph(b);
+  for (DevBuf *d : {&b->cols, &b->rec_pre, &b->tasks, &b->order, &b->item_pre, &b->lam, &b->rec, &b->scratch,
+                    &b->work, &b->status})
+    d->release();
+  if (b->cap) cudaStreamDestroy(b->cap);
+  delete b;
+}

@@ -118,6 +118,46 @@ struct MixedArgs {
   unsigned long long *status;
 };
 
+/* One column of a ragged batch as the batch kernels see it (built from oco_batch_column). */
+struct MBatchCol {
+  int64_t in_off;   /* rho/T of z = 0 in the bound input arrays */
+  int64_t rec_off;  /* first mixed record of the column (dense prefix of nz) */
+  int64_t u_off;    /* first U element of the column */
+  int64_t kv_off;   /* first kappa / V element */
+  int64_t flux_off; /* first emergent-flux element */
+  int64_t lam_off;  /* first float of the column's [MIXED_LN][nw] wavelength table */
+  int32_t nz, nw;
+  float dzf, ldz2;  /* dz and log2(dz^2) */
+  double dz1;       /* 1/dz */
+};
+
+/* Arguments of the ragged-batch kernels (mixed form). */
+struct MixedBatchArgs {
+  const float *rec;        /* [sum nz][MIXED_ZN] */
+  const float *lam;        /* packed wavelength tables */
+  const MBatchCol *cols;
+  const uint2 *tasks;      /* warp-column tiling: (column, 32-wavelength tile), longest first */
+  const int32_t *order;    /* packed tiling: columns, longest first */
+  const int64_t *item_pre; /* packed tiling: prefix sums of nw over order, ncol + 1 entries */
+  int64_t ncol, ntasks, nitems;
+  double *U, *K, *V, *Vtop, *Vbot;
+  int layout;
+  float4 *s4;
+  int64_t slot_stride;
+  unsigned long long *work;
+  unsigned long long *status;
+};
+
+/* Tilings of the batch kernels. */
+constexpr int BATCH_TILING_WARP_COLUMN = 0; /* a warp solves 32 wavelengths of one column, records staged */
+constexpr int BATCH_TILING_PACKED = 1;      /* a warp solves 32 consecutive items of the nz-sorted list */
+
+cudaError_t launch_pillars_mixed_batch(const double *rho, const double *T, const MBatchCol *cols,
+                                       const int64_t *rec_pre, int64_t ncol, int64_t nrec, double fully_ionized_T,
+                                       float *rec, cudaStream_t s);
+cudaError_t launch_batch_mixed(const MixedBatchArgs &a, int tiling, int blocks, int threads, cudaStream_t s);
+int batch_mixed_max_blocks_per_sm(int tiling, int threads);
+
 /* Fills tab[NL*nw] (layout [field][iw]) with the wavelength table of waves[nw] (Angstrom):
  * pre_calc_opacity_quantities' arithmetic plus the hot loop's lambda-only factors
  * (defined in oco_api.cu). */

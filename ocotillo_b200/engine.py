@@ -42,6 +42,23 @@ class OcoParams(ctypes.Structure):
                 ("reserved", ctypes.c_int32)]
 
 
+class OcoBatchColumn(ctypes.Structure):
+    """oco_batch_column: one column of a ragged batch (element offsets into the bound arrays)."""
+    _fields_ = [("in_off", ctypes.c_int64), ("u_off", ctypes.c_int64), ("kv_off", ctypes.c_int64),
+                ("flux_off", ctypes.c_int64), ("wave_off", ctypes.c_int64), ("nz", ctypes.c_int32),
+                ("nw", ctypes.c_int32), ("dz", ctypes.c_double)]
+
+
+class OcoBatchInfo(ctypes.Structure):
+    _fields_ = [("ncol", ctypes.c_int64), ("npoints", ctypes.c_int64), ("max_nz", ctypes.c_int32),
+                ("max_nw", ctypes.c_int32), ("tiling", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
+                ("tuned", ctypes.c_int32), ("ncandidates", ctypes.c_int32), ("cand_tiling", ctypes.c_int32 * 16),
+                ("cand_blocks_per_sm", ctypes.c_int32 * 16), ("cand_ms", ctypes.c_double * 16),
+                ("graph_launches", ctypes.c_int64)]
+
+
+TILING_WARP_COLUMN, TILING_PACKED = 0, 1
+
 _LIB = None
 _DP = ctypes.POINTER(ctypes.c_double)
 
@@ -71,6 +88,16 @@ def load_library(path=None):
         "oco_kernel_times": (I, [V, _DP, _DP, ctypes.POINTER(ctypes.c_int64)]),
         "oco_solve_block_noalloc": (I, [P, _DP, V, V, V, V, V, V, V, V]),
         "oco_noalloc_last_error": (ctypes.c_char_p, []),
+        "oco_batch_create": (I, [V, ctypes.POINTER(OcoBatchColumn), ctypes.c_int64, _DP, ctypes.c_int64,
+                                 ctypes.c_int32, ctypes.c_int32, D, ctypes.POINTER(V)]),
+        "oco_batch_bind": (I, [V, V, V, ctypes.c_int64, V, ctypes.c_int64, V, V, ctypes.c_int64, V, V,
+                               ctypes.c_int64]),
+        "oco_batch_tune": (I, [V]),
+        "oco_batch_set_tiling": (I, [V, ctypes.c_int32, ctypes.c_int32]),
+        "oco_batch_run": (I, [V, V]),
+        "oco_batch_wait": (I, [V]),
+        "oco_batch_get_info": (I, [V, ctypes.POINTER(OcoBatchInfo)]),
+        "oco_batch_destroy": (None, [V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -201,3 +228,133 @@ class Engine:
         a, b, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64()
         self._check(self.lib.oco_kernel_times(self.ctx, ctypes.byref(a), ctypes.byref(b), ctypes.byref(n)))
         return a.value, b.value, n.value
+
+    def batch(self, nz, nw, dz, waves, wave_off, layout=LAYOUT_LAMBDA_FASTEST, fully_ionized_T=2e4, form="mixed"):
+        """A ragged batch of len(nz) columns packed densely (see dense_batch_offsets): column i
+        has nz[i] levels, spacing dz[i] and the nw[i] wavelengths waves[wave_off[i]:...]."""
+        return Batch(self, nz, nw, dz, waves, wave_off, layout, fully_ionized_T, form)
+
+
+def dense_batch_offsets(nz, nw):
+    """Dense packing of a batch's arrays: per column in_off (rho, T), u_off (U),
+    kv_off (kappa, V), flux_off (Vtop, Vbot), and the total element counts of each."""
+    nz = np.asarray(nz, dtype=np.int64)
+    nw = np.asarray(nw, dtype=np.int64)
+
+    def pre(x):
+        return np.concatenate([[0], np.cumsum(x)])
+
+    p_in, p_u, p_kv, p_f = pre(nz), pre((nz + 6) * nw), pre(nz * nw), pre(nw)
+    return {"in_off": p_in[:-1], "u_off": p_u[:-1], "kv_off": p_kv[:-1], "flux_off": p_f[:-1],
+            "n_in": int(p_in[-1]), "n_u": int(p_u[-1]), "n_kv": int(p_kv[-1]), "n_flux": int(p_f[-1])}
+
+
+class Batch:
+    """Ragged batch (include/oco.h, oco_batch_*): independent columns of different nz, dz
+    and wavelength grids, solved by one persistent launch replayed as a CUDA graph.  Arrays
+    are torch CUDA float64 tensors packed as dense_batch_offsets describes; per column U is
+    [z][lambda] (LAYOUT_LAMBDA_FASTEST) or [lambda][z] (LAYOUT_REFERENCE)."""
+
+    def __init__(self, eng, nz, nw, dz, waves, wave_off, layout, fully_ionized_T, form):
+        self.eng, self.lib = eng, eng.lib
+        n = len(nz)
+        self.nz = np.asarray(nz, dtype=np.int64)
+        self.nw = np.asarray(nw, dtype=np.int64)
+        self.offsets = dense_batch_offsets(self.nz, self.nw)
+        cols = (OcoBatchColumn * n)()
+        o = self.offsets
+        for i in range(n):
+            cols[i] = OcoBatchColumn(int(o["in_off"][i]), int(o["u_off"][i]), int(o["kv_off"][i]),
+                                     int(o["flux_off"][i]), int(wave_off[i]), int(self.nz[i]), int(self.nw[i]),
+                                     float(dz[i]))
+        w = np.ascontiguousarray(waves, dtype=np.float64)
+        self.layout = layout
+        self.h = ctypes.c_void_p()
+        rc = self.lib.oco_batch_create(eng.ctx, cols, n, _ptr(w), w.size,
+                                       _FORMS[form] if isinstance(form, str) else int(form), int(layout),
+                                       float(fully_ionized_T), ctypes.byref(self.h))
+        eng._check(rc)
+        self.arrays = None
+
+    def alloc(self, device="cuda", want=("kappa", "V", "Vtop", "Vbot")):
+        """Allocates output tensors of the dense packing."""
+        import torch
+        o = self.offsets
+        out = {"U": torch.empty(o["n_u"], dtype=torch.float64, device=device)}
+        for k in want:
+            out[k] = torch.empty(o["n_kv"] if k in ("kappa", "V") else o["n_flux"], dtype=torch.float64,
+                                 device=device)
+        return out
+
+    def bind(self, rho, T, out):
+        """Binds device inputs (dense rho, T) and outputs (dict of U, kappa, V, Vtop, Vbot)."""
+        o = self.offsets
+
+        def p(t):
+            return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+        g = out.get
+        n_kv = (g("kappa") if g("kappa") is not None else g("V"))
+        n_fl = (g("Vtop") if g("Vtop") is not None else g("Vbot"))
+        rc = self.lib.oco_batch_bind(self.h, p(rho), p(T), min(rho.numel(), T.numel()), p(out["U"]),
+                                     out["U"].numel(), p(g("kappa")), p(g("V")),
+                                     n_kv.numel() if n_kv is not None else 0, p(g("Vtop")), p(g("Vbot")),
+                                     n_fl.numel() if n_fl is not None else 0)
+        self.eng._check(rc)
+        self.arrays = (rho, T, out)
+        return out
+
+    def tune(self):
+        self.eng._check(self.lib.oco_batch_tune(self.h))
+        return self.info()
+
+    def set_tiling(self, tiling, blocks_per_sm=0):
+        """tiling: 'warp_column' or 'packed' (or TILING_*); blocks_per_sm 0 = occupancy limit."""
+        t = {"warp_column": TILING_WARP_COLUMN, "packed": TILING_PACKED}.get(tiling, tiling)
+        self.eng._check(self.lib.oco_batch_set_tiling(self.h, int(t), int(blocks_per_sm)))
+
+    def run(self, stream=None):
+        import torch
+        if stream is None:
+            stream = torch.cuda.current_stream()
+        self.eng._check(self.lib.oco_batch_run(self.h, ctypes.c_void_p(stream.cuda_stream)))
+
+    def wait(self):
+        self.eng._check(self.lib.oco_batch_wait(self.h))
+
+    def info(self):
+        inf = OcoBatchInfo()
+        self.eng._check(self.lib.oco_batch_get_info(self.h, ctypes.byref(inf)))
+        n = inf.ncandidates
+        return {"ncol": inf.ncol, "npoints": inf.npoints, "max_nz": inf.max_nz, "max_nw": inf.max_nw,
+                "tiling": ("warp_column", "packed")[inf.tiling], "blocks_per_sm": inf.blocks_per_sm,
+                "tuned": bool(inf.tuned), "graph_launches": inf.graph_launches,
+                "candidates": [{"tiling": ("warp_column", "packed")[inf.cand_tiling[i]],
+                                "blocks_per_sm": inf.cand_blocks_per_sm[i], "ms": inf.cand_ms[i]}
+                               for i in range(n)]}
+
+    def column(self, out, i, name):
+        """View of column i's block of output `name` as (nz+6, nw) / (nz, nw) / (nw,) in z, lambda
+        order (whatever the layout)."""
+        o = self.offsets
+        nz, nw = int(self.nz[i]), int(self.nw[i])
+        if name == "U":
+            a = out["U"][o["u_off"][i]:o["u_off"][i] + (nz + 6) * nw]
+            rows = nz + 6
+        elif name in ("kappa", "V"):
+            a = out[name][o["kv_off"][i]:o["kv_off"][i] + nz * nw]
+            rows = nz
+        else:
+            return out[name][o["flux_off"][i]:o["flux_off"][i] + nw]
+        return a.view(rows, nw) if self.layout == LAYOUT_LAMBDA_FASTEST else a.view(nw, rows).t()
+
+    def close(self):
+        if self.h:
+            self.lib.oco_batch_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

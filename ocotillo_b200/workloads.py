@@ -65,3 +65,51 @@ def grey_isothermal():
     rho = np.where(rho < RHO_FLOOR, RHO_FLOOR, rho)
     T = np.full(10, 2000.0)
     return rho.reshape(1, 1, 10), T.reshape(1, 1, 10), dz
+
+
+K_CGS, M_U, MU_GAS = 1.380649e-16, 1.66053906660e-24, 0.6
+
+
+def athena_column(nz, rng, rho0=RHO0, sigma_dex=0.5, t_mid=T_MID, sigma_t=SIGMA_T):
+    """One synthetic Athena-style column: density and pressure each Gaussian-stratified times
+    a lognormal turbulence of sigma_dex; T = mu m_u p / (rho k) with mu = 0.6 and a 2000 K
+    floor (the temperature read_athena.f90 reconstructs from E = p/gamma1 with zero momenta
+    and mean_molecular_weight = 0.6).  The pressure scale height combines H and sigma_t so
+    that the mean temperature profile is the Gaussian of `temperature`.  Returns rho, T, dz."""
+    z, dz = grid(nz)
+    g = np.exp(-0.5 * z * z / (H * H))
+    rho = np.maximum(rho0 * g, RHO_FLOOR) * 10.0 ** (sigma_dex * rng.standard_normal(nz))
+    p0 = rho0 * K_CGS * t_mid / (MU_GAS * M_U)
+    pres = p0 * g * np.exp(-0.5 * z * z / (sigma_t * sigma_t)) * 10.0 ** (sigma_dex * rng.standard_normal(nz))
+    T = MU_GAS * M_U * pres / (rho * K_CGS)
+    T = np.where(T > T_FLOOR, T, T_FLOOR)
+    return rho, T, dz
+
+
+def ragged_batch(ncol=8192, seed=4, nz_range=(64, 2048), nw_range=(32, 1024)):
+    """Config 'batching form': ncol independent columns with nz = floor(exp U(ln a, ln b)) and
+    nw likewise, each an athena_column; every column's wavelength grid is log_wavelengths(nw),
+    one grid per distinct nw.  Returns a dict with per-column nz, nw, dz, wave_off, the packed
+    wavelength array, and dense rho, T (concatenated z profiles)."""
+    rng = np.random.default_rng(seed)
+    nz = np.floor(np.exp(rng.uniform(math.log(nz_range[0]), math.log(nz_range[1]), ncol))).astype(np.int64)
+    nw = np.floor(np.exp(rng.uniform(math.log(nw_range[0]), math.log(nw_range[1]), ncol))).astype(np.int64)
+    nz = np.clip(nz, nz_range[0], nz_range[1])
+    nw = np.clip(nw, nw_range[0], nw_range[1])
+    grids, waves, wave_off = {}, [], np.empty(ncol, dtype=np.int64)
+    pos = 0
+    for i, w in enumerate(nw):
+        w = int(w)
+        if w not in grids:
+            grids[w] = pos
+            waves.append(log_wavelengths(w))
+            pos += w
+        wave_off[i] = grids[w]
+    rhos, Ts, dzs = [], [], np.empty(ncol)
+    for i in range(ncol):
+        r, t, dz = athena_column(int(nz[i]), rng)
+        rhos.append(r)
+        Ts.append(t)
+        dzs[i] = dz
+    return {"nz": nz, "nw": nw, "dz": dzs, "wave_off": wave_off, "waves": np.concatenate(waves),
+            "rho": np.concatenate(rhos), "T": np.concatenate(Ts)}

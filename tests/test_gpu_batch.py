@@ -1,0 +1,210 @@
+"""Ragged batches (oco_batch_*): independent columns of different nz, dz and wavelength grids
+in one persistent launch replayed as a CUDA graph, mixed form.
+
+Per column the batch runs the arithmetic of the block solve's mixed form, so every column is
+compared with a 1x1 block solve of the same column (relative difference <= 1e-6: same
+operations, possibly contracted into FMAs differently by the two kernel instantiations), and a
+few columns with the stable FP64 oracle at the mixed form's tolerances.  Tilings and graph
+replays must give identical results.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL_SAME = 1e-6
+TOL_FLUX, TOL_KAPPA, TOL_U = 1e-4, 3e-5, 5e-4
+
+
+@pytest.fixture(scope="module")
+def engine():
+    import torch
+    assert torch.cuda.is_available()
+    from ocotillo_b200 import Engine
+    e = Engine(0)
+    yield e
+    e.close()
+
+
+def _small_batch(seed=11):
+    """Columns covering the edge sizes: nz 2..300 (2 and 3 take the short-column path), nw 1..97
+    (partial 32-wavelength tiles), several grids shared between columns."""
+    from ocotillo_b200 import workloads
+    rng = np.random.default_rng(seed)
+    nz = np.array([2, 3, 4, 5, 7, 31, 32, 33, 64, 100, 257, 300, 40, 41, 64, 2, 128, 90], dtype=np.int64)
+    nw = np.array([1, 5, 31, 32, 33, 64, 70, 97, 1, 7, 40, 33, 32, 64, 96, 3, 65, 31], dtype=np.int64)
+    grids, waves, off = {}, [], []
+    pos = 0
+    for w in nw:
+        w = int(w)
+        if w not in grids:
+            grids[w] = pos
+            waves.append(workloads.log_wavelengths(w, 900.0, 40000.0))
+            pos += w
+        off.append(grids[w])
+    rhos, Ts, dzs = [], [], []
+    for n in nz:
+        r, t, dz = workloads.athena_column(int(n), rng, sigma_dex=0.3)
+        rhos.append(r)
+        Ts.append(t)
+        dzs.append(dz)
+    return {"nz": nz, "nw": nw, "dz": np.array(dzs), "wave_off": np.array(off), "waves": np.concatenate(waves),
+            "rho": np.concatenate(rhos), "T": np.concatenate(Ts)}
+
+
+def _make(engine, d, layout):
+    import torch
+    b = engine.batch(d["nz"], d["nw"], d["dz"], d["waves"], d["wave_off"], layout=layout)
+    dev = torch.device("cuda:0")
+    rho = torch.from_numpy(d["rho"]).to(dev)
+    T = torch.from_numpy(d["T"]).to(dev)
+    out = b.alloc(dev)
+    b.bind(rho, T, out)
+    return b, rho, T, out
+
+
+def _block(engine, d, i):
+    """Column i as a 1x1 block through the block solve (host arrays), mixed form."""
+    o = np.concatenate([[0], np.cumsum(d["nz"])])
+    nz, nw = int(d["nz"][i]), int(d["nw"][i])
+    wa = d["waves"][d["wave_off"][i]:d["wave_off"][i] + nw]
+    engine.set_wavelengths(wa)
+    rho = d["rho"][o[i]:o[i + 1]].reshape(1, 1, nz)
+    T = d["T"][o[i]:o[i + 1]].reshape(1, 1, nz)
+    return engine.solve_block(rho, T, float(d["dz"][i]), form="mixed"), rho, T, wa
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
+
+
+@pytest.mark.parametrize("layout", [0, 1])
+def test_batch_matches_block_solve(engine, layout):
+    d = _small_batch()
+    b, _, _, out = _make(engine, d, layout)
+    b.run()
+    b.wait()
+    for i in range(len(d["nz"])):
+        ref, _, _, _ = _block(engine, d, i)
+        U = b.column(out, i, "U").cpu().numpy()         # (nz+6, nw)
+        K = b.column(out, i, "kappa").cpu().numpy()
+        V = b.column(out, i, "V").cpu().numpy()
+        vt = b.column(out, i, "Vtop").cpu().numpy()
+        vb = b.column(out, i, "Vbot").cpu().numpy()
+        what = f"column {i} nz={d['nz'][i]} nw={d['nw'][i]} layout={layout}"
+        assert _rel(U, ref["U"][:, 0, 0, :].T) <= TOL_SAME, what
+        assert _rel(K, ref["kappa"][:, 0, 0, :].T) <= TOL_SAME, what
+        vmax = np.abs(ref["V"][:, 0, 0, :]).max()
+        assert np.abs(V - ref["V"][:, 0, 0, :].T).max() <= TOL_SAME * vmax, what
+        assert np.array_equal(vt, V[-1]) and np.array_equal(vb, V[0]), what
+    b.close()
+
+
+def test_batch_tilings_and_replay_identical(engine):
+    d = _small_batch(seed=12)
+    b, rho, T, out = _make(engine, d, 1)
+    results = []
+    for tiling, bps in (("warp_column", 0), ("packed", 0), ("warp_column", 2), ("packed", 1)):
+        b.set_tiling(tiling, bps)
+        for _ in range(2):  # graph replay twice
+            for v in out.values():
+                v.fill_(float("nan"))
+            b.run()
+            b.wait()
+            results.append({k: v.cpu().numpy().copy() for k, v in out.items()})
+    for r in results[1:]:
+        for k in r:
+            assert np.array_equal(r[k], results[0][k]), k
+    info = b.info()
+    assert info["graph_launches"] == 8 and info["npoints"] == int((d["nz"] * d["nw"]).sum())
+    b.close()
+
+
+def test_batch_tune_keeps_results(engine):
+    d = _small_batch(seed=13)
+    b, rho, T, out = _make(engine, d, 1)
+    b.run()
+    b.wait()
+    first = {k: v.cpu().numpy().copy() for k, v in out.items()}
+    info = b.tune()
+    assert info["tuned"]
+    assert len(info["candidates"]) >= 2 and all(c["ms"] > 0 for c in info["candidates"])
+    best = min(info["candidates"], key=lambda c: c["ms"])
+    assert (info["tiling"], info["blocks_per_sm"]) == (best["tiling"], best["blocks_per_sm"])
+    for v in out.values():
+        v.zero_()
+    b.run()
+    b.wait()
+    for k, v in out.items():
+        assert np.array_equal(v.cpu().numpy(), first[k]), k
+    b.close()
+
+
+def test_batch_rebinding_new_inputs(engine):
+    """In-place new input values are picked up by the replayed graph; rebinding to other
+    arrays recaptures."""
+    d = _small_batch(seed=14)
+    b, rho, T, out = _make(engine, d, 1)
+    b.run()
+    b.wait()
+    U1 = out["U"].cpu().numpy().copy()
+    T.mul_(1.05)
+    b.run()
+    b.wait()
+    U2 = out["U"].cpu().numpy().copy()
+    assert not np.array_equal(U1, U2)
+    d2 = dict(d, T=d["T"] * 1.05)
+    b2, _, _, out2 = _make(engine, d2, 1)
+    b2.run()
+    b2.wait()
+    assert np.array_equal(out2["U"].cpu().numpy(), U2)
+    b.close()
+    b2.close()
+
+
+def test_batch_against_oracle(engine, oracle):
+    d = _small_batch(seed=15)
+    b, _, _, out = _make(engine, d, 0)
+    b.run()
+    b.wait()
+    o = np.concatenate([[0], np.cumsum(d["nz"])])
+    for i in range(len(d["nz"])):
+        nz, nw = int(d["nz"][i]), int(d["nw"][i])
+        wa = d["waves"][d["wave_off"][i]:d["wave_off"][i] + nw]
+        rho = d["rho"][o[i]:o[i + 1]].reshape(1, 1, nz)
+        T = d["T"][o[i]:o[i + 1]].reshape(1, 1, nz)
+        ref = oracle.solve_block(rho, T, wa, float(d["dz"][i]), form=oracle.FORM_STABLE, backend="ocomath")
+        what = f"column {i} nz={nz} nw={nw}"
+        assert _rel(b.column(out, i, "kappa").cpu().numpy(), ref["kappa"][:, 0, 0, :].T) <= TOL_KAPPA, what
+        assert _rel(b.column(out, i, "U").cpu().numpy(), ref["U"][:, 0, 0, :].T) <= TOL_U, what
+        if nz >= 4:  # see test_gpu_mixed.test_mixed_small_sizes for nz < 4
+            assert _rel(b.column(out, i, "Vtop").cpu().numpy(), ref["V"][:, 0, 0, -1]) <= TOL_FLUX, what
+            assert _rel(b.column(out, i, "Vbot").cpu().numpy(), ref["V"][:, 0, 0, 0]) <= TOL_FLUX, what
+    b.close()
+
+
+def test_batch_rejects_bad_descriptors(engine):
+    import torch
+    from ocotillo_b200 import OcoError
+    d = _small_batch()
+    with pytest.raises(OcoError):
+        engine.batch(d["nz"], d["nw"], d["dz"], d["waves"], d["wave_off"], form="plain")
+    bad = d["nz"].copy()
+    bad[3] = 1
+    with pytest.raises(OcoError):
+        engine.batch(bad, d["nw"], d["dz"], d["waves"], d["wave_off"])
+    off = d["wave_off"].copy()
+    off[0] = len(d["waves"])
+    with pytest.raises(OcoError):
+        engine.batch(d["nz"], d["nw"], d["dz"], d["waves"], off)
+    b = engine.batch(d["nz"], d["nw"], d["dz"], d["waves"], d["wave_off"])
+    dev = torch.device("cuda:0")
+    out = b.alloc(dev)
+    short = torch.zeros(int(d["nz"].sum()) - 1, dtype=torch.float64, device=dev)
+    with pytest.raises(OcoError):
+        b.bind(short, short, out)
+    with pytest.raises(OcoError):
+        b.run()  # not bound
+    with pytest.raises(OcoError):
+        b.set_tiling("packed", 99)
+    b.close()
