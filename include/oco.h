@@ -106,7 +106,7 @@ int oco_set_wavelengths(oco_ctx *ctx, const double *wa_angstrom, int32_t nw);
 
 /* The xy/lambda loop of one block on HOST arrays (reference layout), including the
  * host<->device copies.  Replaces flux_feautrier.f90:160-228 (and the stores at :205,
- * :215-216).  U is required; kappa, V, Vtop, Vbot may be NULL.  Returns OCO_EZEROPIVOT
+ * :215-216).  Any of U, kappa, V, Vtop, Vbot may be NULL (not stored).  Returns OCO_EZEROPIVOT
  * when some (column, wavelength) met an exactly zero pivot (all other results are
  * written; oco_last_error names the first such item). */
 int oco_solve_block(oco_ctx *ctx, const oco_params *p, const double *rho, const double *T,
@@ -114,7 +114,7 @@ int oco_solve_block(oco_ctx *ctx, const oco_params *p, const double *rho, const 
 
 /* Same loop on DEVICE arrays (p->layout selects the output layout), enqueued on `stream`
  * (a cudaStream_t; NULL is the CUDA default stream); returns after enqueueing.  Zero pivots are
- * reported by the next oco_synchronize.  Outputs may be NULL except U.  The inputs must stay
+ * reported by the next oco_synchronize.  Any output may be NULL.  The inputs must stay
  * valid and the outputs untouched until the stream reaches this work. */
 int oco_solve_block_device(oco_ctx *ctx, const oco_params *p, const double *rho,
                            const double *T, double *U, double *kappa, double *V,
@@ -209,8 +209,8 @@ int oco_batch_create(oco_ctx *ctx, const oco_batch_column *cols, int64_t ncol, c
                      oco_batch **batch);
 
 /* Binds the device arrays (element counts for the bounds check of every column's ranges)
- * and captures the batch's launches into a CUDA graph.  kappa, V, Vtop, Vbot may be NULL
- * (then their count is ignored).  Rebinding recaptures. */
+ * and captures the batch's launches into a CUDA graph.  U, kappa, V, Vtop, Vbot may be NULL
+ * (not stored; their count is then ignored).  Rebinding recaptures. */
 int oco_batch_bind(oco_batch *batch, const double *rho, const double *T, int64_t n_in, double *U,
                    int64_t n_u, double *kappa, double *V, int64_t n_kv, double *Vtop, double *Vbot,
                    int64_t n_flux);
@@ -237,6 +237,81 @@ int oco_batch_get_info(const oco_batch *batch, oco_batch_info *info);
 
 /* Releases the batch (waits for its work first). */
 void oco_batch_destroy(oco_batch *batch);
+
+/* ---- Serving loop -----------------------------------------------------------------------
+ * No counterpart in the reference (a batch program that solves one snapshot per run): a
+ * server owns one device and a scheduler thread that takes post-processing jobs (a block of
+ * columns plus its wavelength grid, as for oco_solve_block_device) as they arrive.  Jobs are
+ * admitted first come first served while a job slot is free and the summed device footprint
+ * of admitted jobs stays within the budget; an admitted job's inputs, results and wavelength
+ * tables stay in HBM.  Continuous batching: every admitted job is cut into launches of about
+ * chunk_points mesh*lambda points, and the scheduler keeps two launches in flight per job on
+ * the job's own stream, each persistent grid sized to the job's share of the GPU (full grid /
+ * running jobs), so the work of a job that arrives while others run starts at once and
+ * overlaps theirs on the device.  Results do not depend on the mix: every (column, lambda)
+ * item runs the same arithmetic whatever grid runs it.
+ * Thread safety: all functions may be called from any thread. */
+typedef struct oco_server oco_server;
+
+typedef struct oco_server_config {
+  int32_t device;
+  int32_t max_jobs;      /* job slots (jobs running at once), >= 1 */
+  int32_t max_nz;        /* workspace is sized for nz <= max_nz at creation (larger nz grows it) */
+  int32_t reserved;      /* must be 0 */
+  double budget_bytes;   /* admission limit on the summed footprint of admitted jobs;
+                          * 0: 85% of the device memory free after the workspace */
+  int64_t chunk_points;  /* mesh*lambda points per launch; 0: 2^28 */
+} oco_server_config;
+
+typedef struct oco_job {
+  int32_t nx, ny, nz, nw;
+  double dz;
+  double fully_ionized_T;
+  int32_t form;            /* OCO_FORM_PLAIN, _STABLE or _MIXED (non-grey) */
+  int32_t want_fields;     /* 1: keep U, kappa and V as well as the emergent flux */
+  const double *rho, *T;   /* (nz, ny, nx) reference layout, host or device memory (complete
+                            * when submitted); must stay valid until inputs_consumed is set */
+  const double *waves;     /* nw wavelengths (Angstrom), host memory, copied by submit */
+} oco_job;
+
+#define OCO_JOB_QUEUED 0
+#define OCO_JOB_RUNNING 1
+#define OCO_JOB_DONE 2
+#define OCO_JOB_FAILED 3
+
+typedef struct oco_job_status {
+  int32_t state;           /* OCO_JOB_* */
+  int32_t error;           /* OCO_E* of a failed job (or OCO_EZEROPIVOT on a done job with zero pivots) */
+  int32_t inputs_consumed; /* the job no longer reads rho and T */
+  int32_t reserved;
+  int64_t bytes;           /* device footprint counted by admission */
+  double submit_s, admit_s, done_s; /* host monotonic clock, seconds (0 until reached) */
+} oco_job_status;
+
+int oco_server_create(const oco_server_config *cfg, oco_server **server);
+
+/* Queues a job; returns its id in *job_id.  OCO_EADMIT if its footprint can never fit the
+ * budget, OCO_ECLOSED after oco_server_destroy began. */
+int oco_server_submit(oco_server *server, const oco_job *job, int64_t *job_id);
+
+int oco_server_status(oco_server *server, int64_t job_id, oco_job_status *status);
+
+/* Waits up to timeout_s seconds for the job to finish: OCO_OK when done, OCO_EAGAIN on
+ * timeout, the job's error when it failed. */
+int oco_server_wait(oco_server *server, int64_t job_id, double timeout_s);
+
+/* Copies a done job's results into host arrays (reference layout: Vtop, Vbot (ny, nx, nw);
+ * U (nz+6, ny, nx, nw), kappa and V (nz, ny, nx, nw) when the job kept its fields; any may be
+ * NULL), then releases the job and its device memory. */
+int oco_server_fetch(oco_server *server, int64_t job_id, double *Vtop, double *Vbot, double *U, double *kappa,
+                     double *V);
+
+/* Stops accepting jobs, fails the queued ones with OCO_ECLOSED, finishes the running ones,
+ * joins the scheduler and releases everything (results not fetched are dropped). */
+void oco_server_destroy(oco_server *server);
+
+/* Message of the last failed server call on this thread. */
+const char *oco_server_last_error(void);
 
 #ifdef __cplusplus
 }

@@ -6,10 +6,10 @@ this package is its Python binding (ctypes, with numpy host arrays or torch devi
 tensors).  There is no CPU fallback: if the library is missing, importing the binding
 raises.
 """
-from .engine import (Engine, Batch, OcoError, FORM_PLAIN, FORM_STABLE, FORM_MIXED, LAYOUT_REFERENCE,
+from .engine import (Engine, Batch, Server, OcoError, FORM_PLAIN, FORM_STABLE, FORM_MIXED, LAYOUT_REFERENCE,
                      LAYOUT_LAMBDA_FASTEST, TILING_WARP_COLUMN, TILING_PACKED, calc_wavelength,
                      dense_batch_offsets, load_library)
 
-__all__ = ["Engine", "Batch", "OcoError", "FORM_PLAIN", "FORM_STABLE", "FORM_MIXED", "LAYOUT_REFERENCE",
+__all__ = ["Engine", "Batch", "Server", "OcoError", "FORM_PLAIN", "FORM_STABLE", "FORM_MIXED", "LAYOUT_REFERENCE",
            "LAYOUT_LAMBDA_FASTEST", "TILING_WARP_COLUMN", "TILING_PACKED", "calc_wavelength",
            "dense_batch_offsets", "load_library"]

@@ -302,7 +302,7 @@ __device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int i
   Lam L;
   if (!GREY) load_lam(L, a.lam, iw, a.nw);
   const int64_t idx = (a.layout == 0) ? (int64_t)iw * a.ld_col + a.c_off + cl : (a.c_off + cl) * a.nw + iw;
-  double *Ub = a.U + idx * a.U_is;
+  double *Ub = a.U ? a.U + idx * a.U_is : nullptr; /* NULL: U not stored (flux-only runs) */
   double *Kb = (a.K && active) ? a.K + idx * a.K_is : nullptr;
   double *Vb = (a.V && active) ? a.V + idx * a.V_is : nullptr;
   const double dz = a.dz, dz2 = a.dz2;
@@ -389,7 +389,7 @@ __device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int i
      * stencil on U, accurate where U's differences are below its resolution. */
     const int n = nz;
     double Un = u; /* U_{n-1} */
-    Ub[(3 + n - 1) * uz] = Un;
+    if (Ub) Ub[(3 + n - 1) * uz] = Un;
     double Uk[3], Dt[3];
     for (int t = 0; t < 3; t++) {
       const int k = n - 2 - t;
@@ -397,12 +397,12 @@ __device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int i
       Dt[t] = uf - qs[k * ss] * Un;
       Un = uf - gam[(k + 1) * ss] * Un;
       Uk[t] = Un;
-      Ub[(3 + k) * uz] = Un;
+      if (Ub) Ub[(3 + k) * uz] = Un;
     }
     const double fn = u;
-    Ub[(n + 3) * uz] = 2.0 * fn - Uk[0];
-    Ub[(n + 4) * uz] = 2.0 * fn - Uk[1];
-    Ub[(n + 5) * uz] = 2.0 * fn - Uk[2];
+    if (Ub) Ub[(n + 3) * uz] = 2.0 * fn - Uk[0];
+    if (Ub) Ub[(n + 4) * uz] = 2.0 * fn - Uk[1];
+    if (Ub) Ub[(n + 5) * uz] = 2.0 * fn - Uk[2];
     double d0 = Dt[2], d1 = Dt[1], d2 = Dt[0], d3 = Dt[0], d4 = Dt[1], d5 = Dt[2];
     auto emitD = [&](int j) -> double {
       const double s1 = d2 + d3;
@@ -418,7 +418,7 @@ __device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int i
     auto stepD = [&](int k, double uf, double qk, double gk1) {
       const double Dk = uf - qk * Un;
       Un = uf - gk1 * Un;
-      Ub[(3 + k) * uz] = Un;
+      if (Ub) Ub[(3 + k) * uz] = Un;
       U3 = U2; U2 = U1; U1 = U0; U0 = Un;
       d5 = d4; d4 = d3; d3 = d2; d2 = d1; d1 = d0; d0 = Dk;
       emitD(k + 3);
@@ -436,9 +436,9 @@ __device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int i
       for (int q = 0; q < 8; q++) stepD(k - q, ub[q], qb[q], gb[q]);
     }
     for (; k >= 0; k--) stepD(k, uu[k * ss], qs[k * ss], gam[(k + 1) * ss]);
-    Ub[2 * uz] = 2.0 * U0 - U1;
-    Ub[1 * uz] = 2.0 * U0 - U2;
-    Ub[0] = 2.0 * U0 - U3;
+    if (Ub) Ub[2 * uz] = 2.0 * U0 - U1;
+    if (Ub) Ub[1 * uz] = 2.0 * U0 - U2;
+    if (Ub) Ub[0] = 2.0 * U0 - U3;
     const double D0 = d0, D1 = d1, D2 = d2;
     d5 = d4; d4 = d3; d3 = d2; d2 = d1; d1 = d0; d0 = D0;
     emitD(2);
@@ -458,14 +458,14 @@ __device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int i
     double u2 = uu[(n - 2) * ss] - gam[(n - 1) * ss] * u1;
     double u3 = uu[(n - 3) * ss] - gam[(n - 2) * ss] * u2;
     double u4 = uu[(n - 4) * ss] - gam[(n - 3) * ss] * u3;
-    Ub[(3 + n - 1) * uz] = u1;
-    Ub[(3 + n - 2) * uz] = u2;
-    Ub[(3 + n - 3) * uz] = u3;
-    Ub[(3 + n - 4) * uz] = u4;
+    if (Ub) Ub[(3 + n - 1) * uz] = u1;
+    if (Ub) Ub[(3 + n - 2) * uz] = u2;
+    if (Ub) Ub[(3 + n - 3) * uz] = u3;
+    if (Ub) Ub[(3 + n - 4) * uz] = u4;
     double g1 = 2.0 * u1 - u2, g2 = 2.0 * u1 - u3, g3 = 2.0 * u1 - u4;
-    Ub[(n + 3) * uz] = g1;
-    Ub[(n + 4) * uz] = g2;
-    Ub[(n + 5) * uz] = g3;
+    if (Ub) Ub[(n + 3) * uz] = g1;
+    if (Ub) Ub[(n + 4) * uz] = g2;
+    if (Ub) Ub[(n + 5) * uz] = g3;
     double w0 = u4, w1 = u3, w2 = u2, w3 = u1, w4 = g1, w5 = g2, w6 = g3;
     vtop = emitV(n - 1, o1s[(n - 1) * ss], w0, w1, w2, w4, w5, w6);
     int kk = n - 5;
@@ -481,21 +481,21 @@ __device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int i
 #pragma unroll
       for (int q = 0; q < 8; q++) {
         double Uk = ub[q] - gb[q] * w0;
-        Ub[(3 + kk - q) * uz] = Uk;
+        if (Ub) Ub[(3 + kk - q) * uz] = Uk;
         w6 = w5; w5 = w4; w4 = w3; w3 = w2; w2 = w1; w1 = w0; w0 = Uk;
         emitV(kk - q + 3, ob[q], w0, w1, w2, w4, w5, w6);
       }
     }
     for (; kk >= 0; kk--) {
       double Uk = uu[kk * ss] - gam[(kk + 1) * ss] * w0;
-      Ub[(3 + kk) * uz] = Uk;
+      if (Ub) Ub[(3 + kk) * uz] = Uk;
       w6 = w5; w5 = w4; w4 = w3; w3 = w2; w2 = w1; w1 = w0; w0 = Uk;
       emitV(kk + 3, o1s[(kk + 3) * ss], w0, w1, w2, w4, w5, w6);
     }
     double b1 = 2.0 * w0 - w1, b2 = 2.0 * w0 - w2, b3 = 2.0 * w0 - w3;
-    Ub[2 * uz] = b1;
-    Ub[1 * uz] = b2;
-    Ub[0] = b3;
+    if (Ub) Ub[2 * uz] = b1;
+    if (Ub) Ub[1 * uz] = b2;
+    if (Ub) Ub[0] = b3;
     w6 = w5; w5 = w4; w4 = w3; w3 = w2; w2 = w1; w1 = w0; w0 = b1;
     emitV(2, o1s[2 * ss], w0, w1, w2, w4, w5, w6);
     w6 = w5; w5 = w4; w4 = w3; w3 = w2; w2 = w1; w1 = w0; w0 = b2;
@@ -511,7 +511,8 @@ __device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int i
       f[n1 - i] = 2.0 * f[n1] - f[n1 + i];
       f[n2 + i] = 2.0 * f[n2] - f[n2 - i];
     }
-    for (int m = 0; m < nz + 6; m++) Ub[m * uz] = f[m];
+    if (Ub)
+      for (int m = 0; m < nz + 6; m++) Ub[m * uz] = f[m];
     for (int j = 0; j < nz; j++) {
       int c = n1 + j;
       double df = (1.0 / 60.0) * (((45.0 * (f[c + 1] - f[c - 1])) - 9.0 * (f[c + 2] - f[c - 2])) +

@@ -140,7 +140,7 @@ struct MItem {
   int nz, nw, iw;
   float dzf, ldz2;  /* dz and log2(dz^2) */
   double dz1;       /* 1/dz */
-  double *U;        /* U of z = 0 (ghost zone 0), stride uz; written only when active */
+  double *U;        /* U of z = 0 (ghost zone 0), stride uz, or NULL; written only when active */
   double *K, *V;    /* kappa and V of z = 0 or NULL, strides kz, vz */
   int64_t uz, kz, vz;
   double *vtop, *vbot; /* emergent-flux destinations or NULL */
@@ -157,7 +157,7 @@ __device__ __forceinline__ MItem block_item(const MixedArgs &a, int64_t cl, int 
   it.ldz2 = a.ldz2;
   it.dz1 = 1.0 / a.dz;
   const int64_t idx = (a.layout == 0) ? (int64_t)iw * a.ld_col + a.c_off + cl : (a.c_off + cl) * a.nw + iw;
-  it.U = a.U + idx * a.U_is;
+  it.U = a.U ? a.U + idx * a.U_is : nullptr;
   it.K = a.K ? a.K + idx * a.K_is : nullptr;
   it.V = a.V ? a.V + idx * a.V_is : nullptr;
   it.uz = a.U_zs;
@@ -178,7 +178,7 @@ __device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa
   const int nz = it.nz;
   Lam32 L;
   load_lam32(L, it.lam, it.iw, it.nw);
-  double *Ub = it.U;
+  double *Ub = active ? it.U : nullptr;
   double *Kb = active ? it.K : nullptr;
   double *Vb = active ? it.V : nullptr;
   const float dzf = it.dzf, ldz2 = it.ldz2;
@@ -227,7 +227,7 @@ __device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa
   const double dz1 = it.dz1;
   const int64_t uz = it.uz;
   XF Un = u; /* U_{n-1} */
-  Ub[(int64_t)(3 + n - 1) * uz] = xtod(Un);
+  if (Ub) Ub[(int64_t)(3 + n - 1) * uz] = xtod(Un);
   double vtop = 0.0, vbot = 0.0;
   if (nz >= 4) {
     /* window of differences d0..d5 = D_k..D_{k+5}; V_{k+3} from it */
@@ -250,15 +250,17 @@ __device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa
       XF Dj = xaxpy(uj, 1.0f, Un, -qk);
       Un = xaxpy(uj, 1.0f, Un, g1);
       Uk[t] = xtod(Un);
-      Ub[(int64_t)(3 + k) * uz] = Uk[t];
+      if (Ub) Ub[(int64_t)(3 + k) * uz] = Uk[t];
       Dt[t] = xtod(Dj);
     }
     const float o1_nm2 = o1t[0], o1_nm3 = o1t[1], o1_nm4 = o1t[2];
     /* top ghosts f(n2+i) = 2 f(n2) - f(n2-i) */
     const double fn = xtod(u);
-    Ub[(int64_t)(n + 3) * uz] = 2.0 * fn - Uk[0];
-    Ub[(int64_t)(n + 4) * uz] = 2.0 * fn - Uk[1];
-    Ub[(int64_t)(n + 5) * uz] = 2.0 * fn - Uk[2];
+    if (Ub) {
+      Ub[(int64_t)(n + 3) * uz] = 2.0 * fn - Uk[0];
+      Ub[(int64_t)(n + 4) * uz] = 2.0 * fn - Uk[1];
+      Ub[(int64_t)(n + 5) * uz] = 2.0 * fn - Uk[2];
+    }
     /* window for V_{n-1}: D_{n-4} .. D_{n+1} = Dt[2], Dt[1], Dt[0], D_{n-1}=Dt[0], D_n=Dt[1], D_{n+1}=Dt[2] */
     d0 = Dt[2]; d1 = Dt[1]; d2 = Dt[0]; d3 = Dt[0]; d4 = Dt[1]; d5 = Dt[2];
     auto emit = [&](int j, float o1j) -> double {
@@ -271,6 +273,7 @@ __device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa
       return v;
     };
     vtop = emit(n - 1, nx4_top_o1);
+    double U0 = Uk[2], U1 = Uk[1], U2 = Uk[0], U3 = fn; /* the four lowest U seen so far */
     /* o1 ring: r1, r2, r3 = 1/kappa of k+1, k+2, k+3 before step k */
     float r1 = o1_nm4, r2 = o1_nm3, r3 = o1_nm2;
     auto step = [&](int k, const float4 &w) {
@@ -281,7 +284,9 @@ __device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa
       uj.e = (int)w.w;
       XF Dj = xaxpy(uj, 1.0f, Un, -qk);
       Un = xaxpy(uj, 1.0f, Un, g1);
-      Ub[(int64_t)(3 + k) * uz] = xtod(Un);
+      const double Uv = xtod(Un);
+      if (Ub) Ub[(int64_t)(3 + k) * uz] = Uv;
+      U3 = U2; U2 = U1; U1 = U0; U0 = Uv;
       d5 = d4; d4 = d3; d3 = d2; d2 = d1; d1 = d0; d0 = xtod(Dj);
       emit(k + 3, r3);
       r3 = r2; r2 = r1; r1 = w.y;
@@ -297,10 +302,11 @@ __device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa
     }
     for (; k >= 0; k--) step(k, s4[(int64_t)k * ss]);
     /* bottom ghosts f(n1-i) = 2 f(n1) - f(n1+i); ghost differences mirror D_0, D_1, D_2 */
-    const double f0 = Ub[(int64_t)3 * uz], f1 = Ub[(int64_t)4 * uz], f2 = Ub[(int64_t)5 * uz], f3 = Ub[(int64_t)6 * uz];
-    Ub[(int64_t)2 * uz] = 2.0 * f0 - f1;
-    Ub[(int64_t)1 * uz] = 2.0 * f0 - f2;
-    Ub[0] = 2.0 * f0 - f3;
+    if (Ub) {
+      Ub[(int64_t)2 * uz] = 2.0 * U0 - U1;
+      Ub[(int64_t)1 * uz] = 2.0 * U0 - U2;
+      Ub[0] = 2.0 * U0 - U3;
+    }
     const double D0 = d0, D1 = d1, D2 = d2;
     d5 = d4; d4 = d3; d3 = d2; d2 = d1; d1 = d0; d0 = D0; /* D_{-1} = D_0 */
     emit(2, r3);
@@ -325,7 +331,8 @@ __device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa
       f[n1 - i] = 2.0 * f[n1] - f[n1 + i];
       f[n2 + i] = 2.0 * f[n2] - f[n2 - i];
     }
-    for (int m = 0; m < nz + 6; m++) Ub[(int64_t)m * uz] = f[m];
+    if (Ub)
+      for (int m = 0; m < nz + 6; m++) Ub[(int64_t)m * uz] = f[m];
     for (int j = 0; j < nz; j++) {
       const int c = n1 + j;
       const double df = (1.0 / 60.0) * (((45.0 * (f[c + 1] - f[c - 1])) - 9.0 * (f[c + 2] - f[c - 2])) + (f[c + 3] - f[c - 3]));
@@ -432,12 +439,12 @@ __device__ __forceinline__ MItem batch_item(const MixedBatchArgs &b, const MBatc
   it.ldz2 = c.ldz2;
   it.dz1 = c.dz1;
   if (b.layout == 0) { /* per column [lambda][z] (z fastest) */
-    it.U = b.U + c.u_off + (int64_t)iw * (c.nz + 6);
+    it.U = b.U ? b.U + c.u_off + (int64_t)iw * (c.nz + 6) : nullptr;
     it.K = b.K ? b.K + c.kv_off + (int64_t)iw * c.nz : nullptr;
     it.V = b.V ? b.V + c.kv_off + (int64_t)iw * c.nz : nullptr;
     it.uz = it.kz = it.vz = 1;
   } else { /* per column [z][lambda] */
-    it.U = b.U + c.u_off + iw;
+    it.U = b.U ? b.U + c.u_off + iw : nullptr;
     it.K = b.K ? b.K + c.kv_off + iw : nullptr;
     it.V = b.V ? b.V + c.kv_off + iw : nullptr;
     it.uz = it.kz = it.vz = c.nw;

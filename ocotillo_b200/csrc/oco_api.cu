@@ -263,6 +263,7 @@ static int prepare_solve(oco_ctx *c, int form, int grey, int64_t nitems, int nz,
   int bps = mixed ? solve_mixed_max_blocks_per_sm(kSolveThreads)
                   : solve_fp64_max_blocks_per_sm(form == OCO_FORM_STABLE ? 1 : 0, grey, kSolveThreads);
   int64_t maxb = (int64_t)bps * c->num_sms;
+  if (c->max_blocks > 0) maxb = std::min<int64_t>(maxb, c->max_blocks);
   int64_t need = (nitems + kSolveThreads - 1) / kSolveThreads;
   *blocks = (int)std::max<int64_t>(1, std::min(maxb, need));
   size_t slots = (size_t)(*blocks) * kSolveThreads;
@@ -430,7 +431,7 @@ extern "C" int oco_solve_block_device(oco_ctx *c, const oco_params *p, const dou
   int rc = check_params(c, p);
   if (rc) return rc;
   if (p->form == OCO_FORM_MIXED && p->lgrey) return oco_set_err(c, OCO_EINVAL, "the mixed form has no grey variant");
-  if (!rho || !T || !U) return oco_set_err(c, OCO_EINVAL, "rho, T and U are required");
+  if (!rho || !T) return oco_set_err(c, OCO_EINVAL, "rho and T are required");
   CU(cudaSetDevice(c->device));
   cudaStream_t s = (cudaStream_t)stream; /* NULL is the CUDA default stream */
   const int64_t ncol = (int64_t)p->nx * p->ny;
@@ -461,12 +462,57 @@ extern "C" int oco_solve_block_device(oco_ctx *c, const oco_params *p, const dou
   return OCO_OK;
 }
 
+int oco_ctx_run_columns(oco_ctx *c, const oco_params *p, const double *rho, const double *T, int64_t c0, int64_t nb,
+                        double *U, double *kappa, double *V, double *Vtop, double *Vbot, int max_blocks,
+                        cudaStream_t s) {
+  CU(c->pil.ensure((size_t)nb * p->nz * record_bytes(p->form)));
+  SolveArgs a{};
+  fill_strides(a, p, p->layout, (int64_t)p->nx * p->ny);
+  a.nz = p->nz;
+  a.nw = p->nw;
+  a.dz = p->dz;
+  a.dz1 = 1.0 / p->dz;
+  a.dz2 = p->dz * p->dz;
+  a.sigma_grey = p->sigma_grey;
+  a.U = U;
+  a.K = kappa;
+  a.V = V;
+  a.Vtop = Vtop;
+  a.Vbot = Vbot;
+  a.c_off = c0;
+  c->max_blocks = max_blocks;
+  const int rc = run_chunk(c, p, rho + c0 * p->nz, T + c0 * p->nz, nb, a, s);
+  c->max_blocks = 0;
+  return rc;
+}
+
+int oco_ctx_reset_status(oco_ctx *c, cudaStream_t s) {
+  c->status_pending = false;
+  return reset_status(c, s);
+}
+
+int oco_ctx_read_status(oco_ctx *c, cudaStream_t s, const oco_params *p) { return read_status(c, s, p); }
+
+int oco_ctx_check_params(oco_ctx *c, const oco_params *p) {
+  const int rc = check_params(c, p);
+  if (rc) return rc;
+  if (p->form == OCO_FORM_MIXED && p->lgrey) return oco_set_err(c, OCO_EINVAL, "the mixed form has no grey variant");
+  return OCO_OK;
+}
+
+int oco_ctx_full_blocks(oco_ctx *c, int form, int grey) {
+  const int bps = form == OCO_FORM_MIXED ? solve_mixed_max_blocks_per_sm(kSolveThreads)
+                                         : solve_fp64_max_blocks_per_sm(form == OCO_FORM_STABLE ? 1 : 0, grey,
+                                                                        kSolveThreads);
+  return bps * c->num_sms;
+}
+
 extern "C" int oco_solve_block(oco_ctx *c, const oco_params *p, const double *rho, const double *T, double *U,
                                double *kappa, double *V, double *Vtop, double *Vbot) {
   int rc = check_params(c, p);
   if (rc) return rc;
   if (p->form == OCO_FORM_MIXED && p->lgrey) return oco_set_err(c, OCO_EINVAL, "the mixed form has no grey variant");
-  if (!rho || !T || !U) return oco_set_err(c, OCO_EINVAL, "rho, T and U are required");
+  if (!rho || !T) return oco_set_err(c, OCO_EINVAL, "rho and T are required");
   CU(cudaSetDevice(c->device));
   const int64_t ncol = (int64_t)p->nx * p->ny;
   const int nz = p->nz, nw = p->nw, mz = nz + 6;
@@ -475,7 +521,7 @@ extern "C" int oco_solve_block(oco_ctx *c, const oco_params *p, const double *rh
   for (auto &st : c->stage) {
     CU(st.rho.ensure((size_t)ch * nz * sizeof(double)));
     CU(st.T.ensure((size_t)ch * nz * sizeof(double)));
-    CU(st.U.ensure((size_t)ch * mz * nw * sizeof(double)));
+    if (U) CU(st.U.ensure((size_t)ch * mz * nw * sizeof(double)));
     if (kappa) CU(st.K.ensure((size_t)ch * nz * nw * sizeof(double)));
     if (V) CU(st.V.ensure((size_t)ch * nz * nw * sizeof(double)));
     if (Vtop) CU(st.top.ensure((size_t)ch * nw * sizeof(double)));
@@ -501,7 +547,7 @@ extern "C" int oco_solve_block(oco_ctx *c, const oco_params *p, const double *rh
     CU(cudaMemcpyAsync(st.T.p, T + c0 * nz, (size_t)nb * nz * sizeof(double), cudaMemcpyHostToDevice,
                        c->stream));
     fill_strides(a, p, OCO_LAYOUT_REFERENCE, nb);
-    a.U = st.U.as<double>();
+    a.U = U ? st.U.as<double>() : nullptr;
     a.K = kappa ? st.K.as<double>() : nullptr;
     a.V = V ? st.V.as<double>() : nullptr;
     a.Vtop = Vtop ? st.top.as<double>() : nullptr;
@@ -515,7 +561,7 @@ extern "C" int oco_solve_block(oco_ctx *c, const oco_params *p, const double *rh
     CU(cudaStreamWaitEvent(c->copy, ready, 0));
     CU(cudaEventDestroy(ready));
     const size_t dp_u = (size_t)ncol * mz * sizeof(double), sp_u = (size_t)nb * mz * sizeof(double);
-    CU(cudaMemcpy2DAsync(U + c0 * mz, dp_u, st.U.p, sp_u, sp_u, nw, cudaMemcpyDeviceToHost, c->copy));
+    if (U) CU(cudaMemcpy2DAsync(U + c0 * mz, dp_u, st.U.p, sp_u, sp_u, nw, cudaMemcpyDeviceToHost, c->copy));
     const size_t dp_k = (size_t)ncol * nz * sizeof(double), sp_k = (size_t)nb * nz * sizeof(double);
     if (kappa) CU(cudaMemcpy2DAsync(kappa + c0 * nz, dp_k, st.K.p, sp_k, sp_k, nw, cudaMemcpyDeviceToHost, c->copy));
     if (V) CU(cudaMemcpy2DAsync(V + c0 * nz, dp_k, st.V.p, sp_k, sp_k, nw, cudaMemcpyDeviceToHost, c->copy));

@@ -256,10 +256,9 @@ extern "C" int oco_batch_bind(oco_batch *b, const double *rho, const double *T, 
                               double *kappa, double *V, int64_t n_kv, double *Vtop, double *Vbot, int64_t n_flux) {
   if (!b) return oco_set_err(nullptr, OCO_EINVAL, "oco_batch_bind: NULL batch");
   oco_ctx *c = b->c;
-  if (!rho || !T || !U) return oco_set_err(c, OCO_EINVAL, "oco_batch_bind: rho, T and U are required");
-  if (n_in < b->need_in || n_u < b->need_u)
-    return oco_set_err(c, OCO_EINVAL, "oco_batch_bind: inputs need %lld elements and U %lld",
-                       (long long)b->need_in, (long long)b->need_u);
+  if (!rho || !T) return oco_set_err(c, OCO_EINVAL, "oco_batch_bind: rho and T are required");
+  if (n_in < b->need_in) return oco_set_err(c, OCO_EINVAL, "oco_batch_bind: inputs need %lld elements", (long long)b->need_in);
+  if (U && n_u < b->need_u) return oco_set_err(c, OCO_EINVAL, "oco_batch_bind: U needs %lld elements", (long long)b->need_u);
   if ((kappa || V) && n_kv < b->need_kv)
     return oco_set_err(c, OCO_EINVAL, "oco_batch_bind: kappa and V need %lld elements", (long long)b->need_kv);
   if ((Vtop || Vbot) && n_flux < b->need_flux)

@@ -59,6 +59,7 @@ struct oco_ctx {
   Stage stage[2];
   int64_t launches = 0;
   size_t budget_bytes = 8ull << 30; /* chunk budget for pillars + staged outputs */
+  int max_blocks = 0;               /* cap on the persistent grid (0: occupancy limit x SMs) */
   /* kernel timing (oco_set_profiling) */
   bool prof = false;
   /* device-array calls defer the zero-pivot check to oco_synchronize */
@@ -78,6 +79,22 @@ struct oco_ctx {
     return e;
   }
 };
+
+/* Enqueues columns [c0, c0 + nb) of a block on stream s: the record kernel and the persistent
+ * solve, with the solve grid capped at max_blocks (0: no cap).  Outputs (device arrays of the
+ * whole block, layout p->layout; any may be NULL) are written for those columns only.  Zero
+ * pivots and timeouts accumulate in the context's status until oco_ctx_read_status. */
+int oco_ctx_run_columns(oco_ctx *c, const oco_params *p, const double *rho, const double *T, int64_t c0, int64_t nb,
+                        double *U, double *kappa, double *V, double *Vtop, double *Vbot, int max_blocks,
+                        cudaStream_t s);
+/* Clears the context's status (zero-pivot count, first bad item, timeout flag) on stream s. */
+int oco_ctx_reset_status(oco_ctx *c, cudaStream_t s);
+/* Reads the status after the work on s: OCO_OK, OCO_EZEROPIVOT or OCO_ETIMEDOUT. */
+int oco_ctx_read_status(oco_ctx *c, cudaStream_t s, const oco_params *p);
+/* Validates p and the context's wavelength table for it (OCO_OK or an error code). */
+int oco_ctx_check_params(oco_ctx *c, const oco_params *p);
+/* Full device-resident persistent grid of a form (blocks). */
+int oco_ctx_full_blocks(oco_ctx *c, int form, int grey);
 
 /* Records a message for oco_last_error (on the context, if any, and the calling thread) and
  * returns code. */

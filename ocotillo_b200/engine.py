@@ -59,6 +59,27 @@ class OcoBatchInfo(ctypes.Structure):
 
 TILING_WARP_COLUMN, TILING_PACKED = 0, 1
 
+
+class OcoServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("max_jobs", ctypes.c_int32), ("max_nz", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("budget_bytes", ctypes.c_double), ("chunk_points", ctypes.c_int64)]
+
+
+class OcoJob(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32), ("nw", ctypes.c_int32),
+                ("dz", ctypes.c_double), ("fully_ionized_T", ctypes.c_double), ("form", ctypes.c_int32),
+                ("want_fields", ctypes.c_int32), ("rho", ctypes.c_void_p), ("T", ctypes.c_void_p),
+                ("waves", ctypes.c_void_p)]
+
+
+class OcoJobStatus(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int32), ("error", ctypes.c_int32), ("inputs_consumed", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("bytes", ctypes.c_int64), ("submit_s", ctypes.c_double),
+                ("admit_s", ctypes.c_double), ("done_s", ctypes.c_double)]
+
+
+JOB_STATES = ("queued", "running", "done", "failed")
+
 _LIB = None
 _DP = ctypes.POINTER(ctypes.c_double)
 
@@ -98,6 +119,13 @@ def load_library(path=None):
         "oco_batch_wait": (I, [V]),
         "oco_batch_get_info": (I, [V, ctypes.POINTER(OcoBatchInfo)]),
         "oco_batch_destroy": (None, [V]),
+        "oco_server_create": (I, [ctypes.POINTER(OcoServerConfig), ctypes.POINTER(V)]),
+        "oco_server_submit": (I, [V, ctypes.POINTER(OcoJob), ctypes.POINTER(ctypes.c_int64)]),
+        "oco_server_status": (I, [V, ctypes.c_int64, ctypes.POINTER(OcoJobStatus)]),
+        "oco_server_wait": (I, [V, ctypes.c_int64, D]),
+        "oco_server_fetch": (I, [V, ctypes.c_int64, _DP, _DP, _DP, _DP, _DP]),
+        "oco_server_destroy": (None, [V]),
+        "oco_server_last_error": (ctypes.c_char_p, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -177,7 +205,7 @@ class Engine:
         out = dict(out or {})
         shapes = {"U": (nw, nx, ny, nz + 6), "kappa": (nw, nx, ny, nz), "V": (nw, nx, ny, nz),
                   "Vtop": (nw, nx, ny), "Vbot": (nw, nx, ny)}
-        for k in set(want) | {"U"}:
+        for k in set(want):
             if k not in out:
                 out[k] = np.empty(shapes[k])
         prm = self.params(rho.shape, nw, dz, fully_ionized_T, lgrey, sigma_grey, form)
@@ -192,8 +220,8 @@ class Engine:
     def solve_block_device(self, rho, T, dz, out, fully_ionized_T=2e4, lgrey=False, sigma_grey=0.4,
                            form="plain", layout=LAYOUT_REFERENCE, stream=None):
         """Same loop on torch CUDA tensors (float64, contiguous), enqueued on `stream`
-        (default: torch's current stream).  `out` maps 'U' (required), 'kappa', 'V', 'Vtop',
-        'Vbot' to preallocated tensors of the layout's shapes."""
+        (default: torch's current stream).  `out` maps any of 'U', 'kappa', 'V', 'Vtop', 'Vbot'
+        to preallocated tensors of the layout's shapes (absent names are not stored)."""
         import torch
         nx, ny, nz = rho.shape
         nw = 1 if lgrey else self.nw
@@ -276,15 +304,12 @@ class Batch:
         eng._check(rc)
         self.arrays = None
 
-    def alloc(self, device="cuda", want=("kappa", "V", "Vtop", "Vbot")):
+    def alloc(self, device="cuda", want=("U", "kappa", "V", "Vtop", "Vbot")):
         """Allocates output tensors of the dense packing."""
         import torch
         o = self.offsets
-        out = {"U": torch.empty(o["n_u"], dtype=torch.float64, device=device)}
-        for k in want:
-            out[k] = torch.empty(o["n_kv"] if k in ("kappa", "V") else o["n_flux"], dtype=torch.float64,
-                                 device=device)
-        return out
+        n = {"U": o["n_u"], "kappa": o["n_kv"], "V": o["n_kv"], "Vtop": o["n_flux"], "Vbot": o["n_flux"]}
+        return {k: torch.empty(n[k], dtype=torch.float64, device=device) for k in want}
 
     def bind(self, rho, T, out):
         """Binds device inputs (dense rho, T) and outputs (dict of U, kappa, V, Vtop, Vbot)."""
@@ -296,8 +321,8 @@ class Batch:
         g = out.get
         n_kv = (g("kappa") if g("kappa") is not None else g("V"))
         n_fl = (g("Vtop") if g("Vtop") is not None else g("Vbot"))
-        rc = self.lib.oco_batch_bind(self.h, p(rho), p(T), min(rho.numel(), T.numel()), p(out["U"]),
-                                     out["U"].numel(), p(g("kappa")), p(g("V")),
+        rc = self.lib.oco_batch_bind(self.h, p(rho), p(T), min(rho.numel(), T.numel()), p(g("U")),
+                                     g("U").numel() if g("U") is not None else 0, p(g("kappa")), p(g("V")),
                                      n_kv.numel() if n_kv is not None else 0, p(g("Vtop")), p(g("Vbot")),
                                      n_fl.numel() if n_fl is not None else 0)
         self.eng._check(rc)
@@ -352,6 +377,80 @@ class Batch:
         if self.h:
             self.lib.oco_batch_destroy(self.h)
             self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Serving loop (include/oco.h, oco_server_*): jobs (a block of columns plus its wavelength
+    grid) are admitted as job slots and device memory free up, and their launches overlap on
+    the device.  Inputs are numpy float64 arrays (nx, ny, nz) or torch CUDA float64 tensors of
+    that shape; results come back as numpy arrays in the reference layout."""
+
+    def __init__(self, device=0, max_jobs=4, max_nz=0, budget_bytes=0.0, chunk_points=0):
+        self.lib = load_library()
+        self.h = ctypes.c_void_p()
+        cfg = OcoServerConfig(int(device), int(max_jobs), int(max_nz), 0, float(budget_bytes), int(chunk_points))
+        self._check(self.lib.oco_server_create(ctypes.byref(cfg), ctypes.byref(self.h)))
+        self._jobs = {}
+
+    def _check(self, rc):
+        if rc:
+            raise OcoError(rc, self.lib.oco_server_last_error().decode())
+
+    @staticmethod
+    def _addr(a):
+        if isinstance(a, np.ndarray):
+            assert a.dtype == np.float64 and a.flags.c_contiguous
+            return a.ctypes.data
+        assert a.is_cuda and a.is_contiguous() and str(a.dtype) == "torch.float64"
+        return a.data_ptr()
+
+    def submit(self, rho, T, waves, dz, form="mixed", fully_ionized_T=2e4, want_fields=False):
+        """Queues a job; returns its id.  rho and T are referenced until the job is fetched."""
+        nx, ny, nz = rho.shape
+        w = np.ascontiguousarray(np.atleast_1d(waves), dtype=np.float64)
+        job = OcoJob(nx, ny, nz, w.size, float(dz), float(fully_ionized_T),
+                     _FORMS[form] if isinstance(form, str) else int(form), int(bool(want_fields)),
+                     self._addr(rho), self._addr(T), w.ctypes.data)
+        jid = ctypes.c_int64()
+        self._check(self.lib.oco_server_submit(self.h, ctypes.byref(job), ctypes.byref(jid)))
+        self._jobs[jid.value] = (rho, T, (nx, ny, nz, w.size), bool(want_fields))
+        return jid.value
+
+    def status(self, jid):
+        st = OcoJobStatus()
+        self._check(self.lib.oco_server_status(self.h, int(jid), ctypes.byref(st)))
+        return {"state": JOB_STATES[st.state], "error": st.error, "inputs_consumed": bool(st.inputs_consumed),
+                "bytes": st.bytes, "submit_s": st.submit_s, "admit_s": st.admit_s, "done_s": st.done_s}
+
+    def wait(self, jid, timeout=3600.0):
+        self._check(self.lib.oco_server_wait(self.h, int(jid), float(timeout)))
+
+    def fetch(self, jid, fields=None):
+        """Results of a done job as numpy arrays: Vtop, Vbot (nw, nx, ny) and, if the job kept
+        them (or fields=True), U (nw, nx, ny, nz+6), kappa and V (nw, nx, ny, nz).  Releases the job."""
+        _, _, (nx, ny, nz, nw), kept = self._jobs[jid]
+        fields = kept if fields is None else fields
+        out = {"Vtop": np.empty((nw, nx, ny)), "Vbot": np.empty((nw, nx, ny))}
+        if fields:
+            out["U"] = np.empty((nw, nx, ny, nz + 6))
+            out["kappa"] = np.empty((nw, nx, ny, nz))
+            out["V"] = np.empty((nw, nx, ny, nz))
+        self._check(self.lib.oco_server_fetch(self.h, int(jid), _ptr(out["Vtop"]), _ptr(out["Vbot"]),
+                                              _ptr(out.get("U")), _ptr(out.get("kappa")), _ptr(out.get("V"))))
+        del self._jobs[jid]
+        return out
+
+    def close(self):
+        if self.h:
+            self.lib.oco_server_destroy(self.h)
+            self.h = ctypes.c_void_p()
+            self._jobs.clear()
 
     def __del__(self):
         try:
