@@ -1,5 +1,5 @@
 #!/usr/bin/env python3
-"""Throughput of the B200 engine in mesh*lambda points per second.
+"""Throughput of the B200 engine in mesh*lambda points per second, mixed vs plain FP64.
 
 Workload (one step = one pass of the hot path over the whole grid): the 'plain FP64 non-grey
 AGN grid' -- nx = ny = 256 columns, nz = 512, nw = 256 log-spaced wavelengths from 100 A to
@@ -7,14 +7,21 @@ AGN grid' -- nx = ny = 256 columns, nz = 512, nw = 256 log-spaced wavelengths fr
 lognormal perturbation (0.3 dex) per cell, T = max(6.1e4 K exp(-z^2/2 sigma_T^2), 2000 K),
 fully_ionized_T = 2e4 K.  Seeded synthetic inputs stand in for a snapshot.
 
-  value  device-resident throughput: inputs in HBM, the full grid solved in column chunks,
-         every U (with ghosts), kappa and V of every chunk written to HBM (rotating chunk
-         buffers; 206 GB of outputs per step do not fit at once) plus the emergent planes.
-  e2e    the same metric through the host-array C-ABI call (oco_solve_block) a Fortran or
-         Python caller makes: pinned host inputs copied in, every output copied back to
-         pinned host memory, per step one batch of columns.
+  value   device-resident throughput of the plain FP64 form (the reference's arithmetic):
+          inputs in HBM, the full grid solved in column chunks, every U (with ghosts), kappa
+          and V of every chunk written to HBM (rotating chunk buffers; 206 GB of outputs per
+          step do not fit at once) plus the emergent planes.
+  mixed   the same step in the mixed-precision form, its ratio to `value`, and its emergent-flux
+          error against the FP64 (stable) form over the whole grid.
+  batch   the batching form: 8192 ragged columns (nz 64-2048, nw 32-1024) in one persistent
+          launch replayed as a CUDA graph, autotuned tiling, mixed form.
+  serving the serving form: a Poisson stream of jobs (nx = ny in {64..512}, nz 128-1024, nw
+          64-512) through the serving loop, p50/p99 latency and throughput, mixed and plain.
+  e2e     the headline metric through the host-array C-ABI call (oco_solve_block) a Fortran
+          or Python caller makes: pinned host inputs copied in, every output copied back to
+          pinned host memory, per step one batch of columns.
   --impl reference   the reference's CPU algorithm (the C restatement of the Fortran loop,
-         glibc math) on all host cores, on a bounded sample of the same workload.
+          glibc math) on all host cores, on a bounded sample of the same workload.
 
 Run: python bench.py [--gpus N] [--steps K] [--warmup W] [--form plain|stable|mixed]
 """
@@ -32,6 +39,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+METRIC = "mesh\u00b7\u03bb points/s + p50/p99 latency: mixed vs plain FP64, 1 B200, \u22641e-4 rel"
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -40,7 +49,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="plain", choices=["plain", "stable", "mixed"])
-    ap.add_argument("--layout", default="reference", choices=["reference", "lambda"])
+    ap.add_argument("--layout", default="lambda", choices=["reference", "lambda"])
     ap.add_argument("--nx", type=int, default=256)
     ap.add_argument("--ny", type=int, default=256)
     ap.add_argument("--nz", type=int, default=512)
@@ -50,6 +59,10 @@ def parse():
     ap.add_argument("--cpu-cols", type=int, default=1024, help="columns in the CPU-baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the mixed, batch and serving measurements")
+    ap.add_argument("--serve-jobs", type=int, default=12)
+    ap.add_argument("--serve-rate", type=float, default=1.5, help="job arrivals per second")
+    ap.add_argument("--batch-cols", type=int, default=8192)
     return ap.parse_args()
 
 
@@ -148,7 +161,7 @@ def run_reference(a):
                 times.append(time.perf_counter() - t0)
     pts = cols * a.nz * a.nw
     v = pts * len(times) / sum(times)
-    line = {"impl": "reference", "metric": "mesh*lambda points/s", "value": v, "unit": "points/s",
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "points/s",
             "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -175,6 +188,232 @@ def pct(xs, q):
     return xs[f] + (xs[c] - xs[f]) * (k - f)
 
 
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+class Grid:
+    """The AGN grid on the device and the chunked step over it (one pass of the hot path)."""
+
+    def __init__(self, a, eng, dev, rank):
+        import torch
+        from ocotillo_b200 import workloads, LAYOUT_REFERENCE, LAYOUT_LAMBDA_FASTEST
+        self.a, self.eng, self.dev = a, eng, dev
+        nx, ny, nz, nw = a.nx, a.ny, a.nz, a.nw
+        self.ncol, self.nz, self.nw, self.mz = nx * ny, nz, nw, nz + 6
+        self.rho_h, self.T_h, self.dz = workloads.agn_block(nx, ny, nz, seed=2 + rank)
+        self.wa = workloads.log_wavelengths(nw)
+        self.rho = torch.from_numpy(self.rho_h).to(dev).reshape(self.ncol, nz)
+        self.T = torch.from_numpy(self.T_h).to(dev).reshape(self.ncol, nz)
+        self.layout = LAYOUT_REFERENCE if a.layout == "reference" else LAYOUT_LAMBDA_FASTEST
+        self.CH = min(a.chunk_cols, self.ncol)
+        assert self.ncol % self.CH == 0, "chunk must divide the grid"
+        self.nchunk = self.ncol // self.CH
+        mk = lambda shape: torch.empty(shape, dtype=torch.float64, device=dev)
+        CH, mz = self.CH, self.mz
+        self.sets = []
+        for _ in range(2):
+            if self.layout == LAYOUT_REFERENCE:
+                o = {"U": mk((nw, CH, mz)), "kappa": mk((nw, CH, nz)), "V": mk((nw, CH, nz))}
+            else:
+                o = {"U": mk((mz, CH, nw)), "kappa": mk((nz, CH, nw)), "V": mk((nz, CH, nw))}
+            self.sets.append(o)
+        self.Vtop, self.Vbot = mk((self.nchunk, nw, CH)), mk((self.nchunk, nw, CH))
+        self.stream = torch.cuda.current_stream(dev)
+        self.zero_pivot = False
+
+    def step(self, form, fields=True):
+        for k in range(self.nchunk):
+            o = dict(self.sets[k % 2]) if fields else {}
+            o["Vtop"], o["Vbot"] = self.Vtop[k], self.Vbot[k]
+            r = self.rho[k * self.CH:(k + 1) * self.CH].reshape(self.CH, 1, self.nz)
+            t = self.T[k * self.CH:(k + 1) * self.CH].reshape(self.CH, 1, self.nz)
+            self.eng.solve_block_device(r, t, self.dz, o, form=form, layout=self.layout, stream=self.stream)
+
+    def sync(self):
+        try:
+            self.eng.synchronize()
+        except Exception as e:
+            if getattr(e, "code", None) != -3:
+                raise
+            self.zero_pivot = True
+
+    def measure(self, form, steps, warmup, world, dist=None, clocks=None):
+        """Times `steps` steps of `form` (after `warmup`), CUDA events on the launching stream,
+        max over ranks.  Returns a dict of the timing and the kernel accounting."""
+        import torch
+        for _ in range(warmup):
+            self.step(form)
+        torch.cuda.synchronize(self.dev)
+        self.sync()
+        self.eng.kernel_times()
+        if clocks:
+            clocks.start()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(self.dev)
+        launches0 = self.eng.kernel_launches
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        evs[0].record(self.stream)
+        for i in range(steps):
+            self.step(form)
+            evs[i + 1].record(self.stream)
+        torch.cuda.synchronize(self.dev)
+        if world > 1:
+            dist.barrier()
+        clk = clocks.stop() if clocks else None
+        launches = self.eng.kernel_launches - launches0
+        self.sync()
+        step_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(steps)]
+        total_ms = evs[0].elapsed_time(evs[-1])
+        solve_ms, pil_ms, nsolve = self.eng.kernel_times()
+        if world > 1:
+            t = torch.tensor([total_ms], device=self.dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms = float(t.item())
+        pts_step = self.ncol * self.nz * self.nw
+        return {"value": world * pts_step * steps / (total_ms / 1e3), "total_ms": total_ms, "step_ms": step_ms,
+                "launches": launches, "solve_ms": solve_ms, "pil_ms": pil_ms, "nsolve": nsolve, "clocks": clk,
+                "pts_step": pts_step}
+
+    def roofline(self, m, steps, form):
+        """Roofline of the dominant kernel (the solve).  Algorithmic bytes per mesh*lambda point:
+        outputs U (nz+6 per nz), kappa, V (8 B each) + the per-column records read once (shared
+        by nw wavelengths).  Algorithmic flops per point: the reference's census, 97 (90
+        add/mul + 7 divisions; transcendentals not counted)."""
+        nz, nw = self.nz, self.nw
+        rec = 26 * 8.0 if form != "mixed" else 40 * 4.0
+        bytes_pt = 8.0 * (self.mz / nz) + 16.0 + rec / nw
+        launch_ms = m["solve_ms"] / max(m["nsolve"], 1)
+        pts_launch = m["pts_step"] * steps / max(m["nsolve"], 1)
+        pk = peaks()
+        hbm_peak = pk.get("hbm_gbs", 6650.0)
+        achieved = bytes_pt * pts_launch / (launch_ms / 1e3) / 1e9
+        flops = 97.0 * pts_launch / (launch_ms / 1e3) / 1e12
+        return {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                "traffic": None, "kernel": "k_solve_staged" if form != "mixed" else "k_solve_mixed_staged",
+                "launch_ms": launch_ms, "points_per_launch": pts_launch, "algorithmic_bytes_per_point": bytes_pt,
+                "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in pk else "fallback",
+                "algorithmic_tflops": flops, "flops_per_point": 97,
+                "solve_share_of_step": m["solve_ms"] / m["total_ms"], "pillars_ms_per_step": m["pil_ms"] / steps}
+
+
+def flux_error(g, form_a, form_b, eps=1e-7, seed=7):
+    """Relative difference of the emergent-flux planes of form_a against form_b (FP64) over the
+    whole grid, with the conditioning mask: s = relative change of form_b's flux when rho is
+    perturbed by eps * N(0,1) relative per cell.  Items with s <= 100 eps are 'conditioned'
+    (their FP64 flux is stable to 100x the perturbation); elsewhere the FP64 flux itself moves
+    by more than 1e-5 under perturbations below float32 resolution of the input."""
+    import torch
+
+    def planes(form, rho=None):
+        if rho is not None:
+            keep, g.rho = g.rho, rho
+        g.step(form, fields=False)
+        g.sync()
+        if rho is not None:
+            g.rho = keep
+        return torch.stack([g.Vtop.clone(), g.Vbot.clone()])
+
+    rb = planes(form_b)
+    gen = torch.Generator(device=g.rho.device)
+    gen.manual_seed(seed)
+    pert = g.rho * (1.0 + eps * torch.randn(g.rho.shape, generator=gen, device=g.rho.device, dtype=g.rho.dtype))
+    rp = planes(form_b, pert)
+    del pert
+    ra = planes(form_a)
+    ok = torch.isfinite(rb) & (rb != 0) & torch.isfinite(rp)
+    rel = ((ra - rb).abs() / rb.abs())[ok]
+    sens = ((rp - rb).abs() / rb.abs())[ok]
+    cond = sens <= 100 * eps
+    sub = lambda x: x.float()[torch.randperm(x.numel(), device=x.device)[:1 << 24]]
+    q = lambda x, p: torch.quantile(sub(x), p).item() if x.numel() else None
+    sensitive = sens > 10 * eps  # items whose FP64 flux responds to the perturbation
+    backward = rel[sensitive] / sens[sensitive] * eps
+    return {"reference_form": form_b, "items": int(rel.numel()),
+            "all": {"max": rel.max().item(), "p99": q(rel, 0.99), "p9999": q(rel, 0.9999),
+                    "frac_above_1e-4": (rel > 1e-4).double().mean().item()},
+            "conditioned": {"definition": f"FP64 flux changes by <= {100 * eps:g} under a {eps:g} relative "
+                                          "random perturbation of rho",
+                            "fraction_of_items": cond.double().mean().item(),
+                            "max": rel[cond].max().item(), "p99": q(rel[cond], 0.99),
+                            "frac_above_1e-4": (rel[cond] > 1e-4).double().mean().item()},
+            "sensitive_items": {"definition": f"FP64 flux changes by > {10 * eps:g} under the perturbation",
+                                "count": int(sensitive.sum()),
+                                "equivalent_rho_perturbation_p50": q(backward, 0.5),
+                                "equivalent_rho_perturbation_max": backward.max().item() if backward.numel() else None}}
+
+
+def measure_batch(a, eng, dev):
+    import torch
+    from ocotillo_b200 import workloads
+    d = workloads.ragged_batch(ncol=a.batch_cols, seed=4)
+    b = eng.batch(d["nz"], d["nw"], d["dz"], d["waves"], d["wave_off"], layout=1)
+    rho = torch.from_numpy(d["rho"]).to(dev)
+    T = torch.from_numpy(d["T"]).to(dev)
+    out = b.alloc(dev)
+    b.bind(rho, T, out)
+    info = b.tune()
+    for _ in range(a.warmup):
+        b.run()
+    b.wait()
+    st = torch.cuda.current_stream(dev)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps + 1)]
+    evs[0].record(st)
+    for i in range(a.steps):
+        b.run(st)
+        evs[i + 1].record(st)
+    b.wait()
+    ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(a.steps)]
+    total = evs[0].elapsed_time(evs[-1])
+    res = {"value": info["npoints"] * a.steps / (total / 1e3), "unit": "points/s", "form": "mixed",
+           "ms_per_run": total / a.steps, "p50_ms": pct(ms, 0.5), "p99_ms": pct(ms, 0.99),
+           "columns": info["ncol"], "points": info["npoints"], "max_nz": info["max_nz"], "max_nw": info["max_nw"],
+           "tiling": info["tiling"], "blocks_per_sm": info["blocks_per_sm"],
+           "tuning": [(c["tiling"], c["blocks_per_sm"], round(c["ms"], 3)) for c in info["candidates"]],
+           "graph_replays": info["graph_launches"], "layout": "per column [z][lambda]",
+           "workload": "8192 columns, nz log-uniform [64,2048], nw log-uniform [32,1024], Athena-style rho/p "
+                       "(0.5 dex lognormal), T = mu m_u p/(rho k), mu=0.6, floor 2000 K (seed 4)"}
+    b.close()
+    del out, rho, T
+    return res
+
+
+def measure_serving(a, dev, form, specs, arrays):
+    """Runs the job stream through a fresh server; latency = done - submit (server clock)."""
+    import torch
+    from ocotillo_b200 import Server, workloads
+    srv = Server(dev.index or 0, max_jobs=4, max_nz=1024, reserve_bytes=24e9)
+    wr, wt, _ = workloads.job_arrays_device({"nx": 8, "ny": 8, "nz": 128, "nw": 64, "rho0": 1e-9, "seed": 1}, dev)
+    jid = srv.submit(wr, wt, workloads.log_wavelengths(64), 1e16 / 127, form=form)  # warm-up
+    srv.wait(jid)
+    srv.fetch(jid)
+    torch.cuda.synchronize(dev)
+    ids = []
+    t0 = time.perf_counter()
+    for spec, (rho, T, dz) in zip(specs, arrays):
+        delay = t0 + spec["arrival_s"] - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        ids.append(srv.submit(rho, T, workloads.log_wavelengths(spec["nw"]), dz, form=form))
+    lat, queue, first, last, pts = [], [], None, None, 0
+    for spec, jid in zip(specs, ids):
+        srv.wait(jid, 3600.0)
+        st = srv.status(jid)
+        lat.append(1e3 * (st["done_s"] - st["submit_s"]))
+        queue.append(1e3 * (st["admit_s"] - st["submit_s"]))
+        first = st["submit_s"] if first is None else min(first, st["submit_s"])
+        last = st["done_s"] if last is None else max(last, st["done_s"])
+        pts += spec["nx"] * spec["ny"] * spec["nz"] * spec["nw"]
+        srv.fetch(jid)
+    srv.close()
+    return {"p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99), "mean_ms": sum(lat) / len(lat),
+            "max_queue_ms": max(queue), "throughput_points_per_s": pts / (last - first), "jobs": len(lat)}
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -190,104 +429,29 @@ def main():
     dev = torch.device("cuda", local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
-    from ocotillo_b200 import Engine, workloads, LAYOUT_REFERENCE, LAYOUT_LAMBDA_FASTEST
+    from ocotillo_b200 import Engine, workloads
 
-    nx, ny, nz, nw = a.nx, a.ny, a.nz, a.nw
-    ncol, mz = nx * ny, nz + 6
-    rho_h, T_h, dz = workloads.agn_block(nx, ny, nz, seed=2 + rank)
-    wa = workloads.log_wavelengths(nw)
-    rho = torch.from_numpy(rho_h).to(dev).reshape(ncol, nz)
-    T = torch.from_numpy(T_h).to(dev).reshape(ncol, nz)
     eng = Engine(local)
-    eng.set_wavelengths(wa)
+    g = Grid(a, eng, dev, rank)
+    eng.set_wavelengths(g.wa)
     eng.set_profiling(True)
-    layout = LAYOUT_REFERENCE if a.layout == "reference" else LAYOUT_LAMBDA_FASTEST
-    CH = min(a.chunk_cols, ncol)
-    assert ncol % CH == 0, "chunk must divide the grid"
-    nchunk = ncol // CH
+    ncol, nz, nw, mz = g.ncol, g.nz, g.nw, g.mz
 
-    def mk(shape):
-        return torch.empty(shape, dtype=torch.float64, device=dev)
+    m = g.measure(a.form, a.steps, a.warmup, world, dist, Clocks(local))
+    roof = g.roofline(m, a.steps, a.form)
 
-    sets = []
-    for _ in range(2):
-        if layout == LAYOUT_REFERENCE:
-            o = {"U": mk((nw, CH, mz)), "kappa": mk((nw, CH, nz)), "V": mk((nw, CH, nz))}
-        else:
-            o = {"U": mk((mz, CH, nw)), "kappa": mk((nz, CH, nw)), "V": mk((nz, CH, nw))}
-        sets.append(o)
-    Vtop, Vbot = mk((nchunk, nw, CH)), mk((nchunk, nw, CH))
-    stream = torch.cuda.current_stream(dev)
-
-    def step():
-        for k in range(nchunk):
-            o = dict(sets[k % 2])
-            o["Vtop"], o["Vbot"] = Vtop[k], Vbot[k]
-            r = rho[k * CH:(k + 1) * CH].reshape(CH, 1, nz)
-            t = T[k * CH:(k + 1) * CH].reshape(CH, 1, nz)
-            eng.solve_block_device(r, t, dz, o, form=a.form, layout=layout, stream=stream)
-
-    zero_pivot = False
-
-    def sync_engine():
-        nonlocal zero_pivot
-        try:
-            eng.synchronize()
-        except Exception as e:
-            if getattr(e, "code", None) != -3:
-                raise
-            zero_pivot = True
-
-    for _ in range(a.warmup):
-        step()
-    torch.cuda.synchronize(dev)
-    sync_engine()
-    eng.kernel_times()  # discard warm-up timings
-    clocks = Clocks(local)
-    clocks.start()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
-    launches0 = eng.kernel_launches
-    evs = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps + 1)]
-    evs[0].record(stream)
-    for i in range(a.steps):
-        step()
-        evs[i + 1].record(stream)
-    torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
-    clk = clocks.stop()
-    launches = eng.kernel_launches - launches0
-    sync_engine()
-    step_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(a.steps)]
-    total_ms = evs[0].elapsed_time(evs[-1])
-    solve_ms, pil_ms, nsolve = eng.kernel_times()
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    pts_step = ncol * nz * nw
-    value = world * pts_step * a.steps / (total_ms / 1e3)
-
-    # roofline of the dominant kernel (the solve): algorithmic bytes per mesh*lambda point
-    # = outputs U (nz+6 per nz), kappa, V (8 B each) + per-column pillars read once (26*8 B
-    # per z, shared by nw wavelengths).
-    bytes_pt = 8.0 * (mz / nz) + 16.0 + 26 * 8.0 / nw
-    launch_ms = solve_ms / max(nsolve, 1)
-    pts_launch = pts_step * a.steps / max(nsolve, 1)
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except Exception:
-        pass
-    hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    achieved = bytes_pt * pts_launch / (launch_ms / 1e3) / 1e9
-    roof = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-            "traffic": None, "kernel": "k_solve", "launch_ms": launch_ms,
-            "algorithmic_bytes_per_point": bytes_pt,
-            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-            "solve_share_of_step": solve_ms / total_ms, "pillars_ms_per_step": pil_ms / a.steps}
+    extra = {}
+    if world == 1 and not a.no_extra:
+        other = "mixed" if a.form != "mixed" else "plain"
+        mm = g.measure(other, a.steps, a.warmup, world)
+        plain_v, mixed_v = (m["value"], mm["value"]) if other == "mixed" else (mm["value"], m["value"])
+        mixed_m = mm if other == "mixed" else m
+        extra["mixed"] = {"value": mixed_v, "unit": "points/s", "ms_per_step": mixed_m["total_ms"] / a.steps,
+                          "latency_ms": {"p50": pct(mixed_m["step_ms"], 0.5), "p99": pct(mixed_m["step_ms"], 0.99)},
+                          "ratio_vs_plain_fp64": mixed_v / plain_v,
+                          "emergent_flux_rel_err": flux_error(g, "mixed", "stable"),
+                          "roofline": g.roofline(mixed_m, a.steps, "mixed")}
+        extra["plain_fp64_value"] = plain_v
 
     # ---- e2e: host arrays through oco_solve_block (pinned), one batch of columns per step
     e2e = None
@@ -296,15 +460,15 @@ def main():
         pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
         rho_p = pin((ncol, nz))
         T_p = pin((ncol, nz))
-        rho_p[:] = rho_h.reshape(ncol, nz)
-        T_p[:] = T_h.reshape(ncol, nz)
+        rho_p[:] = g.rho_h.reshape(ncol, nz)
+        T_p[:] = g.T_h.reshape(ncol, nz)
         outs = {"U": pin((nw, E, 1, mz)), "kappa": pin((nw, E, 1, nz)), "V": pin((nw, E, 1, nz)),
                 "Vtop": pin((nw, E, 1)), "Vbot": pin((nw, E, 1))}
         nb = ncol // E
 
         def e2e_step(i):
             c0 = (i % nb) * E
-            eng.solve_block(rho_p[c0:c0 + E].reshape(E, 1, nz), T_p[c0:c0 + E].reshape(E, 1, nz), dz,
+            eng.solve_block(rho_p[c0:c0 + E].reshape(E, 1, nz), T_p[c0:c0 + E].reshape(E, 1, nz), g.dz,
                             form=a.form, out=outs, allow_zero_pivot=True)
 
         for i in range(a.warmup):
@@ -324,26 +488,46 @@ def main():
             el = float(t.item())
         e2e = {"value": world * E * nz * nw * a.steps / el, "unit": "points/s",
                "h2d_bytes_per_step": 2 * E * nz * 8, "d2h_bytes_per_step": E * nw * (mz + 2 * nz + 2) * 8,
-               "columns_per_step": E, "p50_ms": 1e3 * pct(lat, 0.5), "p99_ms": 1e3 * pct(lat, 0.99)}
+               "columns_per_step": E, "form": a.form, "p50_ms": 1e3 * pct(lat, 0.5), "p99_ms": 1e3 * pct(lat, 0.99)}
+        del rho_p, T_p, outs
+
+    if world == 1 and not a.no_extra:
+        del g.sets
+        torch.cuda.empty_cache()
+        extra["batch"] = measure_batch(a, eng, dev)
+        torch.cuda.empty_cache()
+        specs = workloads.serving_stream(a.serve_jobs, a.serve_rate, seed=5)
+        arrays = [workloads.job_arrays_device(sp, dev) for sp in specs]
+        torch.cuda.synchronize(dev)
+        extra["serving"] = {"rate_jobs_per_s": a.serve_rate, "jobs": a.serve_jobs, "max_jobs_resident": 4,
+                            "latency": "submit to results complete on the device (server clock)",
+                            "stream": "Poisson (seed 5); nx=ny in {64,128,256,512}, nz U[128,1024], nw U[64,512], "
+                                      "rho0 log-uniform [1e-11,1e-7]; outputs: emergent-flux planes",
+                            "points": int(sum(sp["nx"] * sp["ny"] * sp["nz"] * sp["nw"] for sp in specs))}
+        for form in ("mixed", "plain"):
+            extra["serving"][form] = measure_serving(a, dev, form, specs, arrays)
+        del arrays
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         procs = os.cpu_count() or 1
-        v, dt, pts = cpu_baseline(rho_h, T_h, wa, dz, min(a.cpu_cols, ncol), procs)
+        v, dt, pts = cpu_baseline(g.rho_h, g.T_h, g.wa, g.dz, min(a.cpu_cols, ncol), procs)
         cpu = {"value": v, "unit": "points/s", "cores": procs, "kind": "port",
                "sample": f"first {min(a.cpu_cols, ncol)} columns of the same grid, all z and lambda "
                          f"({pts:.3g} points, {dt:.1f} s wall on {procs} processes), glibc math"}
 
     if rank == 0:
-        line = {"metric": "mesh*lambda points/s", "value": value, "unit": "points/s", "n_gpus": world,
-                "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic", "config": config_dict(a, a.form),
-                "latency_ms": {"p50": pct(step_ms, 0.5), "p99": pct(step_ms, 0.99)},
-                "zero_pivot_items": zero_pivot, "clocks": clk, "gpu_launches": int(launches),
+        line = {"metric": METRIC, "value": m["value"], "unit": "points/s", "n_gpus": world,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": m["total_ms"] / a.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if a.form != "mixed" else "f32 (FP64 Saha)", "data": "synthetic",
+                "config": config_dict(a, a.form),
+                "latency_ms": {"p50": pct(m["step_ms"], 0.5), "p99": pct(m["step_ms"], 0.99)},
+                "zero_pivot_items": g.zero_pivot, "clocks": m["clocks"], "gpu_launches": int(m["launches"]),
                 "roofline": roof, "e2e": e2e, "cpu_baseline": cpu}
         line["config"]["layout"] = a.layout
-        line["config"]["chunk_columns"] = CH
+        line["config"]["chunk_columns"] = g.CH
+        line.update(extra)
         print(json.dumps(line), flush=True)
     eng.close()
     if world > 1:

@@ -261,6 +261,8 @@ typedef struct oco_server_config {
   double budget_bytes;   /* admission limit on the summed footprint of admitted jobs;
                           * 0: 85% of the device memory free after the workspace */
   int64_t chunk_points;  /* mesh*lambda points per launch; 0: 2^28 */
+  double reserve_bytes;  /* device memory for job arrays mapped at creation, so that the first
+                          * admissions do not wait for the allocator to grow (0: none) */
 } oco_server_config;
 
 typedef struct oco_job {

@@ -25,6 +25,7 @@
 #include <condition_variable>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <deque>
 #include <memory>
 #include <mutex>
@@ -116,11 +117,13 @@ int64_t footprint(const oco_params &p, int want_fields, int64_t *input_bytes) {
 
 struct oco_server {
   int device = 0;
+  bool trace = false; /* OCO_SERVER_TRACE=1: one stderr line per scheduler step slower than 1 ms */
   int64_t chunk_points = 1ll << 28;
   double budget = 0, used = 0;
   std::vector<Slot> slots;
   int full_blocks[3] = {1, 1, 1};
   cudaStream_t misc = nullptr; /* frees of fetched jobs */
+  cudaMemPool_t pool = nullptr; /* job arrays; keeps freed memory mapped for the next job */
   std::mutex mu;
   std::condition_variable cv;      /* wakes the scheduler */
   std::condition_variable cv_done; /* wakes waiters */
@@ -166,26 +169,32 @@ void oco_server::fail(Job *j, int code, const std::string &msg) {
 int oco_server::admit(Job *j, Slot &sl) {
   oco_ctx *c = sl.ctx;
   cudaStream_t s = c->stream;
+  const double t0 = now_s();
   int rc = oco_set_wavelengths(c, j->waves.data(), j->p.nw);
   if (rc) return rc;
   if ((rc = oco_ctx_check_params(c, &j->p))) return rc;
+  const double t1 = now_s();
   const int64_t ncol = (int64_t)j->p.nx * j->p.ny;
   const size_t nin = (size_t)ncol * j->p.nz * sizeof(double);
   const size_t nfl = (size_t)ncol * j->p.nw * sizeof(double);
-  CU(cudaMallocAsync((void **)&j->rho, nin, s));
-  CU(cudaMallocAsync((void **)&j->T, nin, s));
-  CU(cudaMallocAsync((void **)&j->Vtop, nfl, s));
-  CU(cudaMallocAsync((void **)&j->Vbot, nfl, s));
+  CU(cudaMallocFromPoolAsync((void **)&j->rho, nin, pool, s));
+  CU(cudaMallocFromPoolAsync((void **)&j->T, nin, pool, s));
+  CU(cudaMallocFromPoolAsync((void **)&j->Vtop, nfl, pool, s));
+  CU(cudaMallocFromPoolAsync((void **)&j->Vbot, nfl, pool, s));
   if (j->want_fields) {
-    CU(cudaMallocAsync((void **)&j->U, (size_t)ncol * j->p.nw * (j->p.nz + 6) * sizeof(double), s));
-    CU(cudaMallocAsync((void **)&j->K, (size_t)ncol * j->p.nw * j->p.nz * sizeof(double), s));
-    CU(cudaMallocAsync((void **)&j->V, (size_t)ncol * j->p.nw * j->p.nz * sizeof(double), s));
+    CU(cudaMallocFromPoolAsync((void **)&j->U, (size_t)ncol * j->p.nw * (j->p.nz + 6) * sizeof(double), pool, s));
+    CU(cudaMallocFromPoolAsync((void **)&j->K, (size_t)ncol * j->p.nw * j->p.nz * sizeof(double), pool, s));
+    CU(cudaMallocFromPoolAsync((void **)&j->V, (size_t)ncol * j->p.nw * j->p.nz * sizeof(double), pool, s));
   }
+  const double t2 = now_s();
   CU(cudaMemcpyAsync(j->rho, j->rho_in, nin, cudaMemcpyDefault, s));
   CU(cudaMemcpyAsync(j->T, j->T_in, nin, cudaMemcpyDefault, s));
   if (!j->inputs_done) CU(cudaEventCreateWithFlags(&j->inputs_done, cudaEventDisableTiming));
   CU(cudaEventRecord(j->inputs_done, s));
   if ((rc = oco_ctx_reset_status(c, s))) return rc;
+  if (trace)
+    fprintf(stderr, "[oco_server] admit job %lld: tables %.3f ms, allocation %.3f ms, copies %.3f ms\n",
+            (long long)j->id, 1e3 * (t1 - t0), 1e3 * (t2 - t1), 1e3 * (now_s() - t2));
   j->ncol = ncol;
   j->next_col = 0;
   const int64_t per_col = (int64_t)j->p.nz * j->p.nw;
@@ -218,7 +227,9 @@ void oco_server::loop() {
       j->t_admit = now_s();
       used += (double)j->bytes;
       lk.unlock();
+      const double ta = now_s();
       const int rc = admit(j, sl);
+      if (trace) fprintf(stderr, "[oco_server] %.6f admit job %lld: %.3f ms\n", ta, (long long)j->id, 1e3 * (now_s() - ta));
       lk.lock();
       if (rc) fail(j, rc, std::string("admission: ") + oco_last_error(sl.ctx));
       progress = true;
@@ -239,6 +250,7 @@ void oco_server::loop() {
       while ((int)j->inflight.size() < kInFlight && j->next_col < j->ncol) {
         const int64_t nb = std::min(j->chunk_cols, j->ncol - j->next_col);
         const int share = std::max(1, full_blocks[j->p.form] / std::max(1, with_work));
+        const double tl = now_s();
         int rc = oco_ctx_run_columns(sl.ctx, &j->p, j->rho, j->T, j->next_col, nb, j->U, j->K, j->V, j->Vtop,
                                      j->Vbot, share, sl.ctx->stream);
         cudaEvent_t e = sl.take();
@@ -253,6 +265,9 @@ void oco_server::loop() {
         j->inflight.push_back(e);
         j->next_col += nb;
         progress = true;
+        if (trace && now_s() - tl > 1e-3)
+          fprintf(stderr, "[oco_server] %.6f launch job %lld cols %lld+%lld grid %d: %.3f ms\n", tl, (long long)j->id,
+                  (long long)(j->next_col - nb), (long long)nb, share, 1e3 * (now_s() - tl));
       }
     }
     /* 3. retire */
@@ -281,7 +296,9 @@ void oco_server::loop() {
       }
       if (!j || !j->inflight.empty() || j->next_col < j->ncol) continue;
       /* all launches done */
+      const double tr = now_s();
       const int rc = oco_ctx_read_status(sl.ctx, sl.ctx->stream, &j->p);
+      if (trace) fprintf(stderr, "[oco_server] %.6f done job %lld: status read %.3f ms\n", tr, (long long)j->id, 1e3 * (now_s() - tr));
       lk.lock();
       if (rc && rc != OCO_EZEROPIVOT) {
         fail(j, rc, oco_last_error(sl.ctx));
@@ -320,6 +337,7 @@ static void free_server(oco_server *s) {
     if (sl.ctx) oco_destroy(sl.ctx);
   }
   if (s->misc) cudaStreamDestroy(s->misc);
+  if (s->pool) cudaMemPoolDestroy(s->pool);
   delete s;
 }
 
@@ -345,6 +363,19 @@ static int setup_server(oco_server *srv, const oco_server_config *cfg) {
       SCU(c->pil.ensure((size_t)kMaxChunkCols * cfg->max_nz * kRecordBytesMax));
     }
   }
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = cfg->device;
+  SCU(cudaMemPoolCreate(&srv->pool, &props));
+  uint64_t keep = UINT64_MAX;
+  SCU(cudaMemPoolSetAttribute(srv->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  if (cfg->reserve_bytes > 0) { /* grow the pool once; freed blocks stay mapped */
+    void *r = nullptr;
+    SCU(cudaMallocFromPoolAsync(&r, (size_t)cfg->reserve_bytes, srv->pool, srv->misc));
+    SCU(cudaFreeAsync(r, srv->misc));
+    SCU(cudaStreamSynchronize(srv->misc));
+  }
   size_t fr = 0, tot = 0;
   SCU(cudaMemGetInfo(&fr, &tot));
   srv->budget = cfg->budget_bytes > 0 ? cfg->budget_bytes : 0.85 * (double)fr;
@@ -354,12 +385,14 @@ static int setup_server(oco_server *srv, const oco_server_config *cfg) {
 extern "C" int oco_server_create(const oco_server_config *cfg, oco_server **out) {
   if (!cfg || !out) return serr(OCO_EINVAL, "oco_server_create: NULL argument");
   *out = nullptr;
-  if (cfg->max_jobs < 1 || cfg->max_nz < 0 || cfg->reserved != 0 || cfg->budget_bytes < 0 || cfg->chunk_points < 0)
+  if (cfg->max_jobs < 1 || cfg->max_nz < 0 || cfg->reserved != 0 || cfg->budget_bytes < 0 || cfg->chunk_points < 0 ||
+      cfg->reserve_bytes < 0)
     return serr(OCO_EINVAL, "oco_server_create: need max_jobs >= 1, max_nz >= 0, budget >= 0, reserved = 0");
   oco_server *srv = new (std::nothrow) oco_server();
   if (!srv) return serr(OCO_ENOMEM, "oco_server_create: out of host memory");
   srv->device = cfg->device;
   if (cfg->chunk_points > 0) srv->chunk_points = cfg->chunk_points;
+  if (const char *t = getenv("OCO_SERVER_TRACE")) srv->trace = t[0] == '1';
   const int rc = setup_server(srv, cfg);
   if (rc) {
     free_server(srv);

@@ -62,7 +62,8 @@ TILING_WARP_COLUMN, TILING_PACKED = 0, 1
 
 class OcoServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("max_jobs", ctypes.c_int32), ("max_nz", ctypes.c_int32),
-                ("reserved", ctypes.c_int32), ("budget_bytes", ctypes.c_double), ("chunk_points", ctypes.c_int64)]
+                ("reserved", ctypes.c_int32), ("budget_bytes", ctypes.c_double), ("chunk_points", ctypes.c_int64),
+                ("reserve_bytes", ctypes.c_double)]
 
 
 class OcoJob(ctypes.Structure):
@@ -391,10 +392,11 @@ class Server:
     the device.  Inputs are numpy float64 arrays (nx, ny, nz) or torch CUDA float64 tensors of
     that shape; results come back as numpy arrays in the reference layout."""
 
-    def __init__(self, device=0, max_jobs=4, max_nz=0, budget_bytes=0.0, chunk_points=0):
+    def __init__(self, device=0, max_jobs=4, max_nz=0, budget_bytes=0.0, chunk_points=0, reserve_bytes=0.0):
         self.lib = load_library()
         self.h = ctypes.c_void_p()
-        cfg = OcoServerConfig(int(device), int(max_jobs), int(max_nz), 0, float(budget_bytes), int(chunk_points))
+        cfg = OcoServerConfig(int(device), int(max_jobs), int(max_nz), 0, float(budget_bytes), int(chunk_points),
+                              float(reserve_bytes))
         self._check(self.lib.oco_server_create(ctypes.byref(cfg), ctypes.byref(self.h)))
         self._jobs = {}
 

@@ -113,3 +113,37 @@ def ragged_batch(ncol=8192, seed=4, nz_range=(64, 2048), nw_range=(32, 1024)):
         dzs[i] = dz
     return {"nz": nz, "nw": nw, "dz": dzs, "wave_off": wave_off, "waves": np.concatenate(waves),
             "rho": np.concatenate(rhos), "T": np.concatenate(Ts)}
+
+
+SERVING_SIZES = (64, 128, 256, 512)
+
+
+def serving_stream(n_jobs, rate, seed=5):
+    """Config 'serving form': a Poisson stream of n_jobs post-processing jobs at `rate` jobs/s.
+    Per job nx = ny drawn from SERVING_SIZES, nz uniform in [128, 1024], nw uniform in
+    [64, 512], rho0 log-uniform in [1e-11, 1e-7] (the precision config's construction).
+    Returns a list of dicts (arrival_s, nx, ny, nz, nw, rho0, seed)."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n_jobs))
+    jobs = []
+    for k in range(n_jobs):
+        n = int(rng.choice(SERVING_SIZES))
+        jobs.append({"arrival_s": float(t[k] - t[0]), "nx": n, "ny": n, "nz": int(rng.integers(128, 1025)),
+                     "nw": int(rng.integers(64, 513)), "rho0": float(10.0 ** rng.uniform(-11.0, -7.0)),
+                     "seed": int(rng.integers(1 << 30))})
+    return jobs
+
+
+def job_arrays_device(job, device, sigma_dex=0.3):
+    """rho, T (nx, ny, nz) float64 torch tensors on `device` for a serving_stream job: the
+    agn_block construction with the job's rho0, the perturbation drawn on the device."""
+    import torch
+    nz = job["nz"]
+    z, dz = grid(nz)
+    base = np.maximum(job["rho0"] * np.exp(-0.5 * z * z / (H * H)), RHO_FLOOR)
+    g = torch.Generator(device=device)
+    g.manual_seed(job["seed"])
+    pert = torch.randn((job["nx"], job["ny"], nz), generator=g, device=device, dtype=torch.float64)
+    rho = torch.pow(10.0, sigma_dex * pert) * torch.from_numpy(base).to(device)
+    T = torch.from_numpy(temperature(z)).to(device).expand(job["nx"], job["ny"], nz).contiguous()
+    return rho, T, dz
