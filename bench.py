@@ -293,12 +293,22 @@ class Grid:
         hbm_peak = pk.get("hbm_gbs", 6650.0)
         achieved = bytes_pt * pts_launch / (launch_ms / 1e3) / 1e9
         flops = 97.0 * pts_launch / (launch_ms / 1e3) / 1e12
+        tpp = TRAFFIC_BYTES_PER_POINT.get(form) if (self.nz, self.nw, self.layout) == (512, 256, 1) else None
         return {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                "traffic": None, "kernel": "k_solve_staged" if form != "mixed" else "k_solve_mixed_staged",
+                "traffic": tpp * pts_launch if tpp else None,
+                "traffic_source": "ncu capture of a 1024-column launch, scaled by points" if tpp else None,
+                "kernel": "k_solve_staged" if form != "mixed" else "k_solve_mixed_staged",
                 "launch_ms": launch_ms, "points_per_launch": pts_launch, "algorithmic_bytes_per_point": bytes_pt,
                 "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in pk else "fallback",
                 "algorithmic_tflops": flops, "flops_per_point": 97,
                 "solve_share_of_step": m["solve_ms"] / m["total_ms"], "pillars_ms_per_step": m["pil_ms"] / steps}
+
+
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per mesh*lambda point of the solve
+# kernel, from one ncu --set full capture of a 1024-column launch of this grid (outputs 3.2 GB,
+# larger than L2), scaled to a launch by its points: profiles/k_solve_staged_plain_agn_32x32x512x256.txt
+# and profiles/k_solve_mixed_staged_agn_32x32x512x256.txt.
+TRAFFIC_BYTES_PER_POINT = {"plain": 71.9, "mixed": 56.4}
 
 
 def flux_error(g, form_a, form_b, eps=1e-7, seed=7):

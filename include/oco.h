@@ -133,6 +133,12 @@ int64_t oco_kernel_launches(const oco_ctx *ctx);
 int oco_set_profiling(oco_ctx *ctx, int enable);
 int oco_kernel_times(oco_ctx *ctx, double *solve_ms, double *pillars_ms, int64_t *solve_launches);
 
+/* Diagnostic of the failure path: runs the kernels' bounded wait (the mbarrier poll the
+ * solve kernels use for their shared-memory copies) on a barrier phase that nothing
+ * completes, polling spin_limit times.  Returns OCO_ETIMEDOUT when the wait ran out, as a
+ * solve does, with the context still usable.  No reference counterpart. */
+int oco_check_bounded_wait(oco_ctx *ctx, int64_t spin_limit);
+
 /* ---- Solve without device allocation ----------------------------------------------------
  * No counterpart in the reference (whose loop allocates nothing on a GPU): this entry point
  * serves callers that cannot call cudaMalloc -- hosts that own the device heap, plugins not

@@ -634,6 +634,32 @@ int solve_fp64_max_blocks_per_sm(int form, int grey, int threads) {
   return nb > 0 ? nb : 1;
 }
 
+/* Diagnostic: the staged kernels' bounded mbarrier wait, on a barrier phase that no copy or
+ * arrival completes, so the wait runs out after `limit` polls and the timeout is reported in
+ * status[2] as the solve kernels report it.  Nothing is in flight when the block exits. */
+__global__ void k_bounded_wait_check(long long limit, unsigned long long *status) {
+  __shared__ __align__(8) unsigned long long bar;
+  const uint32_t b = smem_addr(&bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  long long spins = 0;
+  bool done = true;
+  while (!mbar_try_wait(b, 0u))
+    if (++spins > limit) {
+      done = false;
+      break;
+    }
+  if (__any_sync(0xffffffffu, !done) && threadIdx.x == 0) atomicOr(&status[2], 1ull);
+}
+
+cudaError_t launch_bounded_wait_check(long long limit, unsigned long long *status, cudaStream_t s) {
+  k_bounded_wait_check<<<1, 32, 0, s>>>(limit, status);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_solve_fp64(const SolveArgs &a, int form, int grey, int blocks, int threads, cudaStream_t s) {
   const bool staged = !grey && solve_uses_staging(a.nw);
   void *args[] = {(void *)&a};

@@ -409,17 +409,18 @@ __global__ void __launch_bounds__(128) k_solve_mixed(const MixedArgs a) {
   }
 }
 
-int solve_mixed_max_blocks_per_sm(int threads) {
-  int a = 0, b = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_solve_mixed, threads, 0) != cudaSuccess) a = 1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_solve_mixed_staged, threads, 0) != cudaSuccess) b = 1;
-  a = a > b ? a : b;
-  return a > 0 ? a : 1;
+static bool mixed_uses_staging(int nw) { return (nw >= 64) || (nw % 32) == 0; }
+
+int solve_mixed_max_blocks_per_sm(int threads, int nw) {
+  int n = 0;
+  const cudaError_t e = mixed_uses_staging(nw)
+                            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solve_mixed_staged, threads, 0)
+                            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solve_mixed, threads, 0);
+  return (e == cudaSuccess && n > 0) ? n : 1;
 }
 
 cudaError_t launch_solve_mixed(const MixedArgs &a, int blocks, int threads, cudaStream_t s) {
-  const bool staged = (a.nw >= 64) || (a.nw % 32) == 0;
-  if (staged)
+  if (mixed_uses_staging(a.nw))
     k_solve_mixed_staged<<<blocks, threads, 0, s>>>(a);
   else
     k_solve_mixed<<<blocks, threads, 0, s>>>(a);

@@ -260,7 +260,7 @@ static const int kSolveThreads = 128;
  * gamma, u, 1/kappa, q (32 B) or, for the mixed form, one float4 (16 B). */
 static int prepare_solve(oco_ctx *c, int form, int grey, int64_t nitems, int nz, int *blocks) {
   const bool mixed = form == OCO_FORM_MIXED;
-  int bps = mixed ? solve_mixed_max_blocks_per_sm(kSolveThreads)
+  int bps = mixed ? solve_mixed_max_blocks_per_sm(kSolveThreads, c->nw)
                   : solve_fp64_max_blocks_per_sm(form == OCO_FORM_STABLE ? 1 : 0, grey, kSolveThreads);
   int64_t maxb = (int64_t)bps * c->num_sms;
   if (c->max_blocks > 0) maxb = std::min<int64_t>(maxb, c->max_blocks);
@@ -501,7 +501,7 @@ int oco_ctx_check_params(oco_ctx *c, const oco_params *p) {
 }
 
 int oco_ctx_full_blocks(oco_ctx *c, int form, int grey) {
-  const int bps = form == OCO_FORM_MIXED ? solve_mixed_max_blocks_per_sm(kSolveThreads)
+  const int bps = form == OCO_FORM_MIXED ? solve_mixed_max_blocks_per_sm(kSolveThreads, 64)
                                          : solve_fp64_max_blocks_per_sm(form == OCO_FORM_STABLE ? 1 : 0, grey,
                                                                         kSolveThreads);
   return bps * c->num_sms;
@@ -585,6 +585,21 @@ extern "C" int oco_synchronize(oco_ctx *c) {
   CU(cudaStreamSynchronize(c->stream));
   CU(cudaStreamSynchronize(c->copy));
   return OCO_OK;
+}
+
+extern "C" int oco_check_bounded_wait(oco_ctx *c, int64_t spin_limit) {
+  if (!c) return oco_set_err(nullptr, OCO_EINVAL, "NULL context");
+  if (spin_limit < 0 || spin_limit > (1ll << 30)) return oco_set_err(c, OCO_EINVAL, "spin_limit must be 0..2^30");
+  CU(cudaSetDevice(c->device));
+  CU(cudaStreamSynchronize(c->stream));
+  c->status_pending = false;
+  int rc = reset_status(c, c->stream);
+  if (rc) return rc;
+  CU(launch_bounded_wait_check(spin_limit, c->status.as<unsigned long long>(), c->stream));
+  c->launches++;
+  oco_params p{};
+  p.nx = p.ny = p.nw = 1;
+  return read_status(c, c->stream, &p);
 }
 
 extern "C" int64_t oco_kernel_launches(const oco_ctx *c) { return c ? c->launches : 0; }

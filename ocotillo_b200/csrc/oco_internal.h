@@ -169,6 +169,8 @@ cudaError_t launch_pillars(const double *rho, const double *T, int64_t ncol, int
 cudaError_t launch_solve_fp64(const SolveArgs &a, int form, int grey, int nslot_blocks,
                               int threads, cudaStream_t s);
 int solve_fp64_max_blocks_per_sm(int form, int grey, int threads);
+/* Runs the bounded-wait diagnostic kernel (one warp) on s; sets status[2] when the wait ran out. */
+cudaError_t launch_bounded_wait_check(long long limit, unsigned long long *status, cudaStream_t s);
 
 /* Mixed-precision kernels (kernels_mixed.cu). */
 constexpr int MIXED_ZN = 40; /* floats per mixed record */
@@ -176,7 +178,7 @@ constexpr int MIXED_LN = 24; /* fields of the mixed wavelength table */
 cudaError_t launch_pillars_mixed(const double *rho, const double *T, int64_t ncol, int nz, double fully_ionized_T,
                                  float *rec, cudaStream_t s);
 cudaError_t launch_solve_mixed(const MixedArgs &a, int blocks, int threads, cudaStream_t s);
-int solve_mixed_max_blocks_per_sm(int threads);
+int solve_mixed_max_blocks_per_sm(int threads, int nw); /* occupancy of the kernel used for nw */
 /* Fills tab32[MIXED_LN*nw] from the FP64 table tab[NL*nw]. */
 void fill_mixed_lambda_table(const double *tab, int nw, float *tab32);
 

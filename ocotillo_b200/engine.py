@@ -106,6 +106,7 @@ def load_library(path=None):
         "oco_solve_block_device": (I, [V, P, V, V, V, V, V, V, V, V]),
         "oco_synchronize": (I, [V]),
         "oco_kernel_launches": (ctypes.c_int64, [V]),
+        "oco_check_bounded_wait": (I, [V, ctypes.c_int64]),
         "oco_set_profiling": (I, [V, I]),
         "oco_kernel_times": (I, [V, _DP, _DP, ctypes.POINTER(ctypes.c_int64)]),
         "oco_solve_block_noalloc": (I, [P, _DP, V, V, V, V, V, V, V, V]),
@@ -244,6 +245,10 @@ class Engine:
 
     def synchronize(self):
         self._check(self.lib.oco_synchronize(self.ctx))
+
+    def check_bounded_wait(self, spin_limit=100):
+        """Return code of the bounded-wait diagnostic (OCO_ETIMEDOUT = -6 expected)."""
+        return self.lib.oco_check_bounded_wait(self.ctx, int(spin_limit))
 
     @property
     def kernel_launches(self):
