@@ -321,6 +321,47 @@ void oco_server_destroy(oco_server *server);
 /* Message of the last failed server call on this thread. */
 const char *oco_server_last_error(void);
 
+/* ---- Decks: the reference's driver around the loop --------------------------------------
+ * A deck is a run directory of the reference: input.in (namelists &input, &temperature_input,
+ * &density_input, &gas_state_input, &athena_input), resolution.in (the Fortran include of
+ * integer parameters nx, ny, nz, nw, nprocx, nprocy, nprocz, nxloc, nyloc; read at run time
+ * here) and, when lread_athena, the Athena snapshot under datadir.  Replaces the main program
+ * flux_feautrier.f90:1-269 with the xy/lambda loop on the GPU. */
+typedef struct oco_deck_info {
+  int32_t nx, ny, nz, nw;
+  int32_t nprocx, nprocy, nprocz;
+  int32_t nxloc, nyloc;
+  int32_t lgrey, lread_athena, reserved;
+  double dz;               /* grid spacing of the block (0 if its inputs were not built) */
+  double sigma_grey;
+  double fully_ionized_T;
+} oco_deck_info;
+
+/* Builds processor block (iprocx, iprocy)'s inputs as the reference does: the synthetic disk
+ * (disk.f90:42-129) or the Athena reader (read_athena.f90:64-291).  rho and T (may be NULL:
+ * then only *info and wa are filled) receive (nz, nyloc, nxloc) values, wa the nw wavelengths
+ * (calc_wavelength), z (may be NULL) the nz+6 grid with ghosts.  Host only, no GPU needed.
+ * snapshot NULL or "" is "0000". */
+int oco_deck_block_inputs(const char *deck_dir, const char *snapshot, int32_t iprocx, int32_t iprocy,
+                          oco_deck_info *info, double *rho, double *T, double *wa, double *z);
+
+/* Runs a deck: every processor block solved on CUDA device `device` in form `form`, writing
+ * into out_dir (NULL or "": deck_dir/output) what the reference writes into output/:
+ * diagnostics.txt (io.f90:31-46, gfortran Ew.d editing), zgrid.txt/.bin and wavegrid.txt/.bin
+ * (io.f90:48-75) and, when write_binary, procx<i>_procy<j>/{mean_intensity,
+ * absorption_coefficients,flux}_<snapshot>.bin as Fortran unformatted sequential records
+ * (io.f90:77-101).  Returns OCO_EZEROPIVOT (after writing everything) where the reference
+ * would stop at a zero pivot.  Messages: oco_deck_last_error(). */
+int oco_run_deck(const char *deck_dir, const char *snapshot, const char *out_dir, int32_t form, int32_t device,
+                 int32_t write_binary);
+
+/* gfortran Ew.d editing of v into out (w characters + NUL); the `0.ddddd-ddd` form for
+ * three-digit exponents, asterisks when the value does not fit. */
+void oco_format_e(double v, int32_t w, int32_t d, char *out);
+
+/* Message of the last failed deck call on this thread. */
+const char *oco_deck_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

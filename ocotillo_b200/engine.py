@@ -81,6 +81,14 @@ class OcoJobStatus(ctypes.Structure):
 
 JOB_STATES = ("queued", "running", "done", "failed")
 
+
+class OcoDeckInfo(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32), ("nw", ctypes.c_int32),
+                ("nprocx", ctypes.c_int32), ("nprocy", ctypes.c_int32), ("nprocz", ctypes.c_int32),
+                ("nxloc", ctypes.c_int32), ("nyloc", ctypes.c_int32), ("lgrey", ctypes.c_int32),
+                ("lread_athena", ctypes.c_int32), ("reserved", ctypes.c_int32), ("dz", ctypes.c_double),
+                ("sigma_grey", ctypes.c_double), ("fully_ionized_T", ctypes.c_double)]
+
 _LIB = None
 _DP = ctypes.POINTER(ctypes.c_double)
 
@@ -128,6 +136,12 @@ def load_library(path=None):
         "oco_server_fetch": (I, [V, ctypes.c_int64, _DP, _DP, _DP, _DP, _DP]),
         "oco_server_destroy": (None, [V]),
         "oco_server_last_error": (ctypes.c_char_p, []),
+        "oco_deck_block_inputs": (I, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32,
+                                      ctypes.POINTER(OcoDeckInfo), _DP, _DP, _DP, _DP]),
+        "oco_run_deck": (I, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32,
+                             ctypes.c_int32]),
+        "oco_format_e": (None, [D, ctypes.c_int32, ctypes.c_int32, ctypes.c_char_p]),
+        "oco_deck_last_error": (ctypes.c_char_p, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -142,6 +156,65 @@ def _ptr(a):
         return None
     assert a.dtype == np.float64 and a.flags.c_contiguous
     return a.ctypes.data_as(_DP)
+
+
+def format_e(v, w=15, d=5):
+    """gfortran Ew.d editing (io.f90's e15.5 fields)."""
+    lib = load_library()
+    buf = ctypes.create_string_buffer(w + 1)
+    lib.oco_format_e(float(v), int(w), int(d), buf)
+    return buf.value.decode()
+
+
+def deck_block_inputs(deck_dir, snapshot="0000", iprocx=0, iprocy=0):
+    """Inputs of processor block (iprocx, iprocy) of a reference deck (synthetic disk or Athena
+    reader), host only: dict with info fields, rho and T (nxloc, nyloc, nz), wa, z (nz+6)."""
+    lib = load_library()
+    info = OcoDeckInfo()
+    rc = lib.oco_deck_block_inputs(deck_dir.encode(), snapshot.encode(), 0, 0, ctypes.byref(info), None, None,
+                                   None, None)
+    if rc:
+        raise OcoError(rc, lib.oco_deck_last_error().decode())
+    rho = np.empty((info.nxloc, info.nyloc, info.nz))
+    T = np.empty_like(rho)
+    wa = np.empty(info.nw)
+    z = np.empty(info.nz + 6)
+    rc = lib.oco_deck_block_inputs(deck_dir.encode(), snapshot.encode(), int(iprocx), int(iprocy),
+                                   ctypes.byref(info), _ptr(rho), _ptr(T), _ptr(wa), _ptr(z))
+    if rc:
+        raise OcoError(rc, lib.oco_deck_last_error().decode())
+    out = {k: getattr(info, k) for k, _ in OcoDeckInfo._fields_}
+    out.update(rho=rho, T=T, wa=wa, z=z)
+    return out
+
+
+def run_deck(deck_dir, snapshot="0000", out_dir=None, form="plain", device=0, write_binary=True):
+    """Runs a reference deck with the loop on the GPU; writes diagnostics.txt, the grids and
+    (write_binary) the per-block Fortran unformatted files into out_dir (default
+    deck_dir/output).  Returns the return code (0, or -3 where the reference stops on a zero
+    pivot); raises on other errors."""
+    lib = load_library()
+    rc = lib.oco_run_deck(deck_dir.encode(), snapshot.encode(), (out_dir or "").encode(),
+                          _FORMS[form] if isinstance(form, str) else int(form), int(device), int(bool(write_binary)))
+    if rc and rc != -3:
+        raise OcoError(rc, lib.oco_deck_last_error().decode())
+    return rc
+
+
+def read_fortran_records(path):
+    """Records of a Fortran unformatted sequential file (gfortran markers and subrecords) as
+    a list of bytes objects."""
+    data = open(path, "rb").read()
+    recs, pos, cur = [], 0, b""
+    while pos < len(data):
+        lead = int.from_bytes(data[pos:pos + 4], "little", signed=True)
+        n = abs(lead)
+        cur += data[pos + 4:pos + 4 + n]
+        pos += 8 + n
+        if lead >= 0:
+            recs.append(cur)
+            cur = b""
+    return recs
 
 
 def calc_wavelength(w1, w0, nw):
