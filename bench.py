@@ -304,6 +304,10 @@ class Grid:
                 "solve_share_of_step": m["solve_ms"] / m["total_ms"], "pillars_ms_per_step": m["pil_ms"] / steps}
 
 
+# The reference's published rate for this path: 0.14415 us per mesh*lambda point (its README,
+# multiInTest sample, one CPU core) = 6.94e6 points/s.
+PUBLISHED_POINTS_PER_S = 1e6 / 0.14415
+
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per mesh*lambda point of the solve
 # kernel, from one ncu --set full capture of a 1024-column launch of this grid (outputs 3.2 GB,
 # larger than L2), scaled to a launch by its points: profiles/k_solve_staged_plain_agn_32x32x512x256.txt
@@ -498,8 +502,29 @@ def main():
             el = float(t.item())
         e2e = {"value": world * E * nz * nw * a.steps / el, "unit": "points/s",
                "h2d_bytes_per_step": 2 * E * nz * 8, "d2h_bytes_per_step": E * nw * (mz + 2 * nz + 2) * 8,
-               "columns_per_step": E, "form": a.form, "p50_ms": 1e3 * pct(lat, 0.5), "p99_ms": 1e3 * pct(lat, 0.99)}
-        del rho_p, T_p, outs
+               "columns_per_step": E, "form": a.form, "outputs": "U, kappa, V, Vtop, Vbot (all, reference layout)",
+               "p50_ms": 1e3 * pct(lat, 0.5), "p99_ms": 1e3 * pct(lat, 0.99)}
+        del outs
+        # the same call returning only the emergent-flux planes (the spectra), whole grid per step
+        if world == 1 and not a.no_extra:
+            fl = {"Vtop": pin((nw, ncol, 1)), "Vbot": pin((nw, ncol, 1))}
+            rho_all, T_all = rho_p.reshape(ncol, 1, nz), T_p.reshape(ncol, 1, nz)
+            for i in range(max(1, a.warmup)):
+                eng.solve_block(rho_all, T_all, g.dz, form=a.form, out=fl, want=("Vtop", "Vbot"),
+                                allow_zero_pivot=True)
+            lat = []
+            for i in range(a.steps):
+                s0 = time.perf_counter()
+                eng.solve_block(rho_all, T_all, g.dz, form=a.form, out=fl, want=("Vtop", "Vbot"),
+                                allow_zero_pivot=True)
+                lat.append(time.perf_counter() - s0)
+            extra["e2e_emergent_flux_only"] = {
+                "value": ncol * nz * nw * a.steps / sum(lat), "unit": "points/s", "form": a.form,
+                "h2d_bytes_per_step": 2 * ncol * nz * 8, "d2h_bytes_per_step": 2 * ncol * nw * 8,
+                "outputs": "Vtop, Vbot only (oco_solve_block with U, kappa, V NULL), whole grid per call",
+                "p50_ms": 1e3 * pct(lat, 0.5), "p99_ms": 1e3 * pct(lat, 0.99)}
+            del fl
+        del rho_p, T_p
 
     if world == 1 and not a.no_extra:
         del g.sets
@@ -529,7 +554,9 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": m["value"], "unit": "points/s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": m["total_ms"] / a.steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": m["value"] / PUBLISHED_POINTS_PER_S,
+                "vs_baseline_source": "reference's published xy-loop rate, 6.94e6 mesh*lambda points/s (one CPU "
+                                      "core, multiInTest sample; README.md:41-42)",
                 "dtype": "f64" if a.form != "mixed" else "f32 (FP64 Saha)", "data": "synthetic",
                 "config": config_dict(a, a.form),
                 "latency_ms": {"p50": pct(m["step_ms"], 0.5), "p99": pct(m["step_ms"], 0.99)},

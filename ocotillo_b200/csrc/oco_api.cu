@@ -277,11 +277,15 @@ static size_t record_bytes(int form) {
 }
 
 /* Columns per chunk so that pillars (+ staged outputs on the host path) fit the budget. */
-static int64_t chunk_columns(oco_ctx *c, const oco_params *p, bool host_path) {
+static int64_t chunk_columns(oco_ctx *c, const oco_params *p, bool host_path, bool u = true, bool k = true,
+                             bool v = true, bool planes = true) {
   const int64_t ncol = (int64_t)p->nx * p->ny;
   size_t per_col = (size_t)p->nz * record_bytes(p->form);
-  if (host_path)
-    per_col += 2 * ((size_t)p->nz * 2 + (size_t)p->nw * ((p->nz + 6) + 2 * (size_t)p->nz + 2)) * sizeof(double);
+  if (host_path) { /* two staging sets of the requested outputs */
+    const size_t per_w = (u ? (size_t)(p->nz + 6) : 0) + (k ? (size_t)p->nz : 0) + (v ? (size_t)p->nz : 0) +
+                         (planes ? 2 : 0);
+    per_col += 2 * ((size_t)p->nz * 2 + (size_t)p->nw * per_w) * sizeof(double);
+  }
   int64_t ch = (int64_t)std::max<size_t>(1, c->budget_bytes / per_col);
   return std::min(ch, ncol);
 }
@@ -516,7 +520,7 @@ extern "C" int oco_solve_block(oco_ctx *c, const oco_params *p, const double *rh
   CU(cudaSetDevice(c->device));
   const int64_t ncol = (int64_t)p->nx * p->ny;
   const int nz = p->nz, nw = p->nw, mz = nz + 6;
-  const int64_t ch = chunk_columns(c, p, true);
+  const int64_t ch = chunk_columns(c, p, true, U != nullptr, kappa != nullptr, V != nullptr, Vtop || Vbot);
   CU(c->pil.ensure((size_t)ch * nz * record_bytes(p->form)));
   for (auto &st : c->stage) {
     CU(st.rho.ensure((size_t)ch * nz * sizeof(double)));
