@@ -20,6 +20,7 @@ import math
 getcontext().prec = 80
 
 EXP_N = 128            # exp table: 2^(j/128), j = 0..127
+EXP_FAST_N = 1024      # fast exp phase: 2^(j/1024), j = 0..1023
 LOG_N = 128            # log table: F = 1 + j/128, j = LOG_JMIN..LOG_JMAX
 LOG_JMIN, LOG_JMAX = -32, 64
 
@@ -107,6 +108,20 @@ def main():
     lines.append(f"#define OCO_EXP_L1 {h(L1)}  /* ln2/N, 35 significant bits */")
     lines.append(f"#define OCO_EXP_L2 {h(L2)}")
     lines.append(f"#define OCO_EXP_L3 {h(L3)}")
+    # Fast exp phase: 2^(j/1024) as (hi, lo) and a Cody-Waite split of ln2/1024 whose head has
+    # 32 significant bits, so that k*L1 is exact for |k| < 2^21 (|x| <= 746 gives |k| <= 1.11e6).
+    exp_fast = [dd((Decimal(j) / EXP_FAST_N * LN2).exp()) for j in range(EXP_FAST_N)]
+    lines.append(f"#define OCO_EXPF_N {EXP_FAST_N}")
+    lines.append(emit_pairs("oco_expf_tab", exp_fast))
+    lf = LN2 / EXP_FAST_N
+    F1 = trunc_bits(lf, 32)
+    rf = lf - Decimal(F1)
+    F2 = rn(rf)
+    F3 = rn(rf - Decimal(F2))
+    lines.append(f"#define OCO_EXPF_INVLN2N {h(rn(EXP_FAST_N / LN2))}  /* 1024/ln2 */")
+    lines.append(f"#define OCO_EXPF_L1 {h(F1)}  /* ln2/1024, 32 significant bits */")
+    lines.append(f"#define OCO_EXPF_L2 {h(F2)}")
+    lines.append(f"#define OCO_EXPF_L3 {h(F3)}")
     # ln2 for the log reconstruction: 42-bit head so that e*LN2_HI is exact for |e| < 2^11.
     LN2_HI = trunc_bits(LN2, 42)
     LN2_LO = rn(LN2 - Decimal(LN2_HI))

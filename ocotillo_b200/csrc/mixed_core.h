@@ -145,11 +145,6 @@ MX_HD float rcp(float x) {
 }
 
 MX_HD float fmaxf_(float a, float b) { return a > b ? a : b; }
-/* log2(2^a + 2^b) */
-MX_HD float lae2(float a, float b) {
-  float m = fmaxf_(a, b), d = (a > b) ? b - a : a - b;
-  return m + lg2(1.0f + ex2(d));
-}
 /* log2(1 - 2^-t) for t > 0 (accurate to a few 1e-7 relative of the result's argument
  * for t >= 2^-6; a two-term series below that). */
 MX_HD float log2_one_minus_exp2neg(float t) {
@@ -277,10 +272,10 @@ MX_HD Opac32 opacity(const Rec &Z, const Lam32 &L) {
   const float t10 = L.cl2 * Z[MZ_TH];
   const float ls = (t10 > 40.0f) ? 0.0f : log2_one_minus_exp2neg(t10);
   /* H bound-free (c_o :233-244): log2(AHbf wa^3) + ls + log2 ionf + log2(unsold + sm) */
-  float lsum = kNeg;
+  float lsum = kNeg, sm = 0.0f;
   const int n0 = L.n0;
   if (n0 <= 6) {
-    float sm = L.g[0];
+    sm = L.g[0];
 #pragma unroll
     for (int n = 2; n <= 6; n++) sm = (n == n0) ? L.g[n - 1] : sm; /* L.g[n0-1] without local memory */
     int q = 0;
@@ -292,10 +287,11 @@ MX_HD Opac32 opacity(const Rec &Z, const Lam32 &L) {
         q++;
       }
     }
-    const float le0 = (n0 >= 2) ? Z[MZ_LE2 + n0 - 2] : 0.0f;
-    lsum = le0 + lg2(sm);
+    lsum = (n0 >= 2) ? Z[MZ_LE2 + n0 - 2] : 0.0f; /* log2 E_n0; the sum is E_n0 * sm */
   }
-  const float lbf = lae2(Z[MZ_LU], lsum);
+  /* log2(Unsold + E_n0 sm) relative to the larger of the two scales (one SFU pair) */
+  const float LU = Z[MZ_LU];
+  const float lbf = (LU >= lsum) ? LU + lg2(1.0f + ex2(lsum - LU) * sm) : lsum + lg2(ex2(LU - lsum) + sm);
   const float A = ((L.law + ls) + Z[MZ_LIONF]) + lbf;
   /* H- bound-free (c_o :318-322) */
   const float B = (ls + Z[MZ_LHM]) + L.ls;
@@ -304,26 +300,37 @@ MX_HD Opac32 opacity(const Rec &Z, const Lam32 &L) {
   const float D = Z[MZ_LESC];
   const float m = fmaxf_(fmaxf_(A, B), fmaxf_(C, D));
   const float eA = ex2(A - m), eB = ex2(B - m), eC = ex2(C - m), eD = ex2(D - m);
-  const float lsig = m + lg2((eA + eB) + (eC + eD)); /* log2 of the sum per H */
-  const float labs0 = m + lg2(fmaxf_((eA + eB) + eC, 1e-37f));
-  const float lkr0 = lsig + log2mp1; /* log2 kappa_rad before the free-free part */
+  const float S4 = (eA + eB) + (eC + eD); /* sum per H / 2^m, in [1, 4] */
+  const float S3 = (eA + eB) + eC;        /* absorption part (no Thomson) */
+  const float X = m + log2mp1;            /* per-mass scale of S4 and S3 */
+  /* Every output is one lg2 of a linear combination scaled to M = max(X, extra term); of the
+   * two scale factors one is exactly 1. */
   Opac32 o;
   float lkr, labs;
-  if (Z[MZ_NEUTRAL] != 0.0f) { /* c_o :262-268 */
+  if (Z[MZ_NEUTRAL] != 0.0f) { /* c_o :262-268: kappa = rho (2 kr0 + kHff/mp), kappa_rad = kr0 + kHff/mp */
     const float gff = 1.0f + L.gff * (Z[MZ_TH1L] * L.chi1 + 0.5f);
-    const float H = ((ls + Z[MZ_LIONFEF]) + L.lal0w) + lg2(gff); /* log2(kHff * mp1) */
-    o.lk = Z[MZ_LRHO] + lae2(1.0f + lkr0, H);
-    lkr = lae2(lkr0, H);
-    labs = lae2(labs0 + log2mp1, H);
-  } else { /* c_o :270-275, bremsstrahlung :281-300 */
+    const float Hf = ((ls + Z[MZ_LIONFEF]) + L.lal0w) + lg2(gff); /* log2(kHff * mp1) */
+    const bool xs = X >= Hf;
+    const float M = xs ? X : Hf;
+    const float e = ex2(-fabsf(X - Hf));
+    const float es = xs ? 1.0f : e, eh = xs ? e : 1.0f;
+    o.lk = Z[MZ_LRHO] + (M + lg2(2.0f * S4 * es + eh));
+    lkr = M + lg2(S4 * es + eh);
+    labs = M + lg2(S3 * es + eh);
+  } else { /* c_o :270-275, bremsstrahlung :281-300: kappa = rho kr0 + kb, kappa_rad = 2 kr0 + kb/rho */
     const float y = 5.960f - 0.551328895f * (L.lnnu9 + Z[MZ_LNTPOW]); /* sqrt(3)/pi */
     const float gaunt = kLn2_f * lg2(ex2(y * kLog2e_f) + 2.71828183f);
     const float xh = L.hnuk * Z[MZ_T1];
     const float lnq = (Z[MZ_LZ] - L.l3nu) + ((xh > 30.0f) ? 0.0f : kLn2_f * log2_one_minus_exp2neg(xh * kLog2e_f));
     const float lkb = 28.4599637f + lnq * kLog2e_f + lg2(gaunt); /* log2(369234910.67735046) */
-    o.lk = lae2(lkr0 + Z[MZ_LRHO], lkb);
-    lkr = lae2(1.0f + lkr0, lkb - Z[MZ_LRHO]);
-    labs = lae2(lae2(1.0f + labs0 + log2mp1, Z[MZ_LESC] + log2mp1), lkb - Z[MZ_LRHO]);
+    const float K = lkb - Z[MZ_LRHO];                           /* log2(kb / rho) */
+    const bool xs = X >= K;
+    const float M = xs ? X : K;
+    const float e = ex2(-fabsf(X - K));
+    const float es = xs ? 1.0f : e, ek = xs ? e : 1.0f;
+    o.lk = Z[MZ_LRHO] + (M + lg2(S4 * es + ek));
+    lkr = M + lg2(2.0f * S4 * es + ek);
+    labs = M + lg2((2.0f * S3 + eD) * es + ek);
   }
   float l1 = labs - lkr;
   if (l1 > 0.0f) l1 = 0.0f;

@@ -10,14 +10,16 @@
  * (+, -, *, /) and explicit fused multiply-adds, so the two produce identical bits.
  *
  * Method (published algorithms, written from their descriptions):
- *   exp: table-driven reduction x = (128k + j) ln2/128 + r, |r| <= ln2/256
+ *   exp: fast phase (Ziv): reduction by ln2/1024 with a 1024-entry table, accurate to
+ *        2^-73 with a rounding test; when the test cannot decide (probability ~4e-6),
+ *        table-driven reduction x = (128k + j) ln2/128 + r, |r| <= ln2/256
  *        (Tang, ACM TOMS 15(2) 1989), with a three-part Cody-Waite split of ln2/128,
  *        2^(j/128) stored as a double-double, and e^r - 1 evaluated in double-double up
- *        to r^2 and by Horner to r^7.  Pre-rounding relative error < 2^-75.
+ *        to r^2 and by FMA Horner to r^7.  Pre-rounding relative error < 2^-75.
  *   log: x = 2^e m, m in [0.75, 1.5), F = 1 + j/128 nearest to m, f = m - F exact,
  *        log x = e ln2 + log F + log1p(f/F) (Tang, ACM TOMS 16(4) 1990), with 1/F and
  *        log F as double-doubles and log1p by a degree-11 series whose first two terms
- *        are double-double.  Pre-rounding relative error < 2^-78.
+ *        are double-double (the rest by FMA Horner).  Pre-rounding relative error < 2^-78.
  *   pow: exp(y log|x|) with log|x| carried as a double-double; x == 10 uses a
  *        double-double ln10.  C99 Annex F special cases.
  * The results are correctly rounded except in rare hard cases (the exact value within
@@ -95,11 +97,60 @@ OCO_HD double oco_nan(void) { return oco_u2d(0x7ff8000000000000ULL); }
 /* 2^k for -1022 <= k <= 1023, built from the exponent bits. */
 OCO_HD double oco_pow2i(int k) { return oco_u2d((uint64_t)(int64_t)(k + 1023) << 52); }
 
+/* Fast phase of e^(xh + xl) (Ziv's strategy): table of 2^(j/1024); the reduced argument
+ * r = xh - k ln2/1024 (|r| <= 2^-11.5) as rh + rl from a three-part Cody-Waite split (head
+ * exact, rl the exact residual of rh up to 2^-128); e^r - 1 = rh + ql with
+ * ql = rl + rh^2 (1/2 + rh/6 + rh^2/24 + rh^3/120); xl (|xl| <= 2^-44) enters as the factor
+ * 1 + xl, i.e. ql += xl (1 + rh + ql); the result T (1 + q) as hi + lo.  Error of hi + lo
+ * relative to the result below 2^-73.4 (r^6/720 < 2^-78.3; rounding of rh^2 < 2^-77; 2 rh rl
+ * omitted < 2^-76.6; Tl ql omitted < 2^-76; roundings of ql and P < 2^-77, 2^-78).  Returns 1
+ * and the correctly rounded value in *res when the remainder of hi + lo after rounding to
+ * nearest stays more than 2^(e-71) (result in [2^e, 2^(e+1))) inside half an ulp, so that
+ * no value within the error bound rounds differently; returns 0 otherwise (the
+ * double-double phase below then decides).  Normal results only. */
+OCO_HD int oco_exp_fast(double xh, double xl, double *res) {
+  const double shift = 0x1.8p52;
+  const double ks = OCO_FMA(xh, OCO_EXPF_INVLN2N, shift);
+  const double kd = OCO_S(ks, shift);
+  const int ki = (int)(uint32_t)oco_d2u(ks);
+  const int j = ki & (OCO_EXPF_N - 1);
+  const int k = ki >> 10; /* floor(ki / 1024) */
+  if (k <= -1021 || k >= 1023) return 0;
+  const double d = OCO_FMA(-kd, OCO_EXPF_L1, xh); /* exact: k L1 has <= 53 bits, Sterbenz */
+  const double rh = OCO_FMA(-kd, OCO_EXPF_L2, d);
+  double rl = OCO_FMA(-kd, OCO_EXPF_L2, OCO_S(d, rh)); /* d - k L2 - rh, one rounding */
+  rl = OCO_FMA(-kd, OCO_EXPF_L3, rl);
+  const double s = OCO_M(rh, rh);
+  double P = OCO_FMA(rh, OCO_EXP_C5, OCO_EXP_C4);
+  P = OCO_FMA(rh, P, OCO_EXP_C3);
+  P = OCO_FMA(rh, P, 0.5);
+  double ql = OCO_FMA(s, P, rl);
+  ql = OCO_A(ql, OCO_FMA(xl, OCO_A(rh, ql), xl)); /* (1 + q)(1 + xl) - 1 - rh */
+  const double Th = OCO_TAB(oco_expf_tab, 2 * j), Tl = OCO_TAB(oco_expf_tab, 2 * j + 1);
+  const double m = OCO_M(Th, rh);
+  const double me = OCO_FMA(Th, rh, -m);
+  const double hh = OCO_A(Th, m); /* Fast2Sum, |Th| >= 1 > |m| */
+  const double e2 = OCO_S(m, OCO_S(hh, Th));
+  const double lo = OCO_A(e2, OCO_A(me, OCO_FMA(Th, ql, OCO_FMA(Tl, rh, Tl))));
+  const double v = OCO_A(hh, lo);
+  const double t = OCO_S(lo, OCO_S(v, hh)); /* exact: v + t = hh + lo */
+  const uint64_t vb = oco_d2u(v);
+  const int ve = (int)(vb >> 52); /* v in (0.99, 2.01): positive, normal */
+  double half = oco_u2d((uint64_t)(ve - 53) << 52);
+  if ((vb & 0x000fffffffffffffULL) == 0 && t < 0.0) half = OCO_M(half, 0.5); /* power of two: finer grid below */
+  const double bound = OCO_S(half, oco_u2d((uint64_t)(ve - 71) << 52));
+  if (!(fabs(t) < bound)) return 0;
+  *res = OCO_M(v, oco_pow2i(k));
+  return 1;
+}
+
 /* e^(xh + xl) for a double-double argument with |xl| <= ulp(xh). */
 OCO_HD double oco_exp_dd(double xh, double xl) {
   if (oco_isnan(xh)) return OCO_A(xh, xh);
   if (xh > 709.8) return oco_inf();
   if (xh < -746.0) return 0.0;
+  double fast;
+  if (oco_exp_fast(xh, xl, &fast)) return fast;
   /* kd = nearest integer to x * 128/ln2; its value also sits in the low bits of the
    * shifted sum (|kd| < 2^18), which gives j and k without a conversion. */
   const double shift = 0x1.8p52;
@@ -126,10 +177,10 @@ OCO_HD double oco_exp_dd(double xh, double xl) {
   double se = OCO_FMA(rh, rh, -s);
   double half = OCO_M(0.5, s);
   double halfe = OCO_A(OCO_M(0.5, se), OCO_M(rh, rl));
-  double P = OCO_A(OCO_EXP_C6, OCO_M(rh, OCO_EXP_C7));
-  P = OCO_A(OCO_EXP_C5, OCO_M(rh, P));
-  P = OCO_A(OCO_EXP_C4, OCO_M(rh, P));
-  P = OCO_A(OCO_EXP_C3, OCO_M(rh, P));
+  double P = OCO_FMA(rh, OCO_EXP_C7, OCO_EXP_C6);
+  P = OCO_FMA(rh, P, OCO_EXP_C5);
+  P = OCO_FMA(rh, P, OCO_EXP_C4);
+  P = OCO_FMA(rh, P, OCO_EXP_C3);
   P = OCO_M(OCO_M(s, rh), P);
   double qh = OCO_A(rh, half); /* Fast2Sum, |rh| >= |half| */
   double ql = OCO_A(OCO_S(half, OCO_S(qh, rh)), OCO_A(rl, OCO_A(halfe, P)));
@@ -191,14 +242,14 @@ OCO_HD void oco_log_dd(double x, double *lh, double *ll) {
   double se = OCO_FMA(uh, uh, -s);
   double half = OCO_M(0.5, s);
   double halfe = OCO_A(OCO_M(0.5, se), OCO_M(uh, ul));
-  double P = OCO_S(OCO_LOG_C10, OCO_M(uh, OCO_LOG_C11));
-  P = OCO_S(OCO_LOG_C9, OCO_M(uh, P));
-  P = OCO_S(OCO_LOG_C8, OCO_M(uh, P));
-  P = OCO_S(OCO_LOG_C7, OCO_M(uh, P));
-  P = OCO_S(OCO_LOG_C6, OCO_M(uh, P));
-  P = OCO_S(OCO_LOG_C5, OCO_M(uh, P));
-  P = OCO_S(OCO_LOG_C4, OCO_M(uh, P));
-  P = OCO_S(OCO_LOG_C3, OCO_M(uh, P));
+  double P = OCO_FMA(-uh, OCO_LOG_C11, OCO_LOG_C10);
+  P = OCO_FMA(-uh, P, OCO_LOG_C9);
+  P = OCO_FMA(-uh, P, OCO_LOG_C8);
+  P = OCO_FMA(-uh, P, OCO_LOG_C7);
+  P = OCO_FMA(-uh, P, OCO_LOG_C6);
+  P = OCO_FMA(-uh, P, OCO_LOG_C5);
+  P = OCO_FMA(-uh, P, OCO_LOG_C4);
+  P = OCO_FMA(-uh, P, OCO_LOG_C3);
   P = OCO_M(OCO_M(s, uh), P);
   double qh = OCO_S(uh, half); /* Fast2Sum, |uh| >= |half| */
   double ql = OCO_A(OCO_S(OCO_S(uh, qh), half), OCO_A(OCO_S(ul, halfe), P));
