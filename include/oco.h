@@ -133,6 +133,22 @@ int64_t oco_kernel_launches(const oco_ctx *ctx);
 int oco_set_profiling(oco_ctx *ctx, int enable);
 int oco_kernel_times(oco_ctx *ctx, double *solve_ms, double *pillars_ms, int64_t *solve_launches);
 
+/* Upward and downward intensities of a block solved on the device: Ip = U + V, Im = U - V on
+ * the interior z (auxiliary.f90:80-94, calc_intensity, which the reference keeps but does not
+ * call).  U, V, Ip, Im are device arrays in p->layout (Ip and Im shaped like V; either may be
+ * NULL); enqueued on `stream`. */
+int oco_intensities_device(oco_ctx *ctx, const oco_params *p, const double *U, const double *V, double *Ip,
+                           double *Im, void *stream);
+
+/* Optical depth and photosphere of a block solved on the device, as the reference's analysis
+ * tools define them (tools/ocoutils/ReadOcotillo.py:248-293): tau(z) = cumulative sum from z
+ * index 1 of kappa * rho * dz (kappa as the solve wrote it, rho the block's input), and per
+ * (column, wavelength) the first 0-based z index with tau >= target_tau, or -1.  kappa and
+ * tau in p->layout, rho (nz, ny, nx), photo_index (ny, nx, nw) like Vtop; tau or photo_index
+ * may be NULL.  Enqueued on `stream`. */
+int oco_optical_depth_device(oco_ctx *ctx, const oco_params *p, const double *kappa, const double *rho,
+                             double target_tau, double *tau, int32_t *photo_index, void *stream);
+
 /* Diagnostic of the failure path: runs the kernels' bounded wait (the mbarrier poll the
  * solve kernels use for their shared-memory copies) on a barrier phase that nothing
  * completes, polling spin_limit times.  Returns OCO_ETIMEDOUT when the wait ran out, as a

@@ -31,6 +31,7 @@ UNITS = [
     ("oco_api.cu", []),
     ("oco_noalloc.cu", []),
     ("oco_batch.cu", []),
+    ("kernels_epilogue.cu", ["-fmad=false"]),
     ("oco_server.cu", []),
 ]
 HOST_UNITS = [("oco_deck.cpp", [])]

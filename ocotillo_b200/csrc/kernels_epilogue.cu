@@ -1,0 +1,78 @@
+/*
+ * kernels_epilogue.cu -- per-(column, wavelength) quantities derived from a solved block, on
+ * the device where the block's arrays already are:
+ *   k_intensities     I+ = U + V and I- = U - V on the interior z (auxiliary.f90:80-94,
+ *                     calc_intensity: upward and downward intensities);
+ *   k_optical_depth   tau(z) = cumulative sum over z from index 1 of kappa rho dz, and the
+ *                     first z index where tau reaches a target (tools/ocoutils/ReadOcotillo.py:
+ *                     248-293, calculate_optical_depth and find_photosphere), -1 if never.
+ * One thread per item, z loop inside; compiled without FMA contraction so that the products
+ * and the running sum round as the reference tools' array arithmetic does.
+ */
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "oco_internal.h"
+
+namespace oco {
+
+/* Address arithmetic of one block's arrays (see EpilogueArgs). */
+__device__ __forceinline__ void item_bases(const EpilogueArgs &a, int64_t item, int64_t &iu, int64_t &iz,
+                                           int64_t &zs_u, int64_t &zs) {
+  const int64_t ncol = a.ncol;
+  const int64_t col = item % ncol, iw = item / ncol; /* item = iw * ncol + col */
+  if (a.layout == 0) {                               /* (nw, ncol, nz[+6]), z fastest */
+    iu = (iw * ncol + col) * (a.nz + 6);
+    iz = (iw * ncol + col) * a.nz;
+    zs_u = zs = 1;
+  } else { /* [z][col][lambda] */
+    iu = iz = col * a.nw + iw;
+    zs_u = zs = ncol * a.nw;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_intensities(const EpilogueArgs a) {
+  const int64_t items = a.ncol * a.nw;
+  for (int64_t item = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; item < items;
+       item += (int64_t)gridDim.x * blockDim.x) {
+    int64_t iu, iz, zs_u, zs;
+    item_bases(a, item, iu, iz, zs_u, zs);
+    for (int z = 0; z < a.nz; z++) {
+      const double u = a.U[iu + (int64_t)(z + 3) * zs_u], v = a.V[iz + (int64_t)z * zs];
+      if (a.Ip) a.Ip[iz + (int64_t)z * zs] = u + v;
+      if (a.Im) a.Im[iz + (int64_t)z * zs] = u - v;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_optical_depth(const EpilogueArgs a) {
+  const int64_t items = a.ncol * a.nw;
+  for (int64_t item = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; item < items;
+       item += (int64_t)gridDim.x * blockDim.x) {
+    int64_t iu, iz, zs_u, zs;
+    item_bases(a, item, iu, iz, zs_u, zs);
+    const int64_t col = item % a.ncol;
+    const double *rho = a.rho + col * a.nz;
+    double tau = 0.0;
+    int photo = -1;
+    for (int z = 0; z < a.nz; z++) {
+      tau = tau + (a.K[iz + (int64_t)z * zs] * rho[z]) * a.dz;
+      if (a.tau) a.tau[iz + (int64_t)z * zs] = tau;
+      if (photo < 0 && tau >= a.target) photo = z;
+    }
+    if (a.photo) a.photo[item] = photo;
+  }
+}
+
+cudaError_t launch_intensities(const EpilogueArgs &a, int blocks, cudaStream_t s) {
+  k_intensities<<<blocks, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_optical_depth(const EpilogueArgs &a, int blocks, cudaStream_t s) {
+  k_optical_depth<<<blocks, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace oco

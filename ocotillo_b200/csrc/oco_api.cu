@@ -591,6 +591,60 @@ extern "C" int oco_synchronize(oco_ctx *c) {
   return OCO_OK;
 }
 
+static int epilogue_args(oco_ctx *c, const oco_params *p, EpilogueArgs &a) {
+  if (!c) return oco_set_err(nullptr, OCO_EINVAL, "NULL context");
+  if (!p || p->nx < 1 || p->ny < 1 || p->nz < 2 || p->nw < 1)
+    return oco_set_err(c, OCO_EINVAL, "bad block dimensions");
+  if (p->layout != OCO_LAYOUT_REFERENCE && p->layout != OCO_LAYOUT_LAMBDA_FASTEST)
+    return oco_set_err(c, OCO_EINVAL, "unknown layout %d", p->layout);
+  a = EpilogueArgs{};
+  a.ncol = (int64_t)p->nx * p->ny;
+  a.nz = p->nz;
+  a.nw = p->nw;
+  a.layout = p->layout;
+  a.dz = p->dz;
+  return OCO_OK;
+}
+
+static int epilogue_blocks(oco_ctx *c, int64_t items) {
+  const int64_t want = (items + 255) / 256, cap = (int64_t)c->num_sms * 8;
+  return (int)std::max<int64_t>(1, std::min(want, cap));
+}
+
+extern "C" int oco_intensities_device(oco_ctx *c, const oco_params *p, const double *U, const double *V, double *Ip,
+                                      double *Im, void *stream) {
+  EpilogueArgs a;
+  int rc = epilogue_args(c, p, a);
+  if (rc) return rc;
+  if (!U || !V || (!Ip && !Im)) return oco_set_err(c, OCO_EINVAL, "U, V and at least one of Ip, Im are required");
+  a.U = U;
+  a.V = V;
+  a.Ip = Ip;
+  a.Im = Im;
+  CU(cudaSetDevice(c->device));
+  CU(launch_intensities(a, epilogue_blocks(c, a.ncol * a.nw), (cudaStream_t)stream));
+  c->launches++;
+  return OCO_OK;
+}
+
+extern "C" int oco_optical_depth_device(oco_ctx *c, const oco_params *p, const double *kappa, const double *rho,
+                                        double target_tau, double *tau, int32_t *photo_index, void *stream) {
+  EpilogueArgs a;
+  int rc = epilogue_args(c, p, a);
+  if (rc) return rc;
+  if (!kappa || !rho || (!tau && !photo_index))
+    return oco_set_err(c, OCO_EINVAL, "kappa, rho and at least one of tau, photo_index are required");
+  a.K = kappa;
+  a.rho = rho;
+  a.tau = tau;
+  a.photo = photo_index;
+  a.target = target_tau;
+  CU(cudaSetDevice(c->device));
+  CU(launch_optical_depth(a, epilogue_blocks(c, a.ncol * a.nw), (cudaStream_t)stream));
+  c->launches++;
+  return OCO_OK;
+}
+
 extern "C" int oco_check_bounded_wait(oco_ctx *c, int64_t spin_limit) {
   if (!c) return oco_set_err(nullptr, OCO_EINVAL, "NULL context");
   if (spin_limit < 0 || spin_limit > (1ll << 30)) return oco_set_err(c, OCO_EINVAL, "spin_limit must be 0..2^30");

@@ -158,6 +158,21 @@ cudaError_t launch_pillars_mixed_batch(const double *rho, const double *T, const
 cudaError_t launch_batch_mixed(const MixedBatchArgs &a, int tiling, int blocks, int threads, cudaStream_t s);
 int batch_mixed_max_blocks_per_sm(int tiling, int threads);
 
+/* Arguments of the epilogue kernels (kernels_epilogue.cu) over one block's device arrays:
+ * layout 0: U (nw, ncol, nz+6), z-indexed arrays (nw, ncol, nz), z fastest;
+ * layout 1: U [nz+6][ncol][nw], z-indexed arrays [nz][ncol][nw];
+ * rho (ncol, nz); per-item planes (nw, ncol). */
+struct EpilogueArgs {
+  const double *U, *V, *K, *rho;
+  double *Ip, *Im, *tau;
+  int32_t *photo;
+  int64_t ncol;
+  int nz, nw, layout;
+  double dz, target;
+};
+cudaError_t launch_intensities(const EpilogueArgs &a, int blocks, cudaStream_t s);
+cudaError_t launch_optical_depth(const EpilogueArgs &a, int blocks, cudaStream_t s);
+
 /* Fills tab[NL*nw] (layout [field][iw]) with the wavelength table of waves[nw] (Angstrom):
  * pre_calc_opacity_quantities' arithmetic plus the hot loop's lambda-only factors
  * (defined in oco_api.cu). */

@@ -115,6 +115,8 @@ def load_library(path=None):
         "oco_synchronize": (I, [V]),
         "oco_kernel_launches": (ctypes.c_int64, [V]),
         "oco_check_bounded_wait": (I, [V, ctypes.c_int64]),
+        "oco_intensities_device": (I, [V, P, V, V, V, V, V]),
+        "oco_optical_depth_device": (I, [V, P, V, V, D, V, V, V]),
         "oco_set_profiling": (I, [V, I]),
         "oco_kernel_times": (I, [V, _DP, _DP, ctypes.POINTER(ctypes.c_int64)]),
         "oco_solve_block_noalloc": (I, [P, _DP, V, V, V, V, V, V, V, V]),
@@ -318,6 +320,33 @@ class Engine:
 
     def synchronize(self):
         self._check(self.lib.oco_synchronize(self.ctx))
+
+    def intensities_device(self, U, V, shape, nw, out, layout=LAYOUT_REFERENCE, stream=None):
+        """Ip = U + V, Im = U - V (calc_intensity) on torch CUDA tensors of a solved block of
+        shape (nx, ny, nz) with nw wavelengths; `out` maps 'Ip' and/or 'Im' to tensors shaped
+        like V."""
+        import torch
+        if stream is None:
+            stream = torch.cuda.current_stream(U.device)
+        prm = self.params(shape, nw, 1.0, layout=layout)
+        p = lambda t: ctypes.c_void_p(t.data_ptr()) if t is not None else None
+        self._check(self.lib.oco_intensities_device(self.ctx, ctypes.byref(prm), p(U), p(V), p(out.get("Ip")),
+                                                    p(out.get("Im")), ctypes.c_void_p(stream.cuda_stream)))
+        return out
+
+    def optical_depth_device(self, kappa, rho, dz, target_tau=1.0, tau=None, photo=None, layout=LAYOUT_REFERENCE,
+                             stream=None):
+        """tau = cumsum_z(kappa rho dz) and the photosphere index (first z with tau >= target,
+        -1 if none) on torch CUDA tensors of a solved block; rho (nx, ny, nz)."""
+        import torch
+        if stream is None:
+            stream = torch.cuda.current_stream(kappa.device)
+        nx, ny, nz = rho.shape
+        nw = kappa.numel() // (nx * ny * nz)
+        prm = self.params((nx, ny, nz), nw, dz, layout=layout)
+        p = lambda t: ctypes.c_void_p(t.data_ptr()) if t is not None else None
+        self._check(self.lib.oco_optical_depth_device(self.ctx, ctypes.byref(prm), p(kappa), p(rho), float(target_tau),
+                                                      p(tau), p(photo), ctypes.c_void_p(stream.cuda_stream)))
 
     def check_bounded_wait(self, spin_limit=100):
         """Return code of the bounded-wait diagnostic (OCO_ETIMEDOUT = -6 expected)."""
