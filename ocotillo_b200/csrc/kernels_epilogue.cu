@@ -76,3 +76,42 @@ cudaError_t launch_optical_depth(const EpilogueArgs &a, int blocks, cudaStream_t
 }
 
 }  // namespace oco
+
+namespace oco {
+
+/* Reference-layout output from a lambda-fastest chunk: for each column col of the chunk, the
+ * (rows x nw) plane src[z * src_zs + col * nw + iw] goes to dst[(iw * ld_col + c_off + col) *
+ * rows + z].  32 x 32 tiles through shared memory, so that the reads run along lambda and the
+ * writes along z, both coalesced.  Block (32, 8); grid (ceil(nw/32), ceil(rows/32), <= 65535)
+ * with a loop over columns. */
+__global__ void __launch_bounds__(256) k_lambda_to_reference(const double *__restrict__ src, int64_t src_zs,
+                                                             double *__restrict__ dst, int64_t ld_col,
+                                                             int64_t c_off, int64_t nb, int rows, int nw) {
+  __shared__ double tile[32][33];
+  const int w0 = blockIdx.x * 32, z0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int64_t col = blockIdx.z; col < nb; col += gridDim.z) {
+#pragma unroll
+    for (int i = 0; i < 32; i += 8) {
+      const int z = z0 + ty + i, iw = w0 + tx;
+      if (z < rows && iw < nw) tile[ty + i][tx] = src[(int64_t)z * src_zs + col * nw + iw];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 32; i += 8) {
+      const int iw = w0 + ty + i, z = z0 + tx;
+      if (z < rows && iw < nw) dst[((int64_t)iw * ld_col + c_off + col) * rows + z] = tile[tx][ty + i];
+    }
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_lambda_to_reference(const double *src, int64_t src_zs, double *dst, int64_t ld_col, int64_t c_off,
+                                       int64_t nb, int rows, int nw, cudaStream_t s) {
+  if (nb <= 0) return cudaSuccess;
+  const dim3 grid((unsigned)((nw + 31) / 32), (unsigned)((rows + 31) / 32), (unsigned)(nb < 65535 ? nb : 65535));
+  k_lambda_to_reference<<<grid, dim3(32, 8), 0, s>>>(src, src_zs, dst, ld_col, c_off, nb, rows, nw);
+  return cudaGetLastError();
+}
+
+}  // namespace oco

@@ -71,6 +71,7 @@ extern "C" int oco_create(oco_ctx **out, int device) {
     oco_destroy(c);
     return code;
   }
+  if (const char *r = getenv("OCO_REFERENCE_STORES")) c->ref_transpose = strcmp(r, "direct") != 0;
   if (const char *g = getenv("OCO_WORKSPACE_GB")) {
     double gb = atof(g);
     if (gb > 0.0) c->budget_bytes = std::max<size_t>((size_t)(gb * (1ull << 30)), 1);
@@ -88,6 +89,9 @@ extern "C" void oco_destroy(oco_ctx *c) {
   c->lam32.release();
   c->pil.release();
   c->scratch.release();
+  c->tmpU.release();
+  c->tmpK.release();
+  c->tmpV.release();
   c->work.release();
   c->status.release();
   for (auto &s : c->stage) {
@@ -271,6 +275,12 @@ static int prepare_solve(oco_ctx *c, int form, int grey, int64_t nitems, int nz,
   return OCO_OK;
 }
 
+/* Reference-layout outputs of a device solve go through lambda-fastest temporaries and a
+ * tiled transpose (coalesced stores) unless disabled or pointless (grey / few wavelengths). */
+static bool uses_transpose(const oco_ctx *c, const oco_params *p, bool u, bool k, bool v) {
+  return c->ref_transpose && p->layout == OCO_LAYOUT_REFERENCE && !p->lgrey && p->nw >= 8 && (u || k || v);
+}
+
 /* Bytes of the per-(column, z) record of a form: the FP64 pillar or the mixed record. */
 static size_t record_bytes(int form) {
   return form == OCO_FORM_MIXED ? MIXED_ZN * sizeof(float) : NF * sizeof(double);
@@ -286,6 +296,9 @@ static int64_t chunk_columns(oco_ctx *c, const oco_params *p, bool host_path, bo
                          (planes ? 2 : 0);
     per_col += 2 * ((size_t)p->nz * 2 + (size_t)p->nw * per_w) * sizeof(double);
   }
+  if (!host_path && uses_transpose(c, p, u, k, v)) /* lambda-fastest temporaries of the chunk */
+    per_col += (size_t)p->nw * ((u ? (size_t)(p->nz + 6) : 0) + (k ? (size_t)p->nz : 0) + (v ? (size_t)p->nz : 0)) *
+               sizeof(double);
   int64_t ch = (int64_t)std::max<size_t>(1, c->budget_bytes / per_col);
   return std::min(ch, ncol);
 }
@@ -429,6 +442,52 @@ static void fill_strides(SolveArgs &a, const oco_params *p, int layout, int64_t 
   }
 }
 
+/* One chunk [c0, c0 + nb) of a device solve into the caller's arrays (whole-block strides, layout
+ * p->layout); reference-layout U, kappa, V go through lambda-fastest temporaries and a transpose. */
+static int device_chunk(oco_ctx *c, const oco_params *p, const double *rho, const double *T, int64_t c0, int64_t nb,
+                        double *U, double *kappa, double *V, double *Vtop, double *Vbot, cudaStream_t s) {
+  const int64_t ncol = (int64_t)p->nx * p->ny;
+  SolveArgs a{};
+  a.nz = p->nz;
+  a.nw = p->nw;
+  a.dz = p->dz;
+  a.dz1 = 1.0 / p->dz;
+  a.dz2 = p->dz * p->dz;
+  a.sigma_grey = p->sigma_grey;
+  if (!uses_transpose(c, p, U != nullptr, kappa != nullptr, V != nullptr)) {
+    fill_strides(a, p, p->layout, ncol);
+    a.U = U;
+    a.K = kappa;
+    a.V = V;
+    a.Vtop = Vtop;
+    a.Vbot = Vbot;
+    a.c_off = c0;
+    return run_chunk(c, p, rho + c0 * p->nz, T + c0 * p->nz, nb, a, s);
+  }
+  const int nz = p->nz, nw = p->nw, mz = nz + 6;
+  const int64_t items = nb * nw;
+  if (U) CU(c->tmpU.ensure((size_t)items * mz * sizeof(double)));
+  if (kappa) CU(c->tmpK.ensure((size_t)items * nz * sizeof(double)));
+  if (V) CU(c->tmpV.ensure((size_t)items * nz * sizeof(double)));
+  a.layout = OCO_LAYOUT_LAMBDA_FASTEST;
+  a.ld_col = ncol; /* emergent planes: caller's plane, offset below */
+  a.c_off = 0;
+  a.U_zs = a.K_zs = a.V_zs = items;
+  a.U_is = a.K_is = a.V_is = 1;
+  a.U = U ? c->tmpU.as<double>() : nullptr;
+  a.K = kappa ? c->tmpK.as<double>() : nullptr;
+  a.V = V ? c->tmpV.as<double>() : nullptr;
+  a.Vtop = Vtop ? Vtop + c0 : nullptr;
+  a.Vbot = Vbot ? Vbot + c0 : nullptr;
+  int rc = run_chunk(c, p, rho + c0 * p->nz, T + c0 * p->nz, nb, a, s);
+  if (rc) return rc;
+  if (U) CU(launch_lambda_to_reference(c->tmpU.as<double>(), items, U, ncol, c0, nb, mz, nw, s));
+  if (kappa) CU(launch_lambda_to_reference(c->tmpK.as<double>(), items, kappa, ncol, c0, nb, nz, nw, s));
+  if (V) CU(launch_lambda_to_reference(c->tmpV.as<double>(), items, V, ncol, c0, nb, nz, nw, s));
+  c->launches += (U ? 1 : 0) + (kappa ? 1 : 0) + (V ? 1 : 0);
+  return OCO_OK;
+}
+
 extern "C" int oco_solve_block_device(oco_ctx *c, const oco_params *p, const double *rho, const double *T,
                                       double *U, double *kappa, double *V, double *Vtop, double *Vbot,
                                       void *stream) {
@@ -439,26 +498,12 @@ extern "C" int oco_solve_block_device(oco_ctx *c, const oco_params *p, const dou
   CU(cudaSetDevice(c->device));
   cudaStream_t s = (cudaStream_t)stream; /* NULL is the CUDA default stream */
   const int64_t ncol = (int64_t)p->nx * p->ny;
-  const int64_t ch = chunk_columns(c, p, false);
+  const int64_t ch = chunk_columns(c, p, false, U != nullptr, kappa != nullptr, V != nullptr, Vtop || Vbot);
   CU(c->pil.ensure((size_t)ch * p->nz * record_bytes(p->form)));
   if ((rc = reset_status(c, s))) return rc;
-  SolveArgs a{};
-  fill_strides(a, p, p->layout, ncol);
-  a.nz = p->nz;
-  a.nw = p->nw;
-  a.dz = p->dz;
-  a.dz1 = 1.0 / p->dz;
-  a.dz2 = p->dz * p->dz;
-  a.sigma_grey = p->sigma_grey;
   for (int64_t c0 = 0; c0 < ncol; c0 += ch) {
     const int64_t nb = std::min(ch, ncol - c0);
-    a.U = U;
-    a.K = kappa;
-    a.V = V;
-    a.Vtop = Vtop;
-    a.Vbot = Vbot;
-    a.c_off = c0;
-    if ((rc = run_chunk(c, p, rho + c0 * p->nz, T + c0 * p->nz, nb, a, s))) return rc;
+    if ((rc = device_chunk(c, p, rho, T, c0, nb, U, kappa, V, Vtop, Vbot, s))) return rc;
   }
   c->status_pending = true;
   c->status_stream = s;
@@ -470,22 +515,8 @@ int oco_ctx_run_columns(oco_ctx *c, const oco_params *p, const double *rho, cons
                         double *U, double *kappa, double *V, double *Vtop, double *Vbot, int max_blocks,
                         cudaStream_t s) {
   CU(c->pil.ensure((size_t)nb * p->nz * record_bytes(p->form)));
-  SolveArgs a{};
-  fill_strides(a, p, p->layout, (int64_t)p->nx * p->ny);
-  a.nz = p->nz;
-  a.nw = p->nw;
-  a.dz = p->dz;
-  a.dz1 = 1.0 / p->dz;
-  a.dz2 = p->dz * p->dz;
-  a.sigma_grey = p->sigma_grey;
-  a.U = U;
-  a.K = kappa;
-  a.V = V;
-  a.Vtop = Vtop;
-  a.Vbot = Vbot;
-  a.c_off = c0;
   c->max_blocks = max_blocks;
-  const int rc = run_chunk(c, p, rho + c0 * p->nz, T + c0 * p->nz, nb, a, s);
+  const int rc = device_chunk(c, p, rho, T, c0, nb, U, kappa, V, Vtop, Vbot, s);
   c->max_blocks = 0;
   return rc;
 }

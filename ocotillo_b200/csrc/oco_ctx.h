@@ -60,6 +60,10 @@ struct oco_ctx {
   int64_t launches = 0;
   size_t budget_bytes = 8ull << 30; /* chunk budget for pillars + staged outputs */
   int max_blocks = 0;               /* cap on the persistent grid (0: occupancy limit x SMs) */
+  /* reference-layout device outputs: solve into lambda-fastest temporaries and transpose
+   * (true), or store directly from the solve kernel (OCO_REFERENCE_STORES=direct) */
+  bool ref_transpose = true;
+  DevBuf tmpU, tmpK, tmpV;
   /* kernel timing (oco_set_profiling) */
   bool prof = false;
   /* device-array calls defer the zero-pivot check to oco_synchronize */

@@ -172,6 +172,10 @@ struct EpilogueArgs {
 };
 cudaError_t launch_intensities(const EpilogueArgs &a, int blocks, cudaStream_t s);
 cudaError_t launch_optical_depth(const EpilogueArgs &a, int blocks, cudaStream_t s);
+/* Copies a lambda-fastest chunk plane set (src[z * src_zs + col * nw + iw], rows z values)
+ * into reference-layout arrays (dst[(iw * ld_col + c_off + col) * rows + z]). */
+cudaError_t launch_lambda_to_reference(const double *src, int64_t src_zs, double *dst, int64_t ld_col, int64_t c_off,
+                                       int64_t nb, int rows, int nw, cudaStream_t s);
 
 /* Fills tab[NL*nw] (layout [field][iw]) with the wavelength table of waves[nw] (Angstrom):
  * pre_calc_opacity_quantities' arithmetic plus the hot loop's lambda-only factors

@@ -348,6 +348,9 @@ static int setup_server(oco_server *srv, const oco_server_config *cfg) {
   for (auto &sl : srv->slots) {
     const int rc = oco_create(&sl.ctx, cfg->device);
     if (rc) return serr(rc, "oco_server_create: %s", oco_last_error(nullptr));
+    /* jobs' reference-layout fields are stored directly: transpose temporaries would be sized
+     * by the launch (up to chunk_points) and allocated while other jobs run */
+    sl.ctx->ref_transpose = false;
   }
   for (int f = 0; f < 3; f++) srv->full_blocks[f] = oco_ctx_full_blocks(srv->slots[0].ctx, f, 0);
   /* workspace reserved up front, so that admissions do not reallocate (a free synchronizes
