@@ -21,7 +21,7 @@
 namespace oco {
 using namespace oco::mx;
 
-constexpr int MZC = 32;            /* z records per staged chunk (32 x 160 B) */
+constexpr int MZC = 24;            /* z records per staged chunk (24 x 208 B) */
 constexpr int MWARPS = 4;          /* warps per 128-thread block */
 constexpr long long kMSpinLimit = 1ll << 26;
 #ifndef OCO_MIXED_PREFETCH
@@ -111,34 +111,15 @@ struct MDirect {
 };
 
 __device__ __forceinline__ void load_lam32(Lam32 &L, const float *__restrict__ t, int iw, int nw) {
-#define LF(f) __ldg(t + (int64_t)(f) * nw + iw)
-  L.cl2 = LF(ML_CL2);
-  L.law = LF(ML_LAW);
-#pragma unroll
-  for (int q = 0; q < 6; q++) L.g[q] = LF(ML_G1 + q);
-  L.n0 = (int)LF(ML_N0);
-  L.ls = LF(ML_LS);
-  L.f1 = LF(ML_F1);
-  L.f2 = LF(ML_F2);
-  L.f3 = LF(ML_F3);
-  L.lal0w = LF(ML_LAL0W);
-  L.gff = LF(ML_GFF);
-  L.chi1 = LF(ML_CHI1);
-  L.lnnu9 = LF(ML_LNNU9);
-  L.hnuk = LF(ML_HNUK);
-  L.l3nu = LF(ML_L3NU);
-  L.ch = LF(ML_CH);
-  L.cl = LF(ML_CL);
-  L.lsi = LF(ML_LSI);
-  L.lsf = LF(ML_LSF);
-#undef LF
+  lam32_from(L, [&](int f) { return __ldg(t + (int64_t)f * nw + iw); });
 }
 
 /* Everything one (column, wavelength) item needs besides its records. */
 struct MItem {
   const float *lam; /* wavelength table [MLN][nw] of the item's grid */
   int nz, nw, iw;
-  float dzf, ldz2;  /* dz and log2(dz^2) */
+  float dzf;        /* dz */
+  float ldz2i, ldz2f; /* log2(dz^2) = integer + fraction */
   double dz1;       /* 1/dz */
   double *U;        /* U of z = 0 (ghost zone 0), stride uz, or NULL; written only when active */
   double *K, *V;    /* kappa and V of z = 0 or NULL, strides kz, vz */
@@ -154,7 +135,8 @@ __device__ __forceinline__ MItem block_item(const MixedArgs &a, int64_t cl, int 
   it.nw = a.nw;
   it.iw = iw;
   it.dzf = (float)a.dz;
-  it.ldz2 = a.ldz2;
+  it.ldz2i = a.ldz2i;
+  it.ldz2f = a.ldz2f;
   it.dz1 = 1.0 / a.dz;
   const int64_t idx = (a.layout == 0) ? (int64_t)iw * a.ld_col + a.c_off + cl : (a.c_off + cl) * a.nw + iw;
   it.U = a.U ? a.U + idx * a.U_is : nullptr;
@@ -181,15 +163,15 @@ __device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa
   double *Ub = active ? it.U : nullptr;
   double *Kb = active ? it.K : nullptr;
   double *Vb = active ? it.V : nullptr;
-  const float dzf = it.dzf, ldz2 = it.ldz2;
+  const float dzf = it.dzf, ldz2i = it.ldz2i, ldz2f = it.ldz2f;
 
   Opac32 cur = opacity(pa.at(0), L);
   Opac32 nxt = opacity(pa.at(1), L);
-  float kc = kappa_lin(cur.lk), kn = kappa_lin(nxt.lk), kprev = 0.0f;
-  Row32 r = row_boundary(kc, cur, dzf, ldz2, false);
+  float kc = kappa_lin(cur), kn = kappa_lin(nxt), kprev = 0.0f;
+  Row32 r = row_boundary(kc, cur, dzf, ldz2i, ldz2f, false);
   float h = r.e, cprev = r.c;
   XF u = xexp2(r.ldi, r.ldf);
-  u = xnorm(u.m * rcp(r.c + h), u.e);
+  u = xnorm(u.m * (r.w * rcp(r.c + h)), u.e);
   float o1 = rcp(kc);
   if (Kb) Kb[0] = (double)kc;
   /* scratch record of z = j: {v_j, 1/kappa_j, u_j mantissa, u_j exponent} where v_j holds the
@@ -202,10 +184,10 @@ __device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa
     kc = kn;
     if (j < nz - 1) {
       nxt = opacity(pa.at(j + 1), L);
-      kn = kappa_lin(nxt.lk);
-      r = row_center(kprev, kc, kn, cur, ldz2);
+      kn = kappa_lin(nxt);
+      r = row_center(kprev, kc, kn, cur, ldz2i, ldz2f);
     } else {
-      r = row_boundary(kc, cur, dzf, ldz2, true);
+      r = row_boundary(kc, cur, dzf, ldz2i, ldz2f, true);
     }
     const float rr = rcp(cprev + h);
     const float qv = h * rr, gv = cprev * rr;
@@ -213,7 +195,7 @@ __device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa
     s4[(int64_t)(j - 1) * ss] = pend;
     h = r.e + (r.a * rr) * h; /* a'/(c'+h) is O(1); a' h alone can overflow */
     const float rb = rcp(r.c + h);
-    u = xaxpy(xexp2(r.ldi, r.ldf), rb, u, r.a * rb);
+    u = xaxpy(xexp2(r.ldi, r.ldf), r.w * rb, u, r.a * rb);
     o1 = rcp(kc);
     if (Kb) Kb[(int64_t)j * it.kz] = (double)kc;
     pend = make_float4(0.0f, o1, u.m, (float)u.e);
@@ -437,7 +419,8 @@ __device__ __forceinline__ MItem batch_item(const MixedBatchArgs &b, const MBatc
   it.nw = c.nw;
   it.iw = iw;
   it.dzf = c.dzf;
-  it.ldz2 = c.ldz2;
+  it.ldz2i = c.ldz2i;
+  it.ldz2f = c.ldz2f;
   it.dz1 = c.dz1;
   if (b.layout == 0) { /* per column [lambda][z] (z fastest) */
     it.U = b.U ? b.U + c.u_off + (int64_t)iw * (c.nz + 6) : nullptr;

@@ -5,21 +5,22 @@
  * Same physics and the same linear system as the reference loop
  * (source/flux_feautrier.f90:160-228), evaluated as follows:
  *   - per (column, z), in FP64: Saha ionization and every z-only factor, as in the FP64
- *     pillar kernel, stored as a record of base-2 logarithms (MixedZ) so that nothing
+ *     pillar kernel, stored as a record (MixedZ) of base-2 logarithms so that nothing
  *     underflows (opacity terms per H atom span ~1e-60..1e-17);
  *   - per (z, lambda), in FP32 log2 space: every opacity term of calc_opacity_and_albedo
  *     (continuous_opacity.f90:175-201) is a sum of log2 factors; terms are added with a
- *     log-sum-exp on the SFU (ex2/lg2).  The source function is the one quantity that needs
- *     more: in optically thick cells U ~ S and the flux is a ~1% difference of U, so S (and
- *     the right-hand side S*e') must be good to ~1e-7, while log2 S reaches ~100 (an FP32
- *     logarithm of that size resolves only ~5e-6).  The Planck exponent x*log2(e) is
- *     therefore formed as a double-float product (hi + lo, FMA two-product of split FP32
- *     factors), and log2 S and log2(S e') are carried as an exact integer plus an FP32
- *     fraction.  The H bound-free level sum
+ *     log-sum-exp on the SFU (ex2/lg2).  Logarithms of that size (|log2| up to ~200) would
+ *     resolve only ~1e-5 as FP32 numbers, and a per-cell error of that size in kappa is what
+ *     sensitive columns amplify, so every large logarithm is carried as an exact integer plus
+ *     a small FP32 fraction (L2: i + f, |f| <= 1/2 when stored).  Integers add exactly in
+ *     FP32, the fractions keep ~3e-8 absolute precision, and every 2^x is taken as
+ *     2^int * ex2(fraction): kappa and the source function come out to a few 1e-7.  The
+ *     Planck exponent x*log2(e) is a double-float product (FMA two-product of split FP32
+ *     factors) for the same reason.  The H bound-free level sum
  *     sum_n g(lambda,n) n^-3 exp(-chi_n/kT) (:237-239) is factored by its first non-zero
  *     level n0(lambda): E_n0 * (g_n0 + sum_{n>n0} g_n * E_n/E_n0), with the ratios E_n/E_n0
- *     precomputed per z.  The albedo enters only as log2(1 - omega), computed from the
- *     absorption terms themselves (no cancellation when scattering dominates).  The
+ *     precomputed per z.  The absorption fraction 1 - omega = kappa_abs/kappa_rad is a linear
+ *     ratio of the same sums (one reciprocal; no cancellation when scattering dominates).  The
  *     reference's double addition of the H free-free opacity (:267-268, :274-275) is kept:
  *     neutral cells get kappa = rho (2 kr0 + kHff/mp), kappa_rad = kr0 + kHff/mp; ionized
  *     cells kappa = rho kr0 + k_brems, kappa_rad = 2 kr0 + k_brems/rho.
@@ -37,6 +38,7 @@
 
 #include <math.h>
 #include <stdint.h>
+#include <string.h>
 
 #include "ocomath.h"
 #include "oco_consts.h"
@@ -50,61 +52,55 @@
 namespace oco {
 namespace mx {
 
-/* Per-(column, z) FP32 record: base-2 logarithms of the z-only factors, a few linear values,
- * and damping_factor_const/T split into hi + lo (the Planck exponent needs it to ~1e-12). */
+/* Per-(column, z) FP32 record: the z-only factors.  A large base-2 logarithm takes two
+ * slots, its fraction and then its integer part (value = integer + fraction); the others are
+ * small logarithms or linear values.  damping_factor_const/T is split into hi + lo (the Planck
+ * exponent needs it to ~1e-12). */
 enum MixedZ {
-  MZ_TH = 0,     /* theta = 5040/T */
-  MZ_LIONF,      /* log2(ionization_factor) */
-  MZ_LE2,        /* log2 exp(-chi_n k1 T1), n = 2..6 (n = 1 is 0) */
-  MZ_LE3,
-  MZ_LE4,
-  MZ_LE5,
-  MZ_LE6,
-  MZ_R,          /* 15 ratios E_n/E_n0 for n0 = 1..5, n = n0+1..6 (linear) */
-  MZ_LU = MZ_R + 15, /* log2(Unsold integral) */
-  MZ_LHM,        /* log2(hm_bf_factor * ionf) */
-  MZ_LAFF,       /* log2(ionf ne k T) */
-  MZ_LGT,        /* log10(theta) */
-  MZ_LGT2,       /* log10(theta)^2 */
-  MZ_LESC,       /* log2(e_scatter) */
-  MZ_LRHO,       /* log2(rho) */
-  MZ_NEUTRAL,    /* 1 if (1 - NHII/N) > switch_ionfraction */
-  MZ_LIONFEF,    /* log2(ionf * energyfactor) */
-  MZ_TH1L,       /* theta1 * log10e */
-  MZ_LNTPOW,     /* ln((T*1e-4)^-1.5) */
-  MZ_LZ,         /* ln(ne (nHI+nHII)) - 0.5 ln T */
-  MZ_T1,         /* 1/T */
-  MZ_DFT1,       /* damping_factor_const / T, high part */
-  MZ_DFT1L,      /* low part */
-  MZN = 40       /* 160 B (padded) */
+  MZ_TH = 0,        /* theta = 5040/T */
+  MZ_R,             /* 15 ratios E_n/E_n0 for n0 = 1..5, n = n0+1..6 (linear) */
+  MZ_PU = MZ_R + 15, /* log2(ionf * Unsold integral) [2] */
+  MZ_PE = MZ_PU + 2, /* log2(ionf * exp(-chi_n/kT)), n = 1..6 [2 each] */
+  MZ_LHM = MZ_PE + 12, /* log2(hm_bf_factor * ionf) [2] */
+  MZ_LAFF = MZ_LHM + 2, /* log2(ionf ne k T) [2] */
+  MZ_LESC = MZ_LAFF + 2, /* log2(e_scatter) [2] */
+  MZ_LIONFEF = MZ_LESC + 2, /* log2(ionf * energyfactor) [2] */
+  MZ_LRHO = MZ_LIONFEF + 2, /* log2(rho) [2] */
+  MZ_LZ2 = MZ_LRHO + 2, /* log2(ne (nHI+nHII) T^-1/2) [2] */
+  MZ_LGT = MZ_LZ2 + 2, /* log10(theta) */
+  MZ_LGT2,          /* log10(theta)^2 */
+  MZ_NEUTRAL,       /* 1 if (1 - NHII/N) > switch_ionfraction */
+  MZ_TH1L,          /* theta1 * log10e */
+  MZ_LNTPOW,        /* ln((T*1e-4)^-1.5) */
+  MZ_T1,            /* 1/T */
+  MZ_DFT1,          /* damping_factor_const / T, high part */
+  MZ_DFT1L,         /* low part */
+  MZ_END,
+  MZN = 52          /* 208 B (padded to 16 B) */
 };
+static_assert(MZ_END <= MZN && MZN % 4 == 0, "mixed record layout");
 
-/* Per-wavelength FP32 record (device layout [field][nw]). */
+/* Per-wavelength FP32 record (device layout [field][nw]); [2] as in MixedZ. */
 enum MixedL {
   ML_CL2 = 0,  /* chi * log2(10) */
-  ML_LAW,      /* log2(AHbf * wa^3) */
-  ML_G1,       /* g(lambda,n) * n^-3, n = 1..6 */
-  ML_G2,
-  ML_G3,
-  ML_G4,
-  ML_G5,
-  ML_G6,
-  ML_N0,       /* first level with g > 0 (1..6), 7 if none */
-  ML_LS,       /* log2(s_coeff) if wa < 16000 else -1000 */
-  ML_F1,
-  ML_F2,
-  ML_F3,
-  ML_LAL0W,    /* log2(alpha0 * wa^3 * mp1) */
-  ML_GFF,
+  ML_LAW,      /* log2(AHbf * wa^3) [2] */
+  ML_G1 = ML_LAW + 2, /* g(lambda,n) * n^-3, n = 1..6 */
+  ML_N0 = ML_G1 + 6,  /* first level with g > 0 (1..6), 7 if none */
+  ML_LS,       /* log2(s_coeff) if wa < 16000 else -1000 [2] */
+  ML_FC = ML_LS + 2, /* (f1 - 26) log2(10) [2] */
+  ML_F2 = ML_FC + 2, /* f2 log2(10) */
+  ML_F3,       /* f3 log2(10) */
+  ML_LAL0W,    /* log2(alpha0 * wa^3 * mp1) [2] */
+  ML_GFF = ML_LAL0W + 2,
   ML_CHI1,
   ML_LNNU9,    /* ln(nu * 1e-9) */
   ML_HNUK,     /* h nu / k */
-  ML_L3NU,     /* 3 ln nu */
-  ML_CH,       /* log2(e) / lambda_cm, high part */
+  ML_L3NU,     /* log2(nu^3) [2] */
+  ML_CH = ML_L3NU + 2, /* log2(e) / lambda_cm, high part */
   ML_CL,       /* low part */
   ML_LSI,      /* log2(2 h c^2 lambda_cm^-5) = LSI + LSF, LSI an integer */
   ML_LSF,
-  MLN = 24
+  MLN
 };
 
 constexpr float kNeg = -1000.0f; /* log2 of a vanishing term */
@@ -161,6 +157,12 @@ MX_HD void split2(double v, float &hi, float &lo) {
   hi = (float)v;
   lo = (float)(v - (double)hi);
 }
+/* A large log2 value as fraction o[0] and integer o[1] (nearest integer: |fraction| <= 1/2). */
+MX_HD void put_l2(double v, float *o) {
+  const double i = floor(v + 0.5);
+  o[0] = (float)(v - i);
+  o[1] = (float)i;
+}
 
 /* ---- per-(column, z) record (gas_state.f90:30-110, c_o :143-163) ------------------------ */
 MX_HD void pillar(double r, double t, double fully_ionized_T, float *o) {
@@ -181,37 +183,39 @@ MX_HD void pillar(double r, double t, double fully_ionized_T, float *o) {
     double n1 = 1.0 / (double)n;
     chi[n] = RydbergEnergy * (1.0 - n1 * n1);
   }
+  const double lionf = ionf > 0.0 ? oco_log(ionf) * kLog2e : (double)kNeg;
   o[MZ_TH] = (float)(theta);
-  o[MZ_LIONF] = tolog(ionf);
-  for (int n = 2; n <= 6; n++) o[MZ_LE2 + n - 2] = (-(chi[n] * ktemp1) * kLog2e);
   int q = 0;
   for (int n0 = 1; n0 <= 5; n0++)
     for (int n = n0 + 1; n <= 6; n++) o[MZ_R + q++] = oco_exp(-((chi[n] - chi[n0]) * ktemp1));
   /* Unsold: 0.5 kT/Ry (exp(-chi_6/kT) - exp(-Ry/kT)) = 0.5 kT/Ry e^{-chi_6/kT} (1 - e^{-(Ry-chi_6)/kT}) */
   double lu = oco_log((0.5 * (k_cgs * t)) * RydbergEnergy1) - chi[6] * ktemp1 +
               oco_log(1.0 - oco_exp(-((RydbergEnergy - chi[6]) * ktemp1)));
-  o[MZ_LU] = (float)((lu * kLog2e));
+  put_l2(ionf > 0.0 ? lionf + lu * kLog2e : (double)kNeg, o + MZ_PU);
+  for (int n = 1; n <= 6; n++)
+    put_l2(ionf > 0.0 ? lionf - (chi[n] * ktemp1) * kLog2e : (double)kNeg, o + MZ_PE + 2 * (n - 1));
   /* hm_bf_factor = 4.158e-10 Pe theta^2.5 10^(0.754 theta), in logs */
   double lhm = (Pe > 0.0 && ionf > 0.0)
-                   ? (oco_log(4.158e-10 * Pe) + 2.5 * oco_log(theta)) * kLog2e + 0.754 * theta * kLog2_10 + oco_log(ionf) * kLog2e
+                   ? (oco_log(4.158e-10 * Pe) + 2.5 * oco_log(theta)) * kLog2e + 0.754 * theta * kLog2_10 + lionf
                    : (double)kNeg;
-  o[MZ_LHM] = (float)(lhm);
-  o[MZ_LAFF] = tolog(((ionf * ne) * k_cgs) * t);
-  o[MZ_LGT] = (float)(lgt);
-  o[MZ_LGT2] = (float)((lgt * lgt));
-  o[MZ_LESC] = tolog(escat);
-  o[MZ_LRHO] = (float)((oco_log(r) * kLog2e));
-  o[MZ_NEUTRAL] = (float)(((1.0 - x) > switch_ionfraction) ? 1.0 : 0.0);
+  put_l2(lhm, o + MZ_LHM);
+  const double aff = ((ionf * ne) * k_cgs) * t;
+  put_l2(aff > 0.0 ? oco_log(aff) * kLog2e : (double)kNeg, o + MZ_LAFF);
+  put_l2(escat > 0.0 ? oco_log(escat) * kLog2e : (double)kNeg, o + MZ_LESC);
   /* energyfactor = 0.5 log10e theta1 / Iev * 10^(-theta Iev) */
   double lef = oco_log(((0.5 * log10e) * theta1) * Iev1) * kLog2e - theta * Iev * kLog2_10;
-  o[MZ_LIONFEF] = (float)(ionf > 0.0 ? (lef + oco_log(ionf) * kLog2e) : (double)kNeg);
+  put_l2(ionf > 0.0 ? lef + lionf : (double)kNeg, o + MZ_LIONFEF);
+  put_l2(oco_log(r) * kLog2e, o + MZ_LRHO);
+  double nprod = ne * (nHI + nHII);
+  put_l2(nprod > 0.0 ? (oco_log(nprod) - 0.5 * oco_log(t)) * kLog2e : (double)kNeg, o + MZ_LZ2);
+  o[MZ_LGT] = (float)(lgt);
+  o[MZ_LGT2] = (float)((lgt * lgt));
+  o[MZ_NEUTRAL] = (float)(((1.0 - x) > switch_ionfraction) ? 1.0 : 0.0);
   o[MZ_TH1L] = (float)((theta1 * log10e));
   o[MZ_LNTPOW] = (float)((-1.5 * oco_log(t * 1e-4)));
-  double nprod = ne * (nHI + nHII);
-  o[MZ_LZ] = (float)(nprod > 0.0 ? (oco_log(nprod) - 0.5 * oco_log(t)) : (double)kNeg * kLn2);
   o[MZ_T1] = (float)(T1);
   split2(damping_factor_const * T1, o[MZ_DFT1], o[MZ_DFT1L]);
-  for (int k2 = MZ_DFT1L + 1; k2 < MZN; k2++) o[k2] = 0.0f;
+  for (int k2 = MZ_END; k2 < MZN; k2++) o[k2] = 0.0f;
 }
 
 /* ---- per-wavelength record from the FP64 table entries --------------------------------- */
@@ -221,23 +225,23 @@ struct LamIn {
 MX_HD void lambda_record(const LamIn &L, float *o) {
   using namespace oco::k;
   o[ML_CL2] = (float)(L.chi * kLog2_10);
-  o[ML_LAW] = (float)(oco_log(AHbf * L.wa3) * kLog2e);
+  put_l2(oco_log(AHbf * L.wa3) * kLog2e, o + ML_LAW);
   int n0 = 7;
   for (int n = 6; n >= 1; n--) {
     o[ML_G1 + n - 1] = (float)L.gn[n - 1];
     if (L.gn[n - 1] > 0.0) n0 = n;
   }
   o[ML_N0] = (float)n0;
-  o[ML_LS] = (L.hmon != 0.0 && L.s > 0.0) ? (float)(oco_log(L.s) * kLog2e) : kNeg;
-  o[ML_F1] = (float)L.f1;
-  o[ML_F2] = (float)L.f2;
-  o[ML_F3] = (float)L.f3;
-  o[ML_LAL0W] = (float)(oco_log((alpha0 * L.wa3) * mp1) * kLog2e);
+  put_l2((L.hmon != 0.0 && L.s > 0.0) ? oco_log(L.s) * kLog2e : (double)kNeg, o + ML_LS);
+  put_l2((L.f1 - 26.0) * kLog2_10, o + ML_FC);
+  o[ML_F2] = (float)(L.f2 * kLog2_10);
+  o[ML_F3] = (float)(L.f3 * kLog2_10);
+  put_l2(oco_log((alpha0 * L.wa3) * mp1) * kLog2e, o + ML_LAL0W);
   o[ML_GFF] = (float)L.gff;
   o[ML_CHI1] = (float)L.chi1;
   o[ML_LNNU9] = (float)oco_log(L.nu9);
   o[ML_HNUK] = (float)L.hnuk;
-  o[ML_L3NU] = (float)L.l3nu;
+  put_l2(L.l3nu * kLog2e, o + ML_L3NU);
   split2(L.wcm1 * kLog2e, o[ML_CH], o[ML_CL]);
   const double lsw5 = oco_log(L.sw5) * kLog2e;
   const double fl = floor(lsw5);
@@ -245,19 +249,50 @@ MX_HD void lambda_record(const LamIn &L, float *o) {
   o[ML_LSF] = (float)(lsw5 - fl);
 }
 
-/* Wavelength constants held in registers by the solve. */
+/* Wavelength constants held in registers by the solve; *i members are the integer parts of
+ * the large logarithms (value = member + member_i). */
 struct Lam32 {
-  float cl2, law, g[6], ls, f1, f2, f3, lal0w, gff, chi1, lnnu9, hnuk, l3nu;
+  float cl2, law, lawi, g[6], ls, lsi_, fc, fci, f2, f3, lal0w, lal0wi, gff, chi1, lnnu9, hnuk, l3nu, l3nui;
   float ch, cl;   /* log2(e)/lambda_cm = ch + cl */
-  float lsi, lsf; /* log2(2 h c^2 lambda_cm^-5) = lsi + lsf */
+  float lsi, lsf; /* log2(2 h c^2 lambda_cm^-5) = lsi + lsf, lsi an integer */
   int n0;
 };
+/* Lam32 from a record laid out as MixedL (field f at t[f * stride]). */
+template <class Get>
+MX_HD void lam32_from(Lam32 &L, Get t) {
+  L.cl2 = t(ML_CL2);
+  L.law = t(ML_LAW);
+  L.lawi = t(ML_LAW + 1);
+  for (int q = 0; q < 6; q++) L.g[q] = t(ML_G1 + q);
+  L.n0 = (int)t(ML_N0);
+  L.ls = t(ML_LS);
+  L.lsi_ = t(ML_LS + 1);
+  L.fc = t(ML_FC);
+  L.fci = t(ML_FC + 1);
+  L.f2 = t(ML_F2);
+  L.f3 = t(ML_F3);
+  L.lal0w = t(ML_LAL0W);
+  L.lal0wi = t(ML_LAL0W + 1);
+  L.gff = t(ML_GFF);
+  L.chi1 = t(ML_CHI1);
+  L.lnnu9 = t(ML_LNNU9);
+  L.hnuk = t(ML_HNUK);
+  L.l3nu = t(ML_L3NU);
+  L.l3nui = t(ML_L3NU + 1);
+  L.ch = t(ML_CH);
+  L.cl = t(ML_CL);
+  L.lsi = t(ML_LSI);
+  L.lsf = t(ML_LSF);
+}
 
-/* Opacity, absorption fraction and source function of one (z, lambda) in log2 form;
- * log2 S = lSi + lSf with lSi an integer. */
+/* Opacity, absorption fraction and source function of one (z, lambda):
+ * log2 kappa = lki + lkf (lki an integer), omw = 1 - omega (linear, in [2^-126, 1]) and
+ * log2(S (1 - omega) / mant(omw)) = lSi + lSf (lSi an integer): the right-hand side takes the
+ * binary exponent of 1 - omega in its exact integer part and the mantissa as a factor in
+ * [1, 2), so that it never underflows. */
 struct Opac32 {
-  float lk;
-  float l1mw;
+  float lki, lkf;
+  float omw;
   float lSi, lSf;
 };
 
@@ -265,17 +300,47 @@ struct Opac32 {
 constexpr float kT2Clamp = (float)(308.0 * kLog2e);
 constexpr float kT2ClampLo = (float)(308.0 * kLog2e - (double)kT2Clamp);
 
+/* w = pow2_mant(w) * 2^pow2_expo(w) with the mantissa in [1, 2), for a normal w > 0; the
+ * exponent is returned as an integer-valued float (bit operations and one exact FADD). */
+MX_HD float pow2_mant(float w) {
+#ifdef __CUDA_ARCH__
+  return __int_as_float((__float_as_int(w) & 0x007fffff) | 0x3f800000);
+#else
+  uint32_t b;
+  memcpy(&b, &w, 4);
+  b = (b & 0x007fffffu) | 0x3f800000u;
+  float r;
+  memcpy(&r, &b, 4);
+  return r;
+#endif
+}
+MX_HD float pow2_expo(float w) {
+#ifdef __CUDA_ARCH__
+  return __int_as_float(0x4b000000 | ((__float_as_int(w) >> 23) & 0xff)) - 8388735.0f; /* 2^23 + 127 */
+#else
+  uint32_t b;
+  memcpy(&b, &w, 4);
+  b = 0x4b000000u | ((b >> 23) & 0xffu);
+  float r;
+  memcpy(&r, &b, 4);
+  return r - 8388735.0f;
+#endif
+}
+
+/* log2(1/mp) and log2(369234910.67735046) (bremsstrahlung constant) as integer + fraction */
+constexpr float kLog2mp1I = 79.0f, kLog2mp1F = -0.0158371009f;
+constexpr float kBremsI = 28.0f, kBremsF = 0.459963723f;
+
 template <class Rec>
 MX_HD Opac32 opacity(const Rec &Z, const Lam32 &L) {
-  const float log2mp1 = 78.9841629f; /* log2(1/mp) */
   /* stim = 1 - 10^(-chi theta) (c_o :171) */
   const float t10 = L.cl2 * Z[MZ_TH];
   const float ls = (t10 > 40.0f) ? 0.0f : log2_one_minus_exp2neg(t10);
-  /* H bound-free (c_o :233-244): log2(AHbf wa^3) + ls + log2 ionf + log2(unsold + sm) */
-  float lsum = kNeg, sm = 0.0f;
+  /* H bound-free (c_o :233-244): AHbf wa^3 stim ionf (Unsold + E_n0 sm) */
+  float ai = Z[MZ_PU + 1], af = Z[MZ_PU];
   const int n0 = L.n0;
   if (n0 <= 6) {
-    sm = L.g[0];
+    float sm = L.g[0];
 #pragma unroll
     for (int n = 2; n <= 6; n++) sm = (n == n0) ? L.g[n - 1] : sm; /* L.g[n0-1] without local memory */
     int q = 0;
@@ -287,54 +352,70 @@ MX_HD Opac32 opacity(const Rec &Z, const Lam32 &L) {
         q++;
       }
     }
-    lsum = (n0 >= 2) ? Z[MZ_LE2 + n0 - 2] : 0.0f; /* log2 E_n0; the sum is E_n0 * sm */
+    const int pe = MZ_PE + 2 * (n0 - 1);
+    const float ef = Z[pe], ei = Z[pe + 1];
+    /* log2(Unsold) - log2(E_n0), both times ionf; the larger one sets the scale */
+    const float d = (ai - ei) + (af - ef);
+    if (d >= 0.0f) {
+      af = af + lg2(1.0f + ex2(-d) * sm);
+    } else {
+      ai = ei;
+      af = ef + lg2(ex2(d) + sm);
+    }
   }
-  /* log2(Unsold + E_n0 sm) relative to the larger of the two scales (one SFU pair) */
-  const float LU = Z[MZ_LU];
-  const float lbf = (LU >= lsum) ? LU + lg2(1.0f + ex2(lsum - LU) * sm) : lsum + lg2(ex2(LU - lsum) + sm);
-  const float A = ((L.law + ls) + Z[MZ_LIONF]) + lbf;
+  const float Ai = ai + L.lawi, Af = (L.law + ls) + af;
   /* H- bound-free (c_o :318-322) */
-  const float B = (ls + Z[MZ_LHM]) + L.ls;
-  /* H- free-free (c_o :337-339) */
-  const float C = Z[MZ_LAFF] + ((((L.f1 + L.f2 * Z[MZ_LGT]) + L.f3 * Z[MZ_LGT2]) - 26.0f) * kLog2_10_f);
-  const float D = Z[MZ_LESC];
-  const float m = fmaxf_(fmaxf_(A, B), fmaxf_(C, D));
-  const float eA = ex2(A - m), eB = ex2(B - m), eC = ex2(C - m), eD = ex2(D - m);
-  const float S4 = (eA + eB) + (eC + eD); /* sum per H / 2^m, in [1, 4] */
+  const float Bi = Z[MZ_LHM + 1] + L.lsi_, Bf = (ls + Z[MZ_LHM]) + L.ls;
+  /* H- free-free (c_o :337-339): log2(ionf ne k T) + (f1 + f2 lgt + f3 lgt^2 - 26) log2(10) */
+  const float Ci = Z[MZ_LAFF + 1] + L.fci, Cf = (Z[MZ_LAFF] + L.fc) + (L.f2 * Z[MZ_LGT] + L.f3 * Z[MZ_LGT2]);
+  const float Di = Z[MZ_LESC + 1], Df = Z[MZ_LESC];
+  /* scale 2^mi, mi the largest integer part: each 2^(term - mi) = ex2((int diff, exact) + frac) */
+  const float mi = fmaxf_(fmaxf_(Ai, Bi), fmaxf_(Ci, Di));
+  const float eA = ex2((Ai - mi) + Af), eB = ex2((Bi - mi) + Bf), eC = ex2((Ci - mi) + Cf), eD = ex2((Di - mi) + Df);
+  const float S4 = (eA + eB) + (eC + eD); /* sum per H / 2^mi */
   const float S3 = (eA + eB) + eC;        /* absorption part (no Thomson) */
-  const float X = m + log2mp1;            /* per-mass scale of S4 and S3 */
-  /* Every output is one lg2 of a linear combination scaled to M = max(X, extra term); of the
-   * two scale factors one is exactly 1. */
+  /* per-mass scale of S4 and S3: 2^(Xi + Xf) */
+  const float Xi = mi + kLog2mp1I, Xf = kLog2mp1F;
+  /* kappa and kappa_rad are one lg2 each of a linear combination scaled to M = max(X, extra
+   * term); of the two scale factors one is exactly 1.  1 - omega = kappa_abs / kappa_rad. */
   Opac32 o;
-  float lkr, labs;
+  float Mi, Mf, es, ex, num, den, lin;
   if (Z[MZ_NEUTRAL] != 0.0f) { /* c_o :262-268: kappa = rho (2 kr0 + kHff/mp), kappa_rad = kr0 + kHff/mp */
     const float gff = 1.0f + L.gff * (Z[MZ_TH1L] * L.chi1 + 0.5f);
-    const float Hf = ((ls + Z[MZ_LIONFEF]) + L.lal0w) + lg2(gff); /* log2(kHff * mp1) */
-    const bool xs = X >= Hf;
-    const float M = xs ? X : Hf;
-    const float e = ex2(-fabsf(X - Hf));
-    const float es = xs ? 1.0f : e, eh = xs ? e : 1.0f;
-    o.lk = Z[MZ_LRHO] + (M + lg2(2.0f * S4 * es + eh));
-    lkr = M + lg2(S4 * es + eh);
-    labs = M + lg2(S3 * es + eh);
+    const float Hi = Z[MZ_LIONFEF + 1] + L.lal0wi, Hf = ((ls + Z[MZ_LIONFEF]) + L.lal0w) + lg2(gff); /* kHff mp1 */
+    const float dx = (Xi - Hi) + (Xf - Hf);
+    const bool xs = dx >= 0.0f;
+    const float e = ex2(-fabsf(dx));
+    es = xs ? 1.0f : e;
+    ex = xs ? e : 1.0f;
+    Mi = xs ? Xi : Hi;
+    Mf = xs ? Xf : Hf;
+    lin = 2.0f * S4 * es + ex;
+    num = S3 * es + ex;
+    den = S4 * es + ex;
   } else { /* c_o :270-275, bremsstrahlung :281-300: kappa = rho kr0 + kb, kappa_rad = 2 kr0 + kb/rho */
     const float y = 5.960f - 0.551328895f * (L.lnnu9 + Z[MZ_LNTPOW]); /* sqrt(3)/pi */
     const float gaunt = kLn2_f * lg2(ex2(y * kLog2e_f) + 2.71828183f);
     const float xh = L.hnuk * Z[MZ_T1];
-    const float lnq = (Z[MZ_LZ] - L.l3nu) + ((xh > 30.0f) ? 0.0f : kLn2_f * log2_one_minus_exp2neg(xh * kLog2e_f));
-    const float lkb = 28.4599637f + lnq * kLog2e_f + lg2(gaunt); /* log2(369234910.67735046) */
-    const float K = lkb - Z[MZ_LRHO];                           /* log2(kb / rho) */
-    const bool xs = X >= K;
-    const float M = xs ? X : K;
-    const float e = ex2(-fabsf(X - K));
-    const float es = xs ? 1.0f : e, ek = xs ? e : 1.0f;
-    o.lk = Z[MZ_LRHO] + (M + lg2(S4 * es + ek));
-    lkr = M + lg2(2.0f * S4 * es + ek);
-    labs = M + lg2((2.0f * S3 + eD) * es + ek);
+    const float lq = (xh > 30.0f) ? 0.0f : log2_one_minus_exp2neg(xh * kLog2e_f); /* log2(1 - e^-xh) */
+    /* log2(kb / rho) = log2(369234910.67735046 ne n T^-1/2 nu^-3 (1 - e^-xh) gaunt / rho) */
+    const float Ki = ((Z[MZ_LZ2 + 1] - L.l3nui) - Z[MZ_LRHO + 1]) + kBremsI;
+    const float Kf = ((Z[MZ_LZ2] - L.l3nu) - Z[MZ_LRHO]) + ((lq + lg2(gaunt)) + kBremsF);
+    const float dx = (Xi - Ki) + (Xf - Kf);
+    const bool xs = dx >= 0.0f;
+    const float e = ex2(-fabsf(dx));
+    es = xs ? 1.0f : e;
+    ex = xs ? e : 1.0f;
+    Mi = xs ? Xi : Ki;
+    Mf = xs ? Xf : Kf;
+    lin = S4 * es + ex;
+    num = (2.0f * S3 + eD) * es + ex;
+    den = 2.0f * S4 * es + ex;
   }
-  float l1 = labs - lkr;
-  if (l1 > 0.0f) l1 = 0.0f;
-  o.l1mw = fmaxf_(l1, -126.0f);
+  o.lki = Z[MZ_LRHO + 1] + Mi;
+  o.lkf = (Z[MZ_LRHO] + Mf) + lg2(lin);
+  const float w = num * rcp(den);
+  o.omw = w > 1.0f ? 1.0f : (w < 1.17549435e-38f ? 1.17549435e-38f : w); /* [2^-126, 1] */
   /* Planck function (c_o :399-407): S = sw5 / (e^x - 1), x = dft1/lambda_cm clamped at 308.
    * t2 = x log2(e) = (dft1_hi + dft1_lo)(ch + cl) as hi + lo (FMA two-product). */
   const float dh = Z[MZ_DFT1], dl = Z[MZ_DFT1L];
@@ -347,7 +428,7 @@ MX_HD Opac32 opacity(const Rec &Z, const Lam32 &L) {
   const float ti = floorf(p);
   const float tf = (p - ti) + lo; /* t2 = ti + tf */
   const float lm = (p > 40.0f) ? 0.0f : log2_one_minus_exp2neg(p);
-  o.lSi = L.lsi - ti;
+  o.lSi = (L.lsi - ti) + pow2_expo(o.omw);
   o.lSf = (L.lsf - tf) - lm;
   return o;
 }
@@ -418,41 +499,55 @@ MX_HD double xtod(XF x) {
 /* ---- scaled tridiagonal rows (auxiliary.f90:125-201 divided by kappa_i^2) ------------- */
 struct Row32 {
   float a, c, e;  /* sub, super, diagonal excess -(a+b+c) */
-  float ldi, ldf; /* log2 of -d (right-hand side) = ldi + ldf, ldi an integer */
+  float ldi, ldf; /* -d (right-hand side) = w * 2^(ldi + ldf), ldi an integer */
+  float w;        /* mantissa of 1 - omega, in [1, 2) */
 };
-/* 2^L for log2 values clamped to the FP32 normal range, split exactly into 2^int * ex2(frac) */
-MX_HD float exp2_split(float L) {
-  L = L < -126.0f ? -126.0f : (L > 127.0f ? 127.0f : L);
-  const float fl = floorf(L);
-  return ex2(L - fl) * pow2f((int)fl);
+/* 2^(i + f) for an integer-valued i and a small f, the exponent clamped to the FP32 normal
+ * range [-126, 127] */
+MX_HD float exp2_split(float i, float f) {
+  const float fl = floorf(f);
+  const float L = i + fl;
+  if (L < -126.0f) return pow2f(-126);
+  if (L >= 127.0f) return pow2f(127);
+  return ex2(f - fl) * pow2f((int)L);
 }
-MX_HD float kappa_lin(float lk) { return exp2_split(lk); }
-/* log2 d = le + log2 S with le split exactly as floor + fraction */
-MX_HD void row_rhs(Row32 &r, float le, const Opac32 &o) {
-  const float fi = floorf(le);
-  r.ldi = fi + o.lSi;
-  r.ldf = (le - fi) + o.lSf;
+MX_HD float kappa_lin(const Opac32 &o) { return exp2_split(o.lki, o.lkf); }
+/* the right-hand side S e' as w 2^(ldi + ldf): le + log2 S with le split as i + f, and the
+ * mantissa w of 1 - omega (its exponent is in o.lSi) */
+MX_HD void row_rhs(Row32 &r, float lei, float lef, const Opac32 &o) {
+  const float fi = floorf(lef);
+  r.ldi = (lei + fi) + o.lSi;
+  r.ldf = (lef - fi) + o.lSf;
+  r.w = pow2_mant(o.omw);
 }
-/* centre row: a' = 1/kappa_{i-1/2}, c' = 1/kappa_{i+1/2}, e' = dz^2 kappa (1-omega), d' = -S e' */
-MX_HD Row32 row_center(float km, float kj, float kp, const Opac32 &o, float ldz2) {
+/* centre row: a' = 1/kappa_{i-1/2}, c' = 1/kappa_{i+1/2}, e' = dz^2 kappa (1-omega), d' = -S e';
+ * log2(dz^2) = ldz2i + ldz2f */
+MX_HD Row32 row_center(float km, float kj, float kp, const Opac32 &o, float ldz2i, float ldz2f) {
   Row32 r;
   r.a = 2.0f * rcp(kj + km);
   r.c = 2.0f * rcp(kp + kj);
-  const float le = (ldz2 + o.lk) + o.l1mw;
-  r.e = exp2_split(le);
-  row_rhs(r, le, o);
+  const float lei = ldz2i + o.lki, lef = ldz2f + o.lkf;
+  r.e = exp2_split(lei, lef) * o.omw;
+  row_rhs(r, lei, lef, o);
   return r;
 }
 /* boundary rows: zeta = kappa dz^2 (1-omega)/4; excess dz + zeta; d' = -S zeta;
  * bottom: a' = 0, c' = 1/kappa; top: a' = 1/kappa, c' = 0 */
-MX_HD Row32 row_boundary(float kj, const Opac32 &o, float dz, float ldz2, bool top) {
+MX_HD Row32 row_boundary(float kj, const Opac32 &o, float dz, float ldz2i, float ldz2f, bool top) {
   Row32 r;
-  const float lz = ((ldz2 + o.lk) + o.l1mw) - 2.0f;
+  const float lei = (ldz2i + o.lki) - 2.0f, lef = ldz2f + o.lkf;
   r.a = top ? rcp(kj) : 0.0f;
   r.c = top ? 0.0f : rcp(kj);
-  r.e = dz + exp2_split(lz);
-  row_rhs(r, lz, o);
+  r.e = dz + exp2_split(lei, lef) * o.omw;
+  row_rhs(r, lei, lef, o);
   return r;
+}
+/* log2(dz^2) as integer + fraction */
+MX_HD void ldz2_split(double dz, float &i, float &f) {
+  const double v = 2.0 * oco_log(dz) * kLog2e;
+  const double n = floor(v + 0.5);
+  i = (float)n;
+  f = (float)(v - n);
 }
 
 /* 6th-order flux at interior index m (auxiliary.f90:64-109) from the differences
@@ -471,15 +566,17 @@ MX_HD double flux_from_diffs(const double *Dl, int m, double o1, double dz1) {
 template <class ZAt>
 MX_HD void solve_item_host(ZAt Zat, const Lam32 &L, int nz, double dz, float *work, double *dwork, double *U,
                            double *K, double *V) {
-  const float dzf = (float)dz, ldz2 = (float)(2.0 * oco_log(dz) * kLog2e);
+  const float dzf = (float)dz;
+  float ldz2i, ldz2f;
+  ldz2_split(dz, ldz2i, ldz2f);
   float *g = work, *um = work + nz, *o1 = work + 2 * nz, *kap = work + 3 * nz, *qv = work + 5 * nz;
   int *ue = (int *)(work + 4 * nz);
   Opac32 cur = opacity(Zat(0), L), nxt = opacity(Zat(1), L);
-  float kc = kappa_lin(cur.lk), kn = kappa_lin(nxt.lk), kprev = 0.0f;
-  Row32 r = row_boundary(kc, cur, dzf, ldz2, false);
+  float kc = kappa_lin(cur), kn = kappa_lin(nxt), kprev = 0.0f;
+  Row32 r = row_boundary(kc, cur, dzf, ldz2i, ldz2f, false);
   float h = r.e, cprev = r.c;
   XF u = xexp2(r.ldi, r.ldf);
-  u.m *= rcp(r.c + h);
+  u.m *= r.w * rcp(r.c + h);
   u = xnorm(u.m, u.e);
   um[0] = u.m;
   ue[0] = u.e;
@@ -491,17 +588,17 @@ MX_HD void solve_item_host(ZAt Zat, const Lam32 &L, int nz, double dz, float *wo
     kc = kn;
     if (j < nz - 1) {
       nxt = opacity(Zat(j + 1), L);
-      kn = kappa_lin(nxt.lk);
-      r = row_center(kprev, kc, kn, cur, ldz2);
+      kn = kappa_lin(nxt);
+      r = row_center(kprev, kc, kn, cur, ldz2i, ldz2f);
     } else {
-      r = row_boundary(kc, cur, dzf, ldz2, true);
+      r = row_boundary(kc, cur, dzf, ldz2i, ldz2f, true);
     }
     const float rr = rcp(cprev + h);
     g[j] = cprev * rr;  /* |gamma_j| = c_{j-1}/(c_{j-1}+h_{j-1}) */
     qv[j - 1] = h * rr; /* q_{j-1} = h_{j-1}/(c_{j-1}+h_{j-1}) */
     h = r.e + (r.a * rr) * h; /* a'/(c'+h) is O(1); a' h alone can overflow */
     const float rb = rcp(r.c + h); /* 1/|bet_j| */
-    u = xaxpy(xexp2(r.ldi, r.ldf), rb, u, r.a * rb); /* u_j = (|d_j| + a_j u_{j-1}) / |bet_j| */
+    u = xaxpy(xexp2(r.ldi, r.ldf), r.w * rb, u, r.a * rb); /* u_j = (|d_j| + a_j u_{j-1}) / |bet_j| */
     um[j] = u.m;
     ue[j] = u.e;
     o1[j] = rcp(kc);

@@ -194,6 +194,8 @@ void oco::fill_lambda_table(const double *waves, int nw, double *tab) {
   }
 }
 
+static_assert(mx::MLN == MIXED_LN && mx::MZN == MIXED_ZN, "mixed record sizes");
+
 void oco::fill_mixed_lambda_table(const double *tab, int nw, float *tab32) {
   for (int iw = 0; iw < nw; iw++) {
     auto T = [&](int f) { return tab[(size_t)f * nw + iw]; };
@@ -331,7 +333,7 @@ static int run_chunk_mixed(oco_ctx *c, const oco_params *p, const double *rho, c
   a.nz = p->nz;
   a.nw = p->nw;
   a.dz = p->dz;
-  a.ldz2 = (float)(2.0 * std::log2(p->dz));
+  mx::ldz2_split(p->dz, a.ldz2i, a.ldz2f);
   a.U = a64.U, a.U_zs = a64.U_zs, a.U_is = a64.U_is;
   a.K = a64.K, a.K_zs = a64.K_zs, a.K_is = a64.K_is;
   a.V = a64.V, a.V_zs = a64.V_zs, a.V_is = a64.V_is;

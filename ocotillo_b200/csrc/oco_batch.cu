@@ -189,7 +189,7 @@ extern "C" int oco_batch_create(oco_ctx *c, const oco_batch_column *cols, int64_
     d.nz = q.nz;
     d.nw = q.nw;
     d.dzf = (float)q.dz;
-    d.ldz2 = (float)(2.0 * std::log2(q.dz));
+    mx::ldz2_split(q.dz, d.ldz2i, d.ldz2f);
     d.dz1 = 1.0 / q.dz;
     rpre[(size_t)i + 1] = rpre[(size_t)i] + q.nz;
     b->npoints += (int64_t)q.nz * q.nw;

@@ -102,7 +102,7 @@ struct MixedArgs {
   int64_t ncol;
   int nz, nw;
   double dz;
-  float ldz2; /* log2(dz^2) */
+  float ldz2i, ldz2f; /* log2(dz^2) = integer + fraction */
   double *U;
   int64_t U_zs, U_is;
   double *K;
@@ -127,7 +127,8 @@ struct MBatchCol {
   int64_t flux_off; /* first emergent-flux element */
   int64_t lam_off;  /* first float of the column's [MIXED_LN][nw] wavelength table */
   int32_t nz, nw;
-  float dzf, ldz2;  /* dz and log2(dz^2) */
+  float dzf;        /* dz */
+  float ldz2i, ldz2f; /* log2(dz^2) = integer + fraction */
   double dz1;       /* 1/dz */
 };
 
@@ -192,8 +193,8 @@ int solve_fp64_max_blocks_per_sm(int form, int grey, int threads);
 cudaError_t launch_bounded_wait_check(long long limit, unsigned long long *status, cudaStream_t s);
 
 /* Mixed-precision kernels (kernels_mixed.cu). */
-constexpr int MIXED_ZN = 40; /* floats per mixed record */
-constexpr int MIXED_LN = 24; /* fields of the mixed wavelength table */
+constexpr int MIXED_ZN = 52; /* floats per mixed record */
+constexpr int MIXED_LN = 28; /* fields of the mixed wavelength table */
 cudaError_t launch_pillars_mixed(const double *rho, const double *T, int64_t ncol, int nz, double fully_ionized_T,
                                  float *rec, cudaStream_t s);
 cudaError_t launch_solve_mixed(const MixedArgs &a, int blocks, int threads, cudaStream_t s);
