@@ -174,10 +174,10 @@ __device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa
   u = xnorm(u.m * (r.w * rcp(r.c + h)), u.e);
   float o1 = rcp(kc);
   if (Kb) Kb[0] = (double)kc;
-  /* scratch record of z = j: {v_j, 1/kappa_j, u_j mantissa, u_j exponent} where v_j holds the
+  /* scratch record of z = j: {v_j, 1/kappa_j, u_j mantissa, u_j exponent (int bits)} where v_j holds the
    * smaller of q_j = h_j/(c_j+h_j) and |gamma_{j+1}| = c_j/(c_j+h_j) (they sum to 1; a negative
    * v_j stores -|gamma_{j+1}|), written once row j+1 is known */
-  float4 pend = make_float4(0.0f, o1, u.m, (float)u.e);
+  float4 pend = make_float4(0.0f, o1, u.m, __int_as_float(u.e));
   for (int j = 1; j < nz; j++) {
     kprev = kc;
     cur = nxt;
@@ -198,7 +198,7 @@ __device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa
     u = xaxpy(xexp2(r.ldi, r.ldf), r.w * rb, u, r.a * rb);
     o1 = rcp(kc);
     if (Kb) Kb[(int64_t)j * it.kz] = (double)kc;
-    pend = make_float4(0.0f, o1, u.m, (float)u.e);
+    pend = make_float4(0.0f, o1, u.m, __int_as_float(u.e));
     cprev = r.c;
   }
   s4[(int64_t)(nz - 1) * ss] = pend;
@@ -228,9 +228,9 @@ __device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa
       const float qk = (w.x >= 0.0f) ? w.x : 1.0f + w.x;
       XF uj;
       uj.m = w.z;
-      uj.e = (int)w.w;
-      XF Dj = xaxpy(uj, 1.0f, Un, -qk);
-      Un = xaxpy(uj, 1.0f, Un, g1);
+      uj.e = __float_as_int(w.w);
+      XF Dj;
+      xaxpy2(uj, Un, g1, -qk, Un, Dj);
       Uk[t] = xtod(Un);
       if (Ub) Ub[(int64_t)(3 + k) * uz] = Uk[t];
       Dt[t] = xtod(Dj);
@@ -263,9 +263,9 @@ __device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa
       const float qk = (w.x >= 0.0f) ? w.x : 1.0f + w.x;  /* q_k */
       XF uj;
       uj.m = w.z;
-      uj.e = (int)w.w;
-      XF Dj = xaxpy(uj, 1.0f, Un, -qk);
-      Un = xaxpy(uj, 1.0f, Un, g1);
+      uj.e = __float_as_int(w.w);
+      XF Dj;
+      xaxpy2(uj, Un, g1, -qk, Un, Dj);
       const double Uv = xtod(Un);
       if (Ub) Ub[(int64_t)(3 + k) * uz] = Uv;
       U3 = U2; U2 = U1; U1 = U0; U0 = Uv;
@@ -305,8 +305,9 @@ __device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa
       const float g1 = (w.x >= 0.0f) ? 1.0f - w.x : -w.x;
       XF uj;
       uj.m = w.z;
-      uj.e = (int)w.w;
-      Un = xaxpy(uj, 1.0f, Un, g1);
+      uj.e = __float_as_int(w.w);
+      XF Dj;
+      xaxpy2(uj, Un, g1, 0.0f, Un, Dj);
       f[n1 + j] = xtod(Un);
     }
     for (int i = 1; i <= 3; i++) {

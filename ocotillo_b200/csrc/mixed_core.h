@@ -433,48 +433,39 @@ MX_HD Opac32 opacity(const Rec &Z, const Lam32 &L) {
   return o;
 }
 
-/* ---- extended-exponent non-negative numbers: value = m * 2^e, m FP32, e int -------------- */
+/* ---- extended-exponent numbers: value = m * 2^e, m FP32, e int ------------------------ */
 struct XF {
   float m;
   int e;
 };
-/* 2^k as a float for -126 <= k <= 127; 0 below. */
-MX_HD float pow2f(int k) {
-  if (k < -126) return 0.0f;
+MX_HD int f2bits(float f) {
 #ifdef __CUDA_ARCH__
-  return __int_as_float((k + 127) << 23);
+  return __float_as_int(f);
 #else
-  union {
-    int i;
-    float f;
-  } u;
-  u.i = (k + 127) << 23;
-  return u.f;
+  int i;
+  memcpy(&i, &f, 4);
+  return i;
 #endif
 }
-MX_HD int float_exponent(float m) {
+MX_HD float bits2f(int i) {
 #ifdef __CUDA_ARCH__
-  return ((__float_as_int(m) >> 23) & 0xff) - 127;
+  return __int_as_float(i);
 #else
-  union {
-    int i;
-    float f;
-  } u;
-  u.f = m;
-  return ((u.i >> 23) & 0xff) - 127;
+  float f;
+  memcpy(&f, &i, 4);
+  return f;
 #endif
 }
-/* renormalise so that m is in [1, 2) (m = 0 keeps e) */
+/* 2^k as a float for -126 <= k <= 127; +0 below (k = -127 is the zero bit pattern). */
+MX_HD float pow2f(int k) { return bits2f(((k < -127 ? -127 : k) + 127) << 23); }
+/* renormalise so that |m| is in [1, 2) with bit operations: the exponent field moves into e.
+ * A zero or subnormal m (exponent field 0) is kept as it is, value-exact. */
 MX_HD XF xnorm(float m, int e) {
+  const int b = f2bits(m);
+  const int ef = (b >> 23) & 0xff;
   XF r;
-  if (m == 0.0f) {
-    r.m = 0.0f;
-    r.e = e;
-    return r;
-  }
-  const int k = float_exponent(m);
-  r.m = m * pow2f(-k);
-  r.e = e + k;
+  r.m = ef ? bits2f((b & (int)0x807fffff) | 0x3f800000) : m;
+  r.e = ef ? e + (ef - 127) : e;
   return r;
 }
 /* 2^(I + F) for an integer-valued float I and a small float F */
@@ -485,11 +476,24 @@ MX_HD XF xexp2(float I, float F) {
   r.m = ex2(F - fl);
   return r;
 }
-/* x*s + y*t for non-negative x, y and FP32 factors s, t >= 0 */
+/* x*s + y*t for FP32 factors s, t: the operand with the smaller exponent is scaled by 2^-|de|
+ * (the other by exactly 1) and added with one FMA. */
 MX_HD XF xaxpy(XF x, float s, XF y, float t) {
-  const int e = x.e > y.e ? x.e : y.e;
-  const float m = x.m * s * pow2f(x.e - e) + y.m * t * pow2f(y.e - e);
-  return xnorm(m, e);
+  const int d = x.e - y.e;
+  const bool ge = d >= 0;
+  const float a = x.m * s, b = y.m * t;
+  const float big = ge ? a : b, small = ge ? b : a;
+  return xnorm(fmaf(small, pow2f(ge ? -d : d), big), ge ? x.e : y.e);
+}
+/* The two back-substitution updates of one step, x + y*t1 and x + y*t2, sharing the alignment. */
+MX_HD void xaxpy2(XF x, XF y, float t1, float t2, XF &r1, XF &r2) {
+  const int d = x.e - y.e;
+  const bool ge = d >= 0;
+  const float p = pow2f(ge ? -d : d);
+  const float b1 = y.m * t1, b2 = y.m * t2;
+  const int e = ge ? x.e : y.e;
+  r1 = xnorm(ge ? fmaf(b1, p, x.m) : fmaf(x.m, p, b1), e);
+  r2 = xnorm(ge ? fmaf(b2, p, x.m) : fmaf(x.m, p, b2), e);
 }
 MX_HD double xtod(XF x) {
   if (x.m == 0.0f || x.e < -1000) return 0.0;
@@ -615,8 +619,8 @@ MX_HD void solve_item_host(ZAt Zat, const Lam32 &L, int nz, double dz, float *wo
     XF uj;
     uj.m = um[j];
     uj.e = ue[j];
-    XF Dj = xaxpy(uj, 1.0f, Un, -qv[j]);
-    Un = xaxpy(uj, 1.0f, Un, g[j + 1]);
+    XF Dj;
+    xaxpy2(uj, Un, g[j + 1], -qv[j], Un, Dj);
     U[n1 + j] = xtod(Un);
     Dl[n1 + j] = xtod(Dj);
   }

@@ -112,7 +112,7 @@ struct MixedArgs {
   double *Vtop, *Vbot;
   int64_t ld_col, c_off;
   int layout;
-  float4 *s4; /* scratch [nz][slots]: |gamma| or q, 1/kappa, u mantissa, u exponent */
+  float4 *s4; /* scratch [nz][slots]: |gamma| or q, 1/kappa, u mantissa, u exponent (int bits) */
   int64_t slot_stride;
   unsigned long long *work;
   unsigned long long *status;
