@@ -120,6 +120,7 @@ struct MItem {
   int nz, nw, iw;
   float dzf;        /* dz */
   float ldz2i, ldz2f; /* log2(dz^2) = integer + fraction */
+  float dz2f;       /* dz^2 */
   double dz1;       /* 1/dz */
   double *U;        /* U of z = 0 (ghost zone 0), stride uz, or NULL; written only when active */
   double *K, *V;    /* kappa and V of z = 0 or NULL, strides kz, vz */
@@ -137,6 +138,7 @@ __device__ __forceinline__ MItem block_item(const MixedArgs &a, int64_t cl, int 
   it.dzf = (float)a.dz;
   it.ldz2i = a.ldz2i;
   it.ldz2f = a.ldz2f;
+  it.dz2f = (float)(a.dz * a.dz);
   it.dz1 = 1.0 / a.dz;
   const int64_t idx = (a.layout == 0) ? (int64_t)iw * a.ld_col + a.c_off + cl : (a.c_off + cl) * a.nw + iw;
   it.U = a.U ? a.U + idx * a.U_is : nullptr;
@@ -163,13 +165,14 @@ __device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa
   double *Ub = active ? it.U : nullptr;
   double *Kb = active ? it.K : nullptr;
   double *Vb = active ? it.V : nullptr;
-  const float dzf = it.dzf, ldz2i = it.ldz2i, ldz2f = it.ldz2f;
+  const float dzf = it.dzf, dz2f = it.dz2f, ldz2i = it.ldz2i, ldz2f = it.ldz2f;
 
   Opac32 cur = opacity(pa.at(0), L);
   Opac32 nxt = opacity(pa.at(1), L);
-  float kc = kappa_lin(cur), kn = kappa_lin(nxt), kprev = 0.0f;
-  Row32 r = row_boundary(kc, cur, dzf, ldz2i, ldz2f, false);
+  float kc = kappa_lin(cur), kn = kappa_lin(nxt);
+  Row32 r = row_boundary(kc, cur, dzf, dz2f, ldz2i, ldz2f, false);
   float h = r.e, cprev = r.c;
+  float an = 2.0f * rcp(kn + kc); /* a' of row 1; then c' of the row below */
   XF u = xexp2(r.ldi, r.ldf);
   u = xnorm(u.m * (r.w * rcp(r.c + h)), u.e);
   float o1 = rcp(kc);
@@ -179,15 +182,15 @@ __device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa
    * v_j stores -|gamma_{j+1}|), written once row j+1 is known */
   float4 pend = make_float4(0.0f, o1, u.m, __int_as_float(u.e));
   for (int j = 1; j < nz; j++) {
-    kprev = kc;
     cur = nxt;
     kc = kn;
     if (j < nz - 1) {
       nxt = opacity(pa.at(j + 1), L);
       kn = kappa_lin(nxt);
-      r = row_center(kprev, kc, kn, cur, ldz2i, ldz2f);
+      r = row_center(an, kc, kn, cur, dz2f, ldz2i, ldz2f);
+      an = r.c;
     } else {
-      r = row_boundary(kc, cur, dzf, ldz2i, ldz2f, true);
+      r = row_boundary(kc, cur, dzf, dz2f, ldz2i, ldz2f, true);
     }
     const float rr = rcp(cprev + h);
     const float qv = h * rr, gv = cprev * rr;
@@ -422,6 +425,7 @@ __device__ __forceinline__ MItem batch_item(const MixedBatchArgs &b, const MBatc
   it.dzf = c.dzf;
   it.ldz2i = c.ldz2i;
   it.ldz2f = c.ldz2f;
+  it.dz2f = (float)(1.0 / (c.dz1 * c.dz1));
   it.dz1 = c.dz1;
   if (b.layout == 0) { /* per column [lambda][z] (z fastest) */
     it.U = b.U ? b.U + c.u_off + (int64_t)iw * (c.nz + 6) : nullptr;

@@ -144,11 +144,10 @@ MX_HD float fmaxf_(float a, float b) { return a > b ? a : b; }
 /* log2(1 - 2^-t) for t > 0 (accurate to a few 1e-7 relative of the result's argument
  * for t >= 2^-6; a two-term series below that). */
 MX_HD float log2_one_minus_exp2neg(float t) {
-  if (t < 0.015625f) {
-    float x = t * kLn2_f; /* 1 - e^-x = x (1 - x/2 + x^2/6) */
-    return lg2(x * (1.0f - x * (0.5f - x * (1.0f / 6.0f))));
-  }
-  return lg2(1.0f - ex2(-t));
+  const float x = t * kLn2_f; /* 1 - e^-x = x (1 - x/2 + x^2/6) below 2^-6; one ex2 and one lg2 */
+  const float series = x * (1.0f - x * (0.5f - x * (1.0f / 6.0f)));
+  const float direct = 1.0f - ex2(-t);
+  return lg2(t < 0.015625f ? series : direct);
 }
 
 MX_HD float tolog(double v) { return v > 0.0 ? (float)(oco_log(v) * kLog2e) : kNeg; }
@@ -356,12 +355,11 @@ MX_HD Opac32 opacity(const Rec &Z, const Lam32 &L) {
     const float ef = Z[pe], ei = Z[pe + 1];
     /* log2(Unsold) - log2(E_n0), both times ionf; the larger one sets the scale */
     const float d = (ai - ei) + (af - ef);
-    if (d >= 0.0f) {
-      af = af + lg2(1.0f + ex2(-d) * sm);
-    } else {
-      ai = ei;
-      af = ef + lg2(ex2(d) + sm);
-    }
+    const bool ug = d >= 0.0f;
+    const float x = ex2(-fabsf(d)); /* branch-free: one ex2 and one lg2 whichever side is larger */
+    const float arg = ug ? fmaf(x, sm, 1.0f) : x + sm;
+    af = (ug ? af : ef) + lg2(arg);
+    ai = ug ? ai : ei;
   }
   const float Ai = ai + L.lawi, Af = (L.law + ls) + af;
   /* H- bound-free (c_o :318-322) */
@@ -524,26 +522,29 @@ MX_HD void row_rhs(Row32 &r, float lei, float lef, const Opac32 &o) {
   r.ldf = (lef - fi) + o.lSf;
   r.w = pow2_mant(o.omw);
 }
-/* centre row: a' = 1/kappa_{i-1/2}, c' = 1/kappa_{i+1/2}, e' = dz^2 kappa (1-omega), d' = -S e';
- * log2(dz^2) = ldz2i + ldz2f */
-MX_HD Row32 row_center(float km, float kj, float kp, const Opac32 &o, float ldz2i, float ldz2f) {
+/* e' = dz^2 kappa (1 - omega) as a linear product (kappa dz^2 capped at FLT_MAX) */
+MX_HD float row_excess(float kj, const Opac32 &o, float dz2f) {
+  const float t = kj * dz2f;
+  return (t < 3.40282347e38f ? t : 3.40282347e38f) * o.omw;
+}
+/* centre row: a' = 1/kappa_{i-1/2} (= c' of the row below, passed in), c' = 1/kappa_{i+1/2},
+ * e' = dz^2 kappa (1-omega), d' = -S e'; log2(dz^2) = ldz2i + ldz2f */
+MX_HD Row32 row_center(float a, float kj, float kp, const Opac32 &o, float dz2f, float ldz2i, float ldz2f) {
   Row32 r;
-  r.a = 2.0f * rcp(kj + km);
+  r.a = a;
   r.c = 2.0f * rcp(kp + kj);
-  const float lei = ldz2i + o.lki, lef = ldz2f + o.lkf;
-  r.e = exp2_split(lei, lef) * o.omw;
-  row_rhs(r, lei, lef, o);
+  r.e = row_excess(kj, o, dz2f);
+  row_rhs(r, ldz2i + o.lki, ldz2f + o.lkf, o);
   return r;
 }
 /* boundary rows: zeta = kappa dz^2 (1-omega)/4; excess dz + zeta; d' = -S zeta;
  * bottom: a' = 0, c' = 1/kappa; top: a' = 1/kappa, c' = 0 */
-MX_HD Row32 row_boundary(float kj, const Opac32 &o, float dz, float ldz2i, float ldz2f, bool top) {
+MX_HD Row32 row_boundary(float kj, const Opac32 &o, float dz, float dz2f, float ldz2i, float ldz2f, bool top) {
   Row32 r;
-  const float lei = (ldz2i + o.lki) - 2.0f, lef = ldz2f + o.lkf;
   r.a = top ? rcp(kj) : 0.0f;
   r.c = top ? 0.0f : rcp(kj);
-  r.e = dz + exp2_split(lei, lef) * o.omw;
-  row_rhs(r, lei, lef, o);
+  r.e = dz + 0.25f * row_excess(kj, o, dz2f);
+  row_rhs(r, (ldz2i + o.lki) - 2.0f, ldz2f + o.lkf, o);
   return r;
 }
 /* log2(dz^2) as integer + fraction */
@@ -570,15 +571,16 @@ MX_HD double flux_from_diffs(const double *Dl, int m, double o1, double dz1) {
 template <class ZAt>
 MX_HD void solve_item_host(ZAt Zat, const Lam32 &L, int nz, double dz, float *work, double *dwork, double *U,
                            double *K, double *V) {
-  const float dzf = (float)dz;
+  const float dzf = (float)dz, dz2f = (float)(dz * dz);
   float ldz2i, ldz2f;
   ldz2_split(dz, ldz2i, ldz2f);
   float *g = work, *um = work + nz, *o1 = work + 2 * nz, *kap = work + 3 * nz, *qv = work + 5 * nz;
   int *ue = (int *)(work + 4 * nz);
   Opac32 cur = opacity(Zat(0), L), nxt = opacity(Zat(1), L);
-  float kc = kappa_lin(cur), kn = kappa_lin(nxt), kprev = 0.0f;
-  Row32 r = row_boundary(kc, cur, dzf, ldz2i, ldz2f, false);
+  float kc = kappa_lin(cur), kn = kappa_lin(nxt);
+  Row32 r = row_boundary(kc, cur, dzf, dz2f, ldz2i, ldz2f, false);
   float h = r.e, cprev = r.c;
+  float an = 2.0f * rcp(kn + kc); /* a' of row 1 */
   XF u = xexp2(r.ldi, r.ldf);
   u.m *= r.w * rcp(r.c + h);
   u = xnorm(u.m, u.e);
@@ -587,15 +589,15 @@ MX_HD void solve_item_host(ZAt Zat, const Lam32 &L, int nz, double dz, float *wo
   o1[0] = rcp(kc);
   kap[0] = kc;
   for (int j = 1; j < nz; j++) {
-    kprev = kc;
     cur = nxt;
     kc = kn;
     if (j < nz - 1) {
       nxt = opacity(Zat(j + 1), L);
       kn = kappa_lin(nxt);
-      r = row_center(kprev, kc, kn, cur, ldz2i, ldz2f);
+      r = row_center(an, kc, kn, cur, dz2f, ldz2i, ldz2f);
+      an = r.c;
     } else {
-      r = row_boundary(kc, cur, dzf, ldz2i, ldz2f, true);
+      r = row_boundary(kc, cur, dzf, dz2f, ldz2i, ldz2f, true);
     }
     const float rr = rcp(cprev + h);
     g[j] = cprev * rr;  /* |gamma_j| = c_{j-1}/(c_{j-1}+h_{j-1}) */
