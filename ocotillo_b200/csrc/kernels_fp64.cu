@@ -151,18 +151,42 @@ struct Opac {
 
 /* calc_opacity_and_albedo for one (z, lambda), continuous_opacity.f90:175-201 with
  * :171, :233-244, :318-322, :337-339, :261-277, :290-298, :399-407. */
+/* 10^y1, 10^y2 and e^x3 as oco_pow10, oco_pow10 and oco_exp compute them, with the three
+ * fast phases side by side (branch-free, so that their dependency chains overlap) and the
+ * full evaluation only where a fast phase cannot decide. */
+__device__ __forceinline__ void pow10_pow10_exp(double y1, double y2, double x3, double &r1, double &r2,
+                                                double &r3) {
+  const double p1 = OCO_M(y1, OCO_LN10_HI), p2 = OCO_M(y2, OCO_LN10_HI);
+  const double l1 = OCO_A(OCO_FMA(y1, OCO_LN10_HI, -p1), OCO_M(y1, OCO_LN10_LO));
+  const double l2 = OCO_A(OCO_FMA(y2, OCO_LN10_HI, -p2), OCO_M(y2, OCO_LN10_LO));
+  double f1, f2, f3;
+  const int ok1 = oco_exp_fast_nb(p1, l1, &f1);
+  const int ok2 = oco_exp_fast_nb(p2, l2, &f2);
+  const int ok3 = oco_exp_fast_nb(x3, 0.0, &f3);
+  if (!ok1) f1 = oco_exp_dd(p1, l1);
+  if (!ok2) f2 = oco_exp_dd(p2, l2);
+  if (!ok3) f3 = oco_exp_dd(x3, 0.0);
+  r1 = OCO_M(1.0, f1);
+  r2 = OCO_M(1.0, f2);
+  r3 = f3;
+}
+
 template <bool STABLE, class R>
 __device__ __forceinline__ Opac opacity_at(const R P, const Lam &L) {
   const double theta = P[F_THETA];
   const double ionf = P[F_IONF];
-  const double stim = 1.0 - oco_pow10(-(L.chi * theta));
+  double damping = P[F_DFT1] * L.wcm1;
+  if (damping > log_overflow_limit) damping = log_overflow_limit;
+  double p10_stim, p10_flam, e_planck;
+  pow10_pow10_exp(-(L.chi * theta), ((L.f1 + L.f2 * P[F_LGT]) + L.f3 * P[F_LGT2]) - 26.0, damping, p10_stim,
+                  p10_flam, e_planck);
+  const double stim = 1.0 - p10_stim;
   double sm = 0.0;
 #pragma unroll
   for (int q = 0; q < 6; q++) sm = sm + L.gn[q] * P[F_E1 + q];
   double kHbf = (((AHbf * stim) * ionf) * L.wa3) * (P[F_UNSOLD] + sm);
   double kHmbf = (L.hmon != 0.0) ? ((P[F_HMBF] * stim) * ionf) * L.s : 0.0;
-  double flam = ((L.f1 + L.f2 * P[F_LGT]) + L.f3 * P[F_LGT2]) - 26.0;
-  double kHmff = P[F_AFF] * oco_pow10(flam);
+  double kHmff = P[F_AFF] * p10_flam; /* 10^(f1 + f2 lgt + f3 lgt^2 - 26) */
   double kr = (((kHbf + kHmbf) + kHmff) + P[F_ESCAT]) * mp1;
   double kabs = STABLE ? ((kHbf + kHmbf) + kHmff) * mp1 : 0.0;
   const double rho = P[F_RHO];
@@ -185,9 +209,7 @@ __device__ __forceinline__ Opac opacity_at(const R P, const Lam &L) {
   o.op = op;
   o.alb = P[F_ESCM] / kr;
   o.oma = STABLE ? kabs / kr : 0.0;
-  double damping = P[F_DFT1] * L.wcm1;
-  if (damping > log_overflow_limit) damping = log_overflow_limit;
-  o.S = L.sw5 / (oco_exp(damping) - 1.0);
+  o.S = L.sw5 / (e_planck - 1.0);
   return o;
 }
 
@@ -557,7 +579,7 @@ __global__ void __launch_bounds__(128) k_solve(const SolveArgs a) {
 /* Staged path: warp tasks are (column, tile of 32 wavelengths); the column's pillar records
  * are streamed into shared memory by bulk copies (see StagedPillars). */
 template <int FORM, bool GREY>
-__global__ void __launch_bounds__(128) k_solve_staged(const SolveArgs a) {
+__global__ void __launch_bounds__(128, 4) k_solve_staged(const SolveArgs a) {
   __shared__ __align__(128) double s_pil[WARPS_PER_BLOCK][2 * ZC * NF];
   __shared__ __align__(8) unsigned long long s_bar[WARPS_PER_BLOCK][2];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;

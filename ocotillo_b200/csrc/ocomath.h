@@ -144,6 +144,46 @@ OCO_HD int oco_exp_fast(double xh, double xl, double *res) {
   return 1;
 }
 
+/* The fast phase above without branches: the same operations on every input (the table
+ * index is always in range; an out-of-range k or a non-finite input only makes *res
+ * meaningless), and 1 exactly when oco_exp_fast would return 1 with the same *res.  Several
+ * of these can be interleaved by the compiler; a caller falls back to oco_exp_dd on 0, which
+ * makes the pair identical to oco_exp_dd for every input. */
+OCO_HD int oco_exp_fast_nb(double xh, double xl, double *res) {
+  const double shift = 0x1.8p52;
+  const double ks = OCO_FMA(xh, OCO_EXPF_INVLN2N, shift);
+  const double kd = OCO_S(ks, shift);
+  const int ki = (int)(uint32_t)oco_d2u(ks);
+  const int j = ki & (OCO_EXPF_N - 1);
+  const int k = ki >> 10;
+  const int kok = (k > -1021) & (k < 1023);
+  const double d = OCO_FMA(-kd, OCO_EXPF_L1, xh);
+  const double rh = OCO_FMA(-kd, OCO_EXPF_L2, d);
+  double rl = OCO_FMA(-kd, OCO_EXPF_L2, OCO_S(d, rh));
+  rl = OCO_FMA(-kd, OCO_EXPF_L3, rl);
+  const double s = OCO_M(rh, rh);
+  double P = OCO_FMA(rh, OCO_EXP_C5, OCO_EXP_C4);
+  P = OCO_FMA(rh, P, OCO_EXP_C3);
+  P = OCO_FMA(rh, P, 0.5);
+  double ql = OCO_FMA(s, P, rl);
+  ql = OCO_A(ql, OCO_FMA(xl, OCO_A(rh, ql), xl));
+  const double Th = OCO_TAB(oco_expf_tab, 2 * j), Tl = OCO_TAB(oco_expf_tab, 2 * j + 1);
+  const double m = OCO_M(Th, rh);
+  const double me = OCO_FMA(Th, rh, -m);
+  const double hh = OCO_A(Th, m);
+  const double e2 = OCO_S(m, OCO_S(hh, Th));
+  const double lo = OCO_A(e2, OCO_A(me, OCO_FMA(Th, ql, OCO_FMA(Tl, rh, Tl))));
+  const double v = OCO_A(hh, lo);
+  const double t = OCO_S(lo, OCO_S(v, hh));
+  const uint64_t vb = oco_d2u(v);
+  const int ve = (int)(vb >> 52) & 0x7ff;
+  double half = oco_u2d((uint64_t)(ve - 53) << 52);
+  half = ((vb & 0x000fffffffffffffULL) == 0 && t < 0.0) ? OCO_M(half, 0.5) : half;
+  const double bound = OCO_S(half, oco_u2d((uint64_t)(ve - 71) << 52));
+  *res = OCO_M(v, oco_pow2i(kok ? k : 0));
+  return kok & (fabs(t) < bound) & (ve >= 0x3fe) & (ve <= 0x400);
+}
+
 /* e^(xh + xl) for a double-double argument with |xl| <= ulp(xh). */
 OCO_HD double oco_exp_dd(double xh, double xl) {
   if (oco_isnan(xh)) return OCO_A(xh, xh);
