@@ -225,7 +225,8 @@ typedef struct oco_batch_info {
 /* Describes a batch of ncol columns on the context's device: validates the descriptors,
  * builds one wavelength table per distinct (wave_off, nw) grid from waves[nwaves] (Angstrom,
  * host memory), sorts the work longest column first and reserves the device workspace.
- * form must be OCO_FORM_MIXED; layout is OCO_LAYOUT_*. */
+ * form is OCO_FORM_PLAIN, OCO_FORM_STABLE (per item the block solve's FP64 arithmetic, so
+ * the same bits) or OCO_FORM_MIXED; layout is OCO_LAYOUT_*. */
 int oco_batch_create(oco_ctx *ctx, const oco_batch_column *cols, int64_t ncol, const double *waves,
                      int64_t nwaves, int32_t form, int32_t layout, double fully_ionized_T,
                      oco_batch **batch);
@@ -243,7 +244,8 @@ int oco_batch_bind(oco_batch *batch, const double *rho, const double *T, int64_t
 int oco_batch_tune(oco_batch *batch);
 
 /* Sets the tiling by hand (instead of oco_batch_tune): tiling OCO_TILING_*, blocks_per_sm
- * from 1 to the kernel's occupancy limit (0 = that limit).  Recaptures the graph if bound. */
+ * from 1 to the kernel's occupancy limit (0 = that limit).  Recaptures the graph if bound.
+ * OCO_TILING_PACKED is available for the mixed form only. */
 int oco_batch_set_tiling(oco_batch *batch, int32_t tiling, int32_t blocks_per_sm);
 
 /* Replays the batch's graph on `stream` (a cudaStream_t; NULL is the CUDA default stream):
@@ -252,7 +254,9 @@ int oco_batch_set_tiling(oco_batch *batch, int32_t tiling, int32_t blocks_per_sm
 int oco_batch_run(oco_batch *batch, void *stream);
 
 /* Waits for the last oco_batch_run; returns OCO_ETIMEDOUT if a bounded wait in the kernel
- * ran out (its results are then incomplete). */
+ * ran out (its results are then incomplete), and for the plain form OCO_EZEROPIVOT when some
+ * item met an exactly zero Thomas pivot (every item is still computed, as in
+ * oco_solve_block; the message names the first column and wavelength). */
 int oco_batch_wait(oco_batch *batch);
 
 int oco_batch_get_info(const oco_batch *batch, oco_batch_info *info);

@@ -36,14 +36,9 @@ using namespace k;
 #endif
 
 /* ---- pillars ------------------------------------------------------------------------ */
-__global__ void __launch_bounds__(256) k_pillars(const double *__restrict__ rho,
-                                                 const double *__restrict__ T, int64_t n,
-                                                 double fully_ionized_T, int grey,
-                                                 double *__restrict__ pil) {
-  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double r = rho[i], t = T[i];
-  double *o = pil + i * NF;
+/* The record of one (column, z) cell from its rho and T. */
+__device__ __forceinline__ void pillar_record(const double r, const double t, double fully_ionized_T, int grey,
+                                              double *__restrict__ o) {
   if (grey) { /* grey_parameters, continuous_opacity.f90:383-384 */
     double t2 = t * t;
     o[G_RHO] = r;
@@ -106,6 +101,36 @@ __global__ void __launch_bounds__(256) k_pillars(const double *__restrict__ rho,
   o[F_LZ] = (oco_log(ne * (nHI + nHII)) + 2.0 * oco_log(1.0)) - 0.5 * oco_log(t);   /* c_o :292-294 */
   o[F_LNRHO] = oco_log(r);
   o[F_PAD] = 0.0;
+}
+
+__global__ void __launch_bounds__(256) k_pillars(const double *__restrict__ rho,
+                                                 const double *__restrict__ T, int64_t n,
+                                                 double fully_ionized_T, int grey,
+                                                 double *__restrict__ pil) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  pillar_record(rho[i], T[i], fully_ionized_T, grey, pil + i * NF);
+}
+
+/* Batch records: thread i is record i of the dense [sum nz] list; its column comes from a
+ * binary search of the nz prefix sums rec_pre[0..ncol]. */
+__global__ void __launch_bounds__(256) k_pillars_batch(const double *__restrict__ rho,
+                                                       const double *__restrict__ T,
+                                                       const MBatchCol *__restrict__ cols,
+                                                       const int64_t *__restrict__ rec_pre, int64_t ncol, int64_t n,
+                                                       double fully_ionized_T, double *__restrict__ pil) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int64_t lo = 0, hi = ncol;
+  while (hi - lo > 1) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (rec_pre[mid] <= i)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const int64_t src = cols[lo].in_off + (i - rec_pre[lo]);
+  pillar_record(rho[src], T[src], fully_ionized_T, 0, pil + i * NF);
 }
 
 /* ---- per-wavelength constants ------------------------------------------------------- */
@@ -315,24 +340,57 @@ struct StagedPillars {
 /* ---- the solve ----------------------------------------------------------------------- */
 /* Solves one (column, wavelength) item.  `active` false: the lane only keeps the warp's
  * shared pipeline in step (staged path, wavelength index beyond nw) and stores nothing. */
-template <int FORM, bool GREY, class PA>
-__device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int iw, bool active, PA &pa,
-                                           double *__restrict__ gam, double *__restrict__ uu,
-                                           double *__restrict__ o1s, double *__restrict__ qs) {
-  const int nz = a.nz;
-  const int64_t ss = a.slot_stride;
+/* What one (column, wavelength) item needs besides its records, as an accessor read on
+ * demand (kernel parameters and descriptors stay in their state spaces instead of registers).
+ * Block kernels: column cl of the chunk, wavelength iw. */
+struct BlockItem {
+  const SolveArgs &a;
+  int64_t cl;
+  int w;
+  __device__ __forceinline__ int64_t idx() const {
+    return (a.layout == 0) ? (int64_t)w * a.ld_col + a.c_off + cl : (a.c_off + cl) * a.nw + w;
+  }
+  __device__ __forceinline__ int64_t pidx() const { return (int64_t)w * a.ld_col + a.c_off + cl; }
+  __device__ __forceinline__ const double *lam() const { return a.lam; }
+  __device__ __forceinline__ int nz() const { return a.nz; }
+  __device__ __forceinline__ int nw() const { return a.nw; }
+  __device__ __forceinline__ int iw() const { return w; }
+  __device__ __forceinline__ double dz() const { return a.dz; }
+  __device__ __forceinline__ double dz2() const { return a.dz2; }
+  __device__ __forceinline__ double dz1() const { return a.dz1; }
+  __device__ __forceinline__ double sigma_grey() const { return a.sigma_grey; }
+  __device__ __forceinline__ double *U() const { return a.U ? a.U + idx() * a.U_is : nullptr; }
+  __device__ __forceinline__ double *K() const { return a.K ? a.K + idx() * a.K_is : nullptr; }
+  __device__ __forceinline__ double *V() const { return a.V ? a.V + idx() * a.V_is : nullptr; }
+  __device__ __forceinline__ int64_t uz() const { return a.U_zs; }
+  __device__ __forceinline__ int64_t kz() const { return a.K_zs; }
+  __device__ __forceinline__ int64_t vz() const { return a.V_zs; }
+  __device__ __forceinline__ double *vtop() const { return a.Vtop ? a.Vtop + pidx() : nullptr; }
+  __device__ __forceinline__ double *vbot() const { return a.Vbot ? a.Vbot + pidx() : nullptr; }
+  __device__ __forceinline__ int64_t ss() const { return a.slot_stride; }
+  __device__ __forceinline__ unsigned long long *status() const { return a.status; }
+  __device__ __forceinline__ unsigned long long id() const {
+    return (unsigned long long)((a.c_off + cl) * a.nw + w);
+  }
+};
+
+template <int FORM, bool GREY, class IT, class PA>
+__device__ __forceinline__ void solve_item(const IT &it, bool active, PA &pa, double *__restrict__ gam,
+                                           double *__restrict__ uu, double *__restrict__ o1s,
+                                           double *__restrict__ qs) {
+  const int nz = it.nz();
+  const int64_t ss = it.ss();
   Lam L;
-  if (!GREY) load_lam(L, a.lam, iw, a.nw);
-  const int64_t idx = (a.layout == 0) ? (int64_t)iw * a.ld_col + a.c_off + cl : (a.c_off + cl) * a.nw + iw;
-  double *Ub = a.U ? a.U + idx * a.U_is : nullptr; /* NULL: U not stored (flux-only runs) */
-  double *Kb = (a.K && active) ? a.K + idx * a.K_is : nullptr;
-  double *Vb = (a.V && active) ? a.V + idx * a.V_is : nullptr;
-  const double dz = a.dz, dz2 = a.dz2;
+  if (!GREY) load_lam(L, it.lam(), it.iw(), it.nw());
+  double *Ub = it.U();
+  double *Kb = active ? it.K() : nullptr;
+  double *Vb = active ? it.V() : nullptr;
+  const double dz = it.dz(), dz2 = it.dz2();
   bool bad = false;
 
   /* forward sweep: row 0 (fill_boundary_coeffs :187-191) */
-  Opac cur = GREY ? opacity_grey(pa.at(0), a.sigma_grey) : opacity_at<FORM == 1>(pa.at(0), L);
-  Opac nxt = GREY ? opacity_grey(pa.at(1), a.sigma_grey) : opacity_at<FORM == 1>(pa.at(1), L);
+  Opac cur = GREY ? opacity_grey(pa.at(0), it.sigma_grey()) : opacity_at<FORM == 1>(pa.at(0), L);
+  Opac nxt = GREY ? opacity_grey(pa.at(1), it.sigma_grey()) : opacity_at<FORM == 1>(pa.at(1), L);
   double o1 = 1.0 / cur.op, o2 = cur.op * cur.op;
   double zeta = ((cur.op * dz2) * (FORM == 1 ? cur.oma : (1.0 - cur.alb))) * 0.25;
   double bet, h = 0.0;
@@ -356,7 +414,7 @@ __device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int i
     o2 = op * op;
     double aa, bb, cc, dd, ee;
     if (j < nz - 1) { /* fill_center_coeffs :159-165 */
-      nxt = GREY ? opacity_grey(pa.at(j + 1), a.sigma_grey) : opacity_at<FORM == 1>(pa.at(j + 1), L);
+      nxt = GREY ? opacity_grey(pa.at(j + 1), it.sigma_grey()) : opacity_at<FORM == 1>(pa.at(j + 1), L);
       aa = o2 / kh_prev;
       double kh = 0.5 * (nxt.op + op);
       cc = o2 / kh;
@@ -390,19 +448,19 @@ __device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int i
     gam[j * ss] = g;
     uu[j * ss] = u;
     o1s[j * ss] = o1;
-    if (Kb) Kb[j * a.K_zs] = op;
+    if (Kb) Kb[j * it.kz()] = op;
     c_prev = cc;
     cur = nxt;
   }
   if (!active) return;
   if (bad) {
-    atomicAdd(&a.status[0], 1ull);
-    atomicMin(&a.status[1], (unsigned long long)((a.c_off + cl) * a.nw + iw));
+    atomicAdd(&it.status()[0], 1ull);
+    atomicMin(&it.status()[1], it.id());
   }
 
   /* reverse sweep: back-substitution (tridag :43-45), ghosts (:49-62), flux (:96-109) */
-  const double dz1 = a.dz1;
-  const int64_t uz = a.U_zs;
+  const double dz1 = it.dz1();
+  const int64_t uz = it.uz();
   double vtop = 0.0, vbot = 0.0;
   if (FORM == 1 && nz >= 4) {
     /* Stable form: the differences D_k = U_k - U_{k+1} = u_k - q_k U_{k+1} come out of the
@@ -432,7 +490,7 @@ __device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int i
       const double s3 = (s2 + d0) + d5;
       const double df = -((1.0 / 60.0) * (((45.0 * s1) - 9.0 * s2) + s3));
       const double v = ((-1.0 * o1s[j * ss]) * df) * dz1;
-      if (Vb) Vb[j * a.V_zs] = v;
+      if (Vb) Vb[j * it.vz()] = v;
       return v;
     };
     vtop = emitD(n - 1);
@@ -472,7 +530,7 @@ __device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int i
     auto emitV = [&](int j, double o1j, double w0, double w1, double w2, double w4, double w5, double w6) -> double {
       double df = (1.0 / 60.0) * (((45.0 * (w4 - w2)) - 9.0 * (w5 - w1)) + (w6 - w0));
       double v = ((-1.0 * o1j) * df) * dz1;
-      if (Vb) Vb[j * a.V_zs] = v;
+      if (Vb) Vb[j * it.vz()] = v;
       return v;
     };
     const int n = nz;
@@ -540,14 +598,13 @@ __device__ __forceinline__ void solve_item(const SolveArgs &a, int64_t cl, int i
       double df = (1.0 / 60.0) * (((45.0 * (f[c + 1] - f[c - 1])) - 9.0 * (f[c + 2] - f[c - 2])) +
                                   (f[c + 3] - f[c - 3]));
       double v = ((-1.0 * o1s[j * ss]) * df) * dz1;
-      if (Vb) Vb[j * a.V_zs] = v;
+      if (Vb) Vb[j * it.vz()] = v;
       if (j == 0) vbot = v;
       if (j == nz - 1) vtop = v;
     }
   }
-  const int64_t pidx = (int64_t)iw * a.ld_col + a.c_off + cl;
-  if (a.Vtop) a.Vtop[pidx] = vtop;
-  if (a.Vbot) a.Vbot[pidx] = vbot;
+  if (double *p = it.vtop()) *p = vtop;
+  if (double *p = it.vbot()) *p = vbot;
 }
 
 /* Generic path: warp tasks are 32 consecutive items of the flattened (column, lambda) index. */
@@ -571,7 +628,7 @@ __global__ void __launch_bounds__(128) k_solve(const SolveArgs a) {
       const int64_t cl = item / a.nw;
       const int iw = (int)(item - cl * a.nw);
       DirectPillars pa{a.pil + cl * (int64_t)a.nz * NF};
-      solve_item<FORM, GREY>(a, cl, iw, true, pa, gam, uu, o1, qs);
+      solve_item<FORM, GREY>(BlockItem{a, cl, iw}, true, pa, gam, uu, o1, qs);
     }
   }
 }
@@ -614,7 +671,7 @@ __global__ void __launch_bounds__(128, 4) k_solve_staged(const SolveArgs a) {
     const bool active = iw_raw < a.nw;
     const int iw = active ? iw_raw : a.nw - 1;
     pa.begin(a.pil + cl * (int64_t)a.nz * NF, lane);
-    solve_item<FORM, GREY>(a, cl, iw, active, pa, gam, uu, o1, qs);
+    solve_item<FORM, GREY>(BlockItem{a, cl, iw}, active, pa, gam, uu, o1, qs);
     if (__any_sync(0xffffffffu, pa.failed)) {
       if (lane == 0) atomicOr(&a.status[2], 1ull);
       /* let copies still in flight land (bounded) before the block's shared memory is released */
@@ -623,6 +680,107 @@ __global__ void __launch_bounds__(128, 4) k_solve_staged(const SolveArgs a) {
       return;
     }
   }
+}
+
+/* ---- ragged batches (FP64 forms) -------------------------------------------------------- */
+/* Item of a batch: wavelength w of column *c (descriptor read through the read-only cache). */
+struct BatchItem {
+  const FP64BatchArgs &b;
+  const MBatchCol *c;
+  int64_t col;
+  int w;
+  __device__ __forceinline__ int nz() const { return __ldg(&c->nz); }
+  __device__ __forceinline__ int nw() const { return __ldg(&c->nw); }
+  __device__ __forceinline__ int iw() const { return w; }
+  __device__ __forceinline__ const double *lam() const { return b.lam + __ldg(&c->lam_off); }
+  __device__ __forceinline__ double dz() const { return __ldg(&c->dz); }
+  __device__ __forceinline__ double dz2() const { return __ldg(&c->dz2); }
+  __device__ __forceinline__ double dz1() const { return __ldg(&c->dz1); }
+  __device__ __forceinline__ double sigma_grey() const { return 0.0; }
+  __device__ __forceinline__ int64_t zoff(int64_t base, int rows) const { /* element z = 0 */
+    return b.layout == 0 ? base + (int64_t)w * rows : base + w;
+  }
+  __device__ __forceinline__ double *U() const { return b.U ? b.U + zoff(__ldg(&c->u_off), nz() + 6) : nullptr; }
+  __device__ __forceinline__ double *K() const { return b.K ? b.K + zoff(__ldg(&c->kv_off), nz()) : nullptr; }
+  __device__ __forceinline__ double *V() const { return b.V ? b.V + zoff(__ldg(&c->kv_off), nz()) : nullptr; }
+  __device__ __forceinline__ int64_t uz() const { return b.layout == 0 ? 1 : nw(); }
+  __device__ __forceinline__ int64_t kz() const { return uz(); }
+  __device__ __forceinline__ int64_t vz() const { return uz(); }
+  __device__ __forceinline__ double *vtop() const { return b.Vtop ? b.Vtop + __ldg(&c->flux_off) + w : nullptr; }
+  __device__ __forceinline__ double *vbot() const { return b.Vbot ? b.Vbot + __ldg(&c->flux_off) + w : nullptr; }
+  __device__ __forceinline__ int64_t ss() const { return b.slot_stride; }
+  __device__ __forceinline__ unsigned long long *status() const { return b.status; }
+  __device__ __forceinline__ unsigned long long id() const { return ((unsigned long long)col << 32) | (unsigned)w; }
+};
+
+/* Warp-column tiling: tasks (column, 32-wavelength tile) from the device queue, longest
+ * columns first; the column's records stream through the warp's shared-memory buffers. */
+template <int FORM>
+__global__ void __launch_bounds__(128, 4) k_batch_fp64_staged(const FP64BatchArgs b) {
+  __shared__ __align__(128) double s_pil[WARPS_PER_BLOCK][2 * ZC * NF];
+  __shared__ __align__(8) unsigned long long s_bar[WARPS_PER_BLOCK][2];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  double *gam = b.gam + slot * 32 + lane;
+  double *uu = b.uu + slot * 32 + lane;
+  double *o1 = b.o1 + slot * 32 + lane;
+  double *qs = b.q + slot * 32 + lane;
+  StagedPillars pa;
+  pa.buf = s_pil[wib];
+  pa.bar0 = smem_addr(&s_bar[wib][0]);
+  pa.waits = 0;
+  pa.inflight = 0;
+  pa.failed = false;
+  if (lane == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(pa.bar0) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(pa.bar0 + 8u) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  for (;;) {
+    unsigned long long task = 0;
+    if (lane == 0) task = atomicAdd(b.work, 1ull);
+    task = __shfl_sync(0xffffffffu, task, 0);
+    if (task >= (unsigned long long)b.ntasks) break;
+    const uint2 t = b.tasks[task];
+    const MBatchCol *c = b.cols + t.x;
+    const int nw = __ldg(&c->nw);
+    const int iw_raw = (int)t.y * 32 + lane;
+    const bool active = iw_raw < nw;
+    const int iw = active ? iw_raw : nw - 1;
+    pa.nz = __ldg(&c->nz);
+    pa.begin(b.pil + __ldg(&c->rec_off) * NF, lane);
+    solve_item<FORM, false>(BatchItem{b, c, (int64_t)t.x, iw}, active, pa, gam, uu, o1, qs);
+    if (__any_sync(0xffffffffu, pa.failed)) {
+      if (lane == 0) atomicOr(&b.status[2], 1ull);
+      pa.wait(0);
+      pa.wait(1);
+      return;
+    }
+  }
+}
+
+cudaError_t launch_pillars_batch(const double *rho, const double *T, const MBatchCol *cols, const int64_t *rec_pre,
+                                 int64_t ncol, int64_t nrec, double fully_ionized_T, double *pil, cudaStream_t s) {
+  if (nrec == 0) return cudaSuccess;
+  k_pillars_batch<<<(unsigned)((nrec + 255) / 256), 256, 0, s>>>(rho, T, cols, rec_pre, ncol, nrec, fully_ionized_T,
+                                                                 pil);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_fp64(const FP64BatchArgs &a, int form, int blocks, int threads, cudaStream_t s) {
+  if (form == 0)
+    k_batch_fp64_staged<0><<<blocks, threads, 0, s>>>(a);
+  else
+    k_batch_fp64_staged<1><<<blocks, threads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+int batch_fp64_max_blocks_per_sm(int form, int threads) {
+  int n = 0;
+  const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &n, form == 0 ? (const void *)k_batch_fp64_staged<0> : (const void *)k_batch_fp64_staged<1>, threads, 0);
+  return (e == cudaSuccess && n > 0) ? n : 1;
 }
 
 cudaError_t launch_pillars(const double *rho, const double *T, int64_t ncol, int nz,

@@ -13,6 +13,9 @@
  * The autotuner (oco_batch_tune) times every (tiling, resident blocks per SM) candidate on
  * the bound arrays and keeps the fastest.
  *
+ * The FP64 forms (plain, stable) run the warp-column tiling only, with the FP64 records and
+ * the block solve's per-item arithmetic (bit-identical to it, and so to the oracle).
+ *
  * Graph.  oco_batch_bind captures: counter reset, status reset, the record kernel over all
  * columns' z values, the solve kernel.  oco_batch_run replays it on the caller's stream.
  */
@@ -37,6 +40,7 @@ static const int kBatchThreads = 128;
 
 struct oco_batch {
   oco_ctx *c = nullptr;
+  int form = OCO_FORM_MIXED;
   int layout = OCO_LAYOUT_LAMBDA_FASTEST;
   double fully_ionized_T = 2e4;
   int64_t ncol = 0, npoints = 0, nrec = 0, nitems = 0, ntasks_tile = 0, ntasks_packed = 0;
@@ -44,7 +48,7 @@ struct oco_batch {
   int64_t need_in = 0, need_u = 0, need_kv = 0, need_flux = 0; /* element counts the arrays must hold */
   DevBuf cols, rec_pre, tasks, order, item_pre, lam, rec, scratch, work, status;
   int64_t slots = 0; /* scratch slots (threads of the largest persistent grid) */
-  int tiling = OCO_TILING_WARP_COLUMN, bps = 1, max_bps[2] = {1, 1};
+  int tiling = OCO_TILING_WARP_COLUMN, bps = 1, max_bps[2] = {1, 1}; /* max_bps 0: tiling not available */
   /* bound arrays */
   bool bound = false;
   const double *rho = nullptr, *T = nullptr;
@@ -81,17 +85,49 @@ static MixedBatchArgs batch_args(const oco_batch *b) {
   return a;
 }
 
+static FP64BatchArgs fp64_args(const oco_batch *b) {
+  FP64BatchArgs a{};
+  a.pil = b->rec.as<double>();
+  a.lam = b->lam.as<double>();
+  a.cols = b->cols.as<MBatchCol>();
+  a.tasks = b->tasks.as<uint2>();
+  a.ntasks = b->ntasks_tile;
+  a.U = b->U;
+  a.K = b->K;
+  a.V = b->V;
+  a.Vtop = b->Vtop;
+  a.Vbot = b->Vbot;
+  a.layout = b->layout;
+  const size_t plane = (size_t)b->slots * b->max_nz;
+  double *sc = b->scratch.as<double>();
+  a.gam = sc;
+  a.uu = sc + plane;
+  a.o1 = sc + 2 * plane;
+  a.q = sc + 3 * plane;
+  a.slot_stride = b->slots;
+  a.work = b->work.as<unsigned long long>();
+  a.status = b->status.as<unsigned long long>();
+  return a;
+}
+
 /* Enqueues one run (counter and status reset, records, solve) on s. */
 static int enqueue_run(oco_batch *b, cudaStream_t s) {
   oco_ctx *c = b->c;
   CU(cudaMemsetAsync(b->work.p, 0, sizeof(unsigned long long), s));
   CU(cudaMemsetAsync(b->status.p, 0, 3 * sizeof(unsigned long long), s));
-  CU(launch_pillars_mixed_batch(b->rho, b->T, b->cols.as<MBatchCol>(), b->rec_pre.as<int64_t>(), b->ncol, b->nrec,
-                                b->fully_ionized_T, b->rec.as<float>(), s));
-  const MixedBatchArgs a = batch_args(b);
+  CU(cudaMemsetAsync(b->status.as<unsigned long long>() + 1, 0xff, sizeof(unsigned long long), s)); /* atomicMin */
   const int blocks = b->bps * c->num_sms;
-  CU(launch_batch_mixed(a, b->tiling == OCO_TILING_PACKED ? BATCH_TILING_PACKED : BATCH_TILING_WARP_COLUMN, blocks,
-                        kBatchThreads, s));
+  if (b->form == OCO_FORM_MIXED) {
+    CU(launch_pillars_mixed_batch(b->rho, b->T, b->cols.as<MBatchCol>(), b->rec_pre.as<int64_t>(), b->ncol, b->nrec,
+                                  b->fully_ionized_T, b->rec.as<float>(), s));
+    const MixedBatchArgs a = batch_args(b);
+    CU(launch_batch_mixed(a, b->tiling == OCO_TILING_PACKED ? BATCH_TILING_PACKED : BATCH_TILING_WARP_COLUMN, blocks,
+                          kBatchThreads, s));
+  } else {
+    CU(launch_pillars_batch(b->rho, b->T, b->cols.as<MBatchCol>(), b->rec_pre.as<int64_t>(), b->ncol, b->nrec,
+                            b->fully_ionized_T, b->rec.as<double>(), s));
+    CU(launch_batch_fp64(fp64_args(b), b->form == OCO_FORM_STABLE ? 1 : 0, blocks, kBatchThreads, s));
+  }
   return OCO_OK;
 }
 
@@ -119,11 +155,17 @@ static int capture(oco_batch *b) {
   return OCO_OK;
 }
 
-static int check_status(oco_batch *b) {
+/* Reads the last run's status: OCO_ETIMEDOUT, then (report_pivots, FP64 forms)
+ * OCO_EZEROPIVOT. */
+static int check_status(oco_batch *b, bool report_pivots = true) {
   oco_ctx *c = b->c;
   unsigned long long st[3];
   CU(cudaMemcpy(st, b->status.p, sizeof st, cudaMemcpyDeviceToHost));
   if (st[2]) return oco_set_err(c, OCO_ETIMEDOUT, "batch: a bounded wait for a record copy ran out; results are incomplete");
+  if (report_pivots && b->form != OCO_FORM_MIXED && st[0])
+    return oco_set_err(c, OCO_EZEROPIVOT,
+                       "ERROR tridiag: bet == 0 in %llu (column, wavelength) items; first: column %llu, iw=%llu",
+                       st[0], st[1] >> 32, (st[1] & 0xffffffffull) + 1);
   return OCO_OK;
 }
 
@@ -133,7 +175,8 @@ extern "C" int oco_batch_create(oco_ctx *c, const oco_batch_column *cols, int64_
   if (!c) return oco_set_err(nullptr, OCO_EINVAL, "oco_batch_create: NULL context");
   if (!out) return oco_set_err(c, OCO_EINVAL, "oco_batch_create: out is NULL");
   *out = nullptr;
-  if (form != OCO_FORM_MIXED) return oco_set_err(c, OCO_EINVAL, "oco_batch_create: batches run the mixed form only");
+  if (form != OCO_FORM_MIXED && form != OCO_FORM_PLAIN && form != OCO_FORM_STABLE)
+    return oco_set_err(c, OCO_EINVAL, "oco_batch_create: bad form %d", form);
   if (layout != OCO_LAYOUT_REFERENCE && layout != OCO_LAYOUT_LAMBDA_FASTEST)
     return oco_set_err(c, OCO_EINVAL, "oco_batch_create: bad layout %d", layout);
   if (!cols || ncol < 1 || ncol > (int64_t)INT32_MAX)
@@ -148,6 +191,7 @@ extern "C" int oco_batch_create(oco_ctx *c, const oco_batch_column *cols, int64_
   if (!b) return oco_set_err(c, OCO_ENOMEM, "oco_batch_create: out of host memory");
   std::unique_ptr<oco_batch, void (*)(oco_batch *)> guard(b, oco_batch_destroy);
   b->c = c;
+  b->form = form;
   b->layout = layout;
   b->fully_ionized_T = fully_ionized_T;
   b->ncol = ncol;
@@ -156,7 +200,9 @@ extern "C" int oco_batch_create(oco_ctx *c, const oco_batch_column *cols, int64_
   std::vector<MBatchCol> dc((size_t)ncol);
   std::vector<int64_t> rpre((size_t)ncol + 1, 0);
   std::map<std::pair<int64_t, int32_t>, int64_t> grids;
-  std::vector<float> lam;
+  const bool fp64 = form != OCO_FORM_MIXED;
+  std::vector<float> lam;     /* mixed tables */
+  std::vector<double> lam64;  /* FP64 tables */
   std::vector<double> tab;
   for (int64_t i = 0; i < ncol; i++) {
     const oco_batch_column &q = cols[i];
@@ -170,11 +216,16 @@ extern "C" int oco_batch_create(oco_ctx *c, const oco_batch_column *cols, int64_
     auto it = grids.find(key);
     int64_t loff;
     if (it == grids.end()) {
-      loff = (int64_t)lam.size();
       tab.assign((size_t)NL * q.nw, 0.0);
       fill_lambda_table(waves + q.wave_off, q.nw, tab.data());
-      lam.resize(lam.size() + (size_t)MIXED_LN * q.nw);
-      fill_mixed_lambda_table(tab.data(), q.nw, lam.data() + loff);
+      if (fp64) {
+        loff = (int64_t)lam64.size();
+        lam64.insert(lam64.end(), tab.begin(), tab.end());
+      } else {
+        loff = (int64_t)lam.size();
+        lam.resize(lam.size() + (size_t)MIXED_LN * q.nw);
+        fill_mixed_lambda_table(tab.data(), q.nw, lam.data() + loff);
+      }
       grids.emplace(key, loff);
     } else {
       loff = it->second;
@@ -191,6 +242,8 @@ extern "C" int oco_batch_create(oco_ctx *c, const oco_batch_column *cols, int64_
     d.dzf = (float)q.dz;
     mx::ldz2_split(q.dz, d.ldz2i, d.ldz2f);
     d.dz1 = 1.0 / q.dz;
+    d.dz = q.dz;
+    d.dz2 = q.dz * q.dz;
     rpre[(size_t)i + 1] = rpre[(size_t)i] + q.nz;
     b->npoints += (int64_t)q.nz * q.nw;
     b->nitems += q.nw;
@@ -221,8 +274,13 @@ extern "C" int oco_batch_create(oco_ctx *c, const oco_batch_column *cols, int64_
   /* device state */
   CU(cudaSetDevice(c->device));
   CU(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
-  b->max_bps[0] = batch_mixed_max_blocks_per_sm(BATCH_TILING_WARP_COLUMN, kBatchThreads);
-  b->max_bps[1] = batch_mixed_max_blocks_per_sm(BATCH_TILING_PACKED, kBatchThreads);
+  if (fp64) {
+    b->max_bps[0] = batch_fp64_max_blocks_per_sm(form == OCO_FORM_STABLE ? 1 : 0, kBatchThreads);
+    b->max_bps[1] = 0;
+  } else {
+    b->max_bps[0] = batch_mixed_max_blocks_per_sm(BATCH_TILING_WARP_COLUMN, kBatchThreads);
+    b->max_bps[1] = batch_mixed_max_blocks_per_sm(BATCH_TILING_PACKED, kBatchThreads);
+  }
   b->slots = (int64_t)std::max(b->max_bps[0], b->max_bps[1]) * c->num_sms * kBatchThreads;
   b->tiling = OCO_TILING_WARP_COLUMN;
   b->bps = b->max_bps[0];
@@ -231,9 +289,15 @@ extern "C" int oco_batch_create(oco_ctx *c, const oco_batch_column *cols, int64_
   CU(b->tasks.ensure(tasks.size() * sizeof(uint2)));
   CU(b->order.ensure(order.size() * sizeof(int32_t)));
   CU(b->item_pre.ensure(ipre.size() * sizeof(int64_t)));
-  CU(b->lam.ensure(lam.size() * sizeof(float)));
-  CU(b->rec.ensure((size_t)b->nrec * MIXED_ZN * sizeof(float)));
-  CU(b->scratch.ensure((size_t)b->slots * b->max_nz * sizeof(float4)));
+  if (fp64) {
+    CU(b->lam.ensure(lam64.size() * sizeof(double)));
+    CU(b->rec.ensure((size_t)b->nrec * NF * sizeof(double)));
+    CU(b->scratch.ensure((size_t)4 * b->slots * b->max_nz * sizeof(double)));
+  } else {
+    CU(b->lam.ensure(lam.size() * sizeof(float)));
+    CU(b->rec.ensure((size_t)b->nrec * MIXED_ZN * sizeof(float)));
+    CU(b->scratch.ensure((size_t)b->slots * b->max_nz * sizeof(float4)));
+  }
   CU(b->work.ensure(64));
   CU(b->status.ensure(64));
   CU(cudaMemcpy(b->cols.p, dc.data(), dc.size() * sizeof(MBatchCol), cudaMemcpyHostToDevice));
@@ -241,7 +305,10 @@ extern "C" int oco_batch_create(oco_ctx *c, const oco_batch_column *cols, int64_
   CU(cudaMemcpy(b->tasks.p, tasks.data(), tasks.size() * sizeof(uint2), cudaMemcpyHostToDevice));
   CU(cudaMemcpy(b->order.p, order.data(), order.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   CU(cudaMemcpy(b->item_pre.p, ipre.data(), ipre.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(b->lam.p, lam.data(), lam.size() * sizeof(float), cudaMemcpyHostToDevice));
+  if (fp64)
+    CU(cudaMemcpy(b->lam.p, lam64.data(), lam64.size() * sizeof(double), cudaMemcpyHostToDevice));
+  else
+    CU(cudaMemcpy(b->lam.p, lam.data(), lam.size() * sizeof(float), cudaMemcpyHostToDevice));
   CU(cudaMemset(b->status.p, 0, 64));
 
   b->info.ncol = ncol;
@@ -292,7 +359,7 @@ extern "C" int oco_batch_tune(oco_batch *b) {
   std::vector<Cand> cands;
   for (int t = 0; t < 2; t++)
     for (int d = 0; d < 3; d++) {
-      const int bps = b->max_bps[t] - d;
+      const int bps = b->max_bps[t] - d; /* max_bps 0: tiling not available for the form */
       if (bps >= 1) cands.push_back({t, bps, 0.0f});
     }
   if (cands.size() > 16) cands.resize(16);
@@ -315,7 +382,7 @@ extern "C" int oco_batch_tune(oco_batch *b) {
       break;
     }
     cudaEventElapsedTime(&k.ms, e0, e1);
-    if ((rc = check_status(b))) break;
+    if ((rc = check_status(b, false))) break; /* zero pivots are reported by oco_batch_wait */
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -341,6 +408,7 @@ extern "C" int oco_batch_set_tiling(oco_batch *b, int32_t tiling, int32_t blocks
   if (tiling != OCO_TILING_WARP_COLUMN && tiling != OCO_TILING_PACKED)
     return oco_set_err(c, OCO_EINVAL, "oco_batch_set_tiling: bad tiling %d", tiling);
   const int lim = b->max_bps[tiling];
+  if (lim == 0) return oco_set_err(c, OCO_EINVAL, "oco_batch_set_tiling: the packed tiling runs the mixed form only");
   if (blocks_per_sm < 0 || blocks_per_sm > lim)
     return oco_set_err(c, OCO_EINVAL, "oco_batch_set_tiling: blocks_per_sm must be 0..%d", lim);
   CU(cudaSetDevice(c->device));

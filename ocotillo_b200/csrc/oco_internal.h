@@ -125,11 +125,12 @@ struct MBatchCol {
   int64_t u_off;    /* first U element of the column */
   int64_t kv_off;   /* first kappa / V element */
   int64_t flux_off; /* first emergent-flux element */
-  int64_t lam_off;  /* first float of the column's [MIXED_LN][nw] wavelength table */
+  int64_t lam_off;  /* first element of the column's wavelength table ([MIXED_LN][nw] floats or [NL][nw] doubles) */
   int32_t nz, nw;
   float dzf;        /* dz */
   float ldz2i, ldz2f; /* log2(dz^2) = integer + fraction */
   double dz1;       /* 1/dz */
+  double dz, dz2;   /* dz and dz*dz (FP64 forms, flux_feautrier.f90:151-154) */
 };
 
 /* Arguments of the ragged-batch kernels (mixed form). */
@@ -148,6 +149,25 @@ struct MixedBatchArgs {
   unsigned long long *work;
   unsigned long long *status;
 };
+
+/* Arguments of the ragged-batch kernels (plain and stable FP64 forms; warp-column tiling). */
+struct FP64BatchArgs {
+  const double *pil;       /* [sum nz][NF] records */
+  const double *lam;       /* packed [NL][nw] wavelength tables */
+  const MBatchCol *cols;
+  const uint2 *tasks;      /* (column, 32-wavelength tile), longest column first */
+  int64_t ntasks;
+  double *U, *K, *V, *Vtop, *Vbot;
+  int layout;
+  double *gam, *uu, *o1, *q; /* scratch [max_nz][slots] each */
+  int64_t slot_stride;
+  unsigned long long *work;
+  unsigned long long *status; /* [0] zero pivots, [1] first (column << 32 | wavelength), [2] timeout */
+};
+cudaError_t launch_pillars_batch(const double *rho, const double *T, const MBatchCol *cols, const int64_t *rec_pre,
+                                 int64_t ncol, int64_t nrec, double fully_ionized_T, double *pil, cudaStream_t s);
+cudaError_t launch_batch_fp64(const FP64BatchArgs &a, int form, int blocks, int threads, cudaStream_t s);
+int batch_fp64_max_blocks_per_sm(int form, int threads);
 
 /* Tilings of the batch kernels. */
 constexpr int BATCH_TILING_WARP_COLUMN = 0; /* a warp solves 32 wavelengths of one column, records staged */

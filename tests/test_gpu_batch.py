@@ -1,11 +1,15 @@
 """Ragged batches (oco_batch_*): independent columns of different nz, dz and wavelength grids
-in one persistent launch replayed as a CUDA graph, mixed form.
+in one persistent launch replayed as a CUDA graph.
 
-Per column the batch runs the arithmetic of the block solve's mixed form, so every column is
-compared with a 1x1 block solve of the same column (relative difference <= 1e-6: same
-operations, possibly contracted into FMAs differently by the two kernel instantiations), and a
-few columns with the stable FP64 oracle at the mixed form's tolerances.  Tilings and graph
-replays must give identical results.
+Mixed form: per column the batch runs the arithmetic of the block solve's mixed form, so every
+column is compared with a 1x1 block solve of the same column (relative difference <= 1e-6:
+same operations, possibly contracted into FMAs differently by the two kernel instantiations),
+and a few columns with the stable FP64 oracle at the mixed form's tolerances.  Tilings and
+graph replays must give identical results.
+
+Plain and stable FP64 forms: per item the block solve's FP64 arithmetic, so every column must
+equal a 1x1 block solve of it bit for bit, and the plain form must equal the oracle (reference
+arithmetic, ocomath back-end) bit for bit.
 """
 import numpy as np
 import pytest
@@ -52,9 +56,9 @@ def _small_batch(seed=11):
             "rho": np.concatenate(rhos), "T": np.concatenate(Ts)}
 
 
-def _make(engine, d, layout):
+def _make(engine, d, layout, form="mixed"):
     import torch
-    b = engine.batch(d["nz"], d["nw"], d["dz"], d["waves"], d["wave_off"], layout=layout)
+    b = engine.batch(d["nz"], d["nw"], d["dz"], d["waves"], d["wave_off"], layout=layout, form=form)
     dev = torch.device("cuda:0")
     rho = torch.from_numpy(d["rho"]).to(dev)
     T = torch.from_numpy(d["T"]).to(dev)
@@ -63,15 +67,33 @@ def _make(engine, d, layout):
     return b, rho, T, out
 
 
-def _block(engine, d, i):
-    """Column i as a 1x1 block through the block solve (host arrays), mixed form."""
+def _block(engine, d, i, form="mixed"):
+    """Column i as a 1x1 block through the block solve (host arrays)."""
     o = np.concatenate([[0], np.cumsum(d["nz"])])
     nz, nw = int(d["nz"][i]), int(d["nw"][i])
     wa = d["waves"][d["wave_off"][i]:d["wave_off"][i] + nw]
     engine.set_wavelengths(wa)
     rho = d["rho"][o[i]:o[i + 1]].reshape(1, 1, nz)
     T = d["T"][o[i]:o[i + 1]].reshape(1, 1, nz)
-    return engine.solve_block(rho, T, float(d["dz"][i]), form="mixed"), rho, T, wa
+    return engine.solve_block(rho, T, float(d["dz"][i]), form=form, allow_zero_pivot=True), rho, T, wa
+
+
+def _same(t, ref):
+    """Bit-for-bit equality; the reference arithmetic can give NaN (a zero pivot), which must
+    then sit in the same places."""
+    a = np.ascontiguousarray(t.cpu().numpy() if hasattr(t, "cpu") else t)
+    ref = np.ascontiguousarray(ref)
+    return a.shape == ref.shape and np.array_equal(a.view(np.uint64), ref.view(np.uint64))
+
+
+def _run_fp64(b):
+    """Runs a plain/stable batch; a zero pivot (plain form) is reported after every item is done."""
+    from ocotillo_b200 import OcoError
+    b.run()
+    try:
+        b.wait()
+    except OcoError as e:
+        assert e.code == -3, e
 
 
 def _rel(a, b):
@@ -188,7 +210,11 @@ def test_batch_rejects_bad_descriptors(engine):
     from ocotillo_b200 import OcoError
     d = _small_batch()
     with pytest.raises(OcoError):
-        engine.batch(d["nz"], d["nw"], d["dz"], d["waves"], d["wave_off"], form="plain")
+        engine.batch(d["nz"], d["nw"], d["dz"], d["waves"], d["wave_off"], form=7)
+    bp = engine.batch(d["nz"], d["nw"], d["dz"], d["waves"], d["wave_off"], form="plain")
+    with pytest.raises(OcoError):
+        bp.set_tiling("packed", 0)  # the packed tiling runs the mixed form only
+    bp.close()
     bad = d["nz"].copy()
     bad[3] = 1
     with pytest.raises(OcoError):
@@ -207,4 +233,42 @@ def test_batch_rejects_bad_descriptors(engine):
         b.run()  # not bound
     with pytest.raises(OcoError):
         b.set_tiling("packed", 99)
+    b.close()
+
+
+@pytest.mark.parametrize("form,layout", [("plain", 0), ("plain", 1), ("stable", 0), ("stable", 1)])
+def test_batch_fp64_bitwise_block_solve(engine, form, layout):
+    d = _small_batch(seed=16)
+    b, _, _, out = _make(engine, d, layout, form=form)
+    _run_fp64(b)
+    for i in range(len(d["nz"])):
+        ref, _, _, _ = _block(engine, d, i, form=form)
+        what = f"column {i} nz={d['nz'][i]} nw={d['nw'][i]} form={form} layout={layout}"
+        assert _same(b.column(out, i, "U"), ref["U"][:, 0, 0, :].T), what
+        assert _same(b.column(out, i, "kappa"), ref["kappa"][:, 0, 0, :].T), what
+        assert _same(b.column(out, i, "V"), ref["V"][:, 0, 0, :].T), what
+        assert _same(b.column(out, i, "Vtop"), ref["Vtop"][:, 0, 0]), what
+        assert _same(b.column(out, i, "Vbot"), ref["Vbot"][:, 0, 0]), what
+    b.close()
+
+
+def test_batch_plain_bitwise_oracle(engine, oracle):
+    d = _small_batch(seed=17)
+    b, _, _, out = _make(engine, d, 1, form="plain")
+    _run_fp64(b)
+    b.set_tiling("warp_column", 2)  # another resident-block count, same bits
+    first = {k: v.cpu().numpy().copy() for k, v in out.items()}
+    _run_fp64(b)
+    o = np.concatenate([[0], np.cumsum(d["nz"])])
+    for i in range(len(d["nz"])):
+        nz, nw = int(d["nz"][i]), int(d["nw"][i])
+        wa = d["waves"][d["wave_off"][i]:d["wave_off"][i] + nw]
+        rho = d["rho"][o[i]:o[i + 1]].reshape(1, 1, nz)
+        T = d["T"][o[i]:o[i + 1]].reshape(1, 1, nz)
+        ref = oracle.solve_block(rho, T, wa, float(d["dz"][i]), form=oracle.FORM_REFERENCE, backend="ocomath")
+        what = f"column {i} nz={nz} nw={nw}"
+        for name in ("U", "kappa", "V"):
+            assert _same(b.column(out, i, name), ref[name][:, 0, 0, :].T), (name, what)
+    for k, v in out.items():
+        assert _same(v, first[k]), k
     b.close()
