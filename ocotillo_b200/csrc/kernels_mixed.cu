@@ -27,6 +27,11 @@ constexpr long long kMSpinLimit = 1ll << 26;
 #ifndef OCO_MIXED_PREFETCH
 #define OCO_MIXED_PREFETCH 4 /* reverse-sweep steps whose scratch loads are issued together */
 #endif
+#ifndef OCO_MIXED_L2_AHEAD
+#define OCO_MIXED_L2_AHEAD 8 /* reverse-sweep steps between the L2 prefetch and the load of a scratch level */
+#endif
+
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
 /* Shared-memory record accessor. */
 struct MRec {
@@ -280,6 +285,11 @@ __device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa
     constexpr int PF = OCO_MIXED_PREFETCH;
     for (; k >= PF - 1; k -= PF) { /* scratch loads of PF steps hoisted off the serial chain */
       float4 w[PF];
+      /* the scratch level OCO_MIXED_L2_AHEAD steps ahead into L2 (it was written a whole
+       * forward sweep ago and has usually left L2) */
+#pragma unroll
+      for (int q = 0; q < PF; q++)
+        if (k - q >= OCO_MIXED_L2_AHEAD) prefetch_l2(s4 + (int64_t)(k - q - OCO_MIXED_L2_AHEAD) * ss);
 #pragma unroll
       for (int q = 0; q < PF; q++) w[q] = s4[(int64_t)(k - q) * ss];
 #pragma unroll
