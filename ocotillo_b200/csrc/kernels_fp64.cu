@@ -15,6 +15,10 @@
  *               (:49-62) and 6th-order flux (:64-109) in one reverse sweep with a 7-point
  *               register window.
  *
+ * Output stores (U, kappa, V and the emergent flux) use the streaming cache hint (st.global.cs,
+ * evict first): they are never read back, and L2 then keeps more of the forward sweep's scratch
+ * for the reverse sweep.
+ *
  * This translation unit is compiled with -fmad=false (no FMA contraction) and IEEE
  * division/square root, and calls the ocomath functions, so FORM_PLAIN reproduces the CPU
  * oracle (ocomath back-end) bit for bit.  FORM_STABLE replaces the pivot recursion
@@ -404,7 +408,7 @@ __device__ __forceinline__ void solve_item(const IT &it, bool active, PA &pa, do
   double u = (-((cur.S * zeta) * o2)) / bet;
   uu[0] = u;
   o1s[0] = o1;
-  if (Kb) Kb[0] = cur.op;
+  if (Kb) __stcs(&Kb[0], cur.op);
   double c_prev = cur.op;
   double kh_prev = 0.5 * (nxt.op + cur.op); /* kappa_p(1) = kappa_m(2), :147-154 */
   cur = nxt;
@@ -448,7 +452,7 @@ __device__ __forceinline__ void solve_item(const IT &it, bool active, PA &pa, do
     gam[j * ss] = g;
     uu[j * ss] = u;
     o1s[j * ss] = o1;
-    if (Kb) Kb[j * it.kz()] = op;
+    if (Kb) __stcs(&Kb[j * it.kz()], op);
     c_prev = cc;
     cur = nxt;
   }
@@ -469,7 +473,7 @@ __device__ __forceinline__ void solve_item(const IT &it, bool active, PA &pa, do
      * stencil on U, accurate where U's differences are below its resolution. */
     const int n = nz;
     double Un = u; /* U_{n-1} */
-    if (Ub) Ub[(3 + n - 1) * uz] = Un;
+    if (Ub) __stcs(&Ub[(3 + n - 1) * uz], Un);
     double Uk[3], Dt[3];
     for (int t = 0; t < 3; t++) {
       const int k = n - 2 - t;
@@ -477,12 +481,12 @@ __device__ __forceinline__ void solve_item(const IT &it, bool active, PA &pa, do
       Dt[t] = uf - qs[k * ss] * Un;
       Un = uf - gam[(k + 1) * ss] * Un;
       Uk[t] = Un;
-      if (Ub) Ub[(3 + k) * uz] = Un;
+      if (Ub) __stcs(&Ub[(3 + k) * uz], Un);
     }
     const double fn = u;
-    if (Ub) Ub[(n + 3) * uz] = 2.0 * fn - Uk[0];
-    if (Ub) Ub[(n + 4) * uz] = 2.0 * fn - Uk[1];
-    if (Ub) Ub[(n + 5) * uz] = 2.0 * fn - Uk[2];
+    if (Ub) __stcs(&Ub[(n + 3) * uz], 2.0 * fn - Uk[0]);
+    if (Ub) __stcs(&Ub[(n + 4) * uz], 2.0 * fn - Uk[1]);
+    if (Ub) __stcs(&Ub[(n + 5) * uz], 2.0 * fn - Uk[2]);
     double d0 = Dt[2], d1 = Dt[1], d2 = Dt[0], d3 = Dt[0], d4 = Dt[1], d5 = Dt[2];
     auto emitD = [&](int j) -> double {
       const double s1 = d2 + d3;
@@ -490,7 +494,7 @@ __device__ __forceinline__ void solve_item(const IT &it, bool active, PA &pa, do
       const double s3 = (s2 + d0) + d5;
       const double df = -((1.0 / 60.0) * (((45.0 * s1) - 9.0 * s2) + s3));
       const double v = ((-1.0 * o1s[j * ss]) * df) * dz1;
-      if (Vb) Vb[j * it.vz()] = v;
+      if (Vb) __stcs(&Vb[j * it.vz()], v);
       return v;
     };
     vtop = emitD(n - 1);
@@ -498,7 +502,7 @@ __device__ __forceinline__ void solve_item(const IT &it, bool active, PA &pa, do
     auto stepD = [&](int k, double uf, double qk, double gk1) {
       const double Dk = uf - qk * Un;
       Un = uf - gk1 * Un;
-      if (Ub) Ub[(3 + k) * uz] = Un;
+      if (Ub) __stcs(&Ub[(3 + k) * uz], Un);
       U3 = U2; U2 = U1; U1 = U0; U0 = Un;
       d5 = d4; d4 = d3; d3 = d2; d2 = d1; d1 = d0; d0 = Dk;
       emitD(k + 3);
@@ -516,9 +520,9 @@ __device__ __forceinline__ void solve_item(const IT &it, bool active, PA &pa, do
       for (int q = 0; q < 8; q++) stepD(k - q, ub[q], qb[q], gb[q]);
     }
     for (; k >= 0; k--) stepD(k, uu[k * ss], qs[k * ss], gam[(k + 1) * ss]);
-    if (Ub) Ub[2 * uz] = 2.0 * U0 - U1;
-    if (Ub) Ub[1 * uz] = 2.0 * U0 - U2;
-    if (Ub) Ub[0] = 2.0 * U0 - U3;
+    if (Ub) __stcs(&Ub[2 * uz], 2.0 * U0 - U1);
+    if (Ub) __stcs(&Ub[1 * uz], 2.0 * U0 - U2);
+    if (Ub) __stcs(&Ub[0], 2.0 * U0 - U3);
     const double D0 = d0, D1 = d1, D2 = d2;
     d5 = d4; d4 = d3; d3 = d2; d2 = d1; d1 = d0; d0 = D0;
     emitD(2);
@@ -530,7 +534,7 @@ __device__ __forceinline__ void solve_item(const IT &it, bool active, PA &pa, do
     auto emitV = [&](int j, double o1j, double w0, double w1, double w2, double w4, double w5, double w6) -> double {
       double df = (1.0 / 60.0) * (((45.0 * (w4 - w2)) - 9.0 * (w5 - w1)) + (w6 - w0));
       double v = ((-1.0 * o1j) * df) * dz1;
-      if (Vb) Vb[j * it.vz()] = v;
+      if (Vb) __stcs(&Vb[j * it.vz()], v);
       return v;
     };
     const int n = nz;
@@ -538,14 +542,14 @@ __device__ __forceinline__ void solve_item(const IT &it, bool active, PA &pa, do
     double u2 = uu[(n - 2) * ss] - gam[(n - 1) * ss] * u1;
     double u3 = uu[(n - 3) * ss] - gam[(n - 2) * ss] * u2;
     double u4 = uu[(n - 4) * ss] - gam[(n - 3) * ss] * u3;
-    if (Ub) Ub[(3 + n - 1) * uz] = u1;
-    if (Ub) Ub[(3 + n - 2) * uz] = u2;
-    if (Ub) Ub[(3 + n - 3) * uz] = u3;
-    if (Ub) Ub[(3 + n - 4) * uz] = u4;
+    if (Ub) __stcs(&Ub[(3 + n - 1) * uz], u1);
+    if (Ub) __stcs(&Ub[(3 + n - 2) * uz], u2);
+    if (Ub) __stcs(&Ub[(3 + n - 3) * uz], u3);
+    if (Ub) __stcs(&Ub[(3 + n - 4) * uz], u4);
     double g1 = 2.0 * u1 - u2, g2 = 2.0 * u1 - u3, g3 = 2.0 * u1 - u4;
-    if (Ub) Ub[(n + 3) * uz] = g1;
-    if (Ub) Ub[(n + 4) * uz] = g2;
-    if (Ub) Ub[(n + 5) * uz] = g3;
+    if (Ub) __stcs(&Ub[(n + 3) * uz], g1);
+    if (Ub) __stcs(&Ub[(n + 4) * uz], g2);
+    if (Ub) __stcs(&Ub[(n + 5) * uz], g3);
     double w0 = u4, w1 = u3, w2 = u2, w3 = u1, w4 = g1, w5 = g2, w6 = g3;
     vtop = emitV(n - 1, o1s[(n - 1) * ss], w0, w1, w2, w4, w5, w6);
     int kk = n - 5;
@@ -561,21 +565,21 @@ __device__ __forceinline__ void solve_item(const IT &it, bool active, PA &pa, do
 #pragma unroll
       for (int q = 0; q < 8; q++) {
         double Uk = ub[q] - gb[q] * w0;
-        if (Ub) Ub[(3 + kk - q) * uz] = Uk;
+        if (Ub) __stcs(&Ub[(3 + kk - q) * uz], Uk);
         w6 = w5; w5 = w4; w4 = w3; w3 = w2; w2 = w1; w1 = w0; w0 = Uk;
         emitV(kk - q + 3, ob[q], w0, w1, w2, w4, w5, w6);
       }
     }
     for (; kk >= 0; kk--) {
       double Uk = uu[kk * ss] - gam[(kk + 1) * ss] * w0;
-      if (Ub) Ub[(3 + kk) * uz] = Uk;
+      if (Ub) __stcs(&Ub[(3 + kk) * uz], Uk);
       w6 = w5; w5 = w4; w4 = w3; w3 = w2; w2 = w1; w1 = w0; w0 = Uk;
       emitV(kk + 3, o1s[(kk + 3) * ss], w0, w1, w2, w4, w5, w6);
     }
     double b1 = 2.0 * w0 - w1, b2 = 2.0 * w0 - w2, b3 = 2.0 * w0 - w3;
-    if (Ub) Ub[2 * uz] = b1;
-    if (Ub) Ub[1 * uz] = b2;
-    if (Ub) Ub[0] = b3;
+    if (Ub) __stcs(&Ub[2 * uz], b1);
+    if (Ub) __stcs(&Ub[1 * uz], b2);
+    if (Ub) __stcs(&Ub[0], b3);
     w6 = w5; w5 = w4; w4 = w3; w3 = w2; w2 = w1; w1 = w0; w0 = b1;
     emitV(2, o1s[2 * ss], w0, w1, w2, w4, w5, w6);
     w6 = w5; w5 = w4; w4 = w3; w3 = w2; w2 = w1; w1 = w0; w0 = b2;
@@ -592,19 +596,19 @@ __device__ __forceinline__ void solve_item(const IT &it, bool active, PA &pa, do
       f[n2 + i] = 2.0 * f[n2] - f[n2 - i];
     }
     if (Ub)
-      for (int m = 0; m < nz + 6; m++) Ub[m * uz] = f[m];
+      for (int m = 0; m < nz + 6; m++) __stcs(&Ub[m * uz], f[m]);
     for (int j = 0; j < nz; j++) {
       int c = n1 + j;
       double df = (1.0 / 60.0) * (((45.0 * (f[c + 1] - f[c - 1])) - 9.0 * (f[c + 2] - f[c - 2])) +
                                   (f[c + 3] - f[c - 3]));
       double v = ((-1.0 * o1s[j * ss]) * df) * dz1;
-      if (Vb) Vb[j * it.vz()] = v;
+      if (Vb) __stcs(&Vb[j * it.vz()], v);
       if (j == 0) vbot = v;
       if (j == nz - 1) vtop = v;
     }
   }
-  if (double *p = it.vtop()) *p = vtop;
-  if (double *p = it.vbot()) *p = vbot;
+  if (double *p = it.vtop()) __stcs(p, vtop);
+  if (double *p = it.vbot()) __stcs(p, vbot);
 }
 
 /* Generic path: warp tasks are 32 consecutive items of the flattened (column, lambda) index. */
