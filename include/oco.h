@@ -149,6 +149,14 @@ int oco_intensities_device(oco_ctx *ctx, const oco_params *p, const double *U, c
 int oco_optical_depth_device(oco_ctx *ctx, const oco_params *p, const double *kappa, const double *rho,
                              double target_tau, double *tau, int32_t *photo_index, void *stream);
 
+/* Wavelength-integrated emergent flux of a block solved on the device: for an emergent-flux
+ * plane V laid out like Vtop / Vbot (ny, nx, nw), F[col] = sum over the context's wavelength
+ * grid of the trapezoid rule in lambda (cm), (ny, nx) values; summed in increasing wavelength
+ * index with weights from oco_set_wavelengths (a single wavelength gives 0).  p->nw must equal
+ * the context's grid.  No reference counterpart (the bolometric flux of each column).
+ * Enqueued on `stream`. */
+int oco_integrated_flux_device(oco_ctx *ctx, const oco_params *p, const double *V, double *F, void *stream);
+
 /* Diagnostic of the failure path: runs the kernels' bounded wait (the mbarrier poll the
  * solve kernels use for their shared-memory copies) on a barrier phase that nothing
  * completes, polling spin_limit times.  Returns OCO_ETIMEDOUT when the wait ran out, as a

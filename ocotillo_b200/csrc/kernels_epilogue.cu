@@ -6,6 +6,12 @@
  *   k_optical_depth   tau(z) = cumulative sum over z from index 1 of kappa rho dz, and the
  *                     first z index where tau reaches a target (tools/ocoutils/ReadOcotillo.py:
  *                     248-293, calculate_optical_depth and find_photosphere), -1 if never.
+ *   k_integrated_flux the wavelength-integrated emergent flux per column, the trapezoid rule
+ *                     over the wavelength grid as a weighted sum (weights in cm) in increasing
+ *                     wavelength index; one thread per column, so a warp reads 32 adjacent
+ *                     columns of a [lambda][column] flux plane (coalesced) and the sum order is
+ *                     fixed.  No reference counterpart (the reference writes per-lambda planes
+ *                     only); the bolometric emergent flux of each column.
  * One thread per item, z loop inside; compiled without FMA contraction so that the products
  * and the running sum round as the reference tools' array arithmetic does.
  */
@@ -65,6 +71,22 @@ __global__ void __launch_bounds__(256) k_optical_depth(const EpilogueArgs a) {
   }
 }
 
+__global__ void __launch_bounds__(256) k_integrated_flux(const double *__restrict__ V, const double *__restrict__ w,
+                                                         int64_t ncol, int nw, int64_t ld_col, double *__restrict__ F) {
+  for (int64_t col = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; col < ncol;
+       col += (int64_t)gridDim.x * blockDim.x) {
+    double f = 0.0;
+    for (int iw = 0; iw < nw; iw++) f = f + __ldg(&w[iw]) * V[(int64_t)iw * ld_col + col];
+    F[col] = f;
+  }
+}
+
+cudaError_t launch_integrated_flux(const double *V, const double *w, int64_t ncol, int nw, int64_t ld_col, double *F,
+                                   int blocks, cudaStream_t s) {
+  k_integrated_flux<<<blocks, 256, 0, s>>>(V, w, ncol, nw, ld_col, F);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_intensities(const EpilogueArgs &a, int blocks, cudaStream_t s) {
   k_intensities<<<blocks, 256, 0, s>>>(a);
   return cudaGetLastError();
@@ -81,26 +103,32 @@ namespace oco {
 
 /* Reference-layout output from a lambda-fastest chunk: for each column col of the chunk, the
  * (rows x nw) plane src[z * src_zs + col * nw + iw] goes to dst[(iw * ld_col + c_off + col) *
- * rows + z].  32 x 32 tiles through shared memory, so that the reads run along lambda and the
- * writes along z, both coalesced.  Block (32, 8); grid (ceil(nw/32), ceil(rows/32), <= 65535)
- * with a loop over columns. */
+ * rows + z].  Tiles of 64 z x 32 wavelengths through shared memory, so that the reads run
+ * along lambda and the writes along z (256-byte runs both ways), eight elements per thread in
+ * flight.  Block (32, 8); grid (ceil(nw/32), ceil(rows/64), <= 65535) with a loop over
+ * columns. */
+constexpr int TZ = 64; /* z rows per tile */
 __global__ void __launch_bounds__(256) k_lambda_to_reference(const double *__restrict__ src, int64_t src_zs,
                                                              double *__restrict__ dst, int64_t ld_col,
                                                              int64_t c_off, int64_t nb, int rows, int nw) {
-  __shared__ double tile[32][33];
-  const int w0 = blockIdx.x * 32, z0 = blockIdx.y * 32;
+  __shared__ double tile[TZ][33];
+  const int w0 = blockIdx.x * 32, z0 = blockIdx.y * TZ;
   const int tx = threadIdx.x, ty = threadIdx.y;
   for (int64_t col = blockIdx.z; col < nb; col += gridDim.z) {
+    double v[TZ / 8];
 #pragma unroll
-    for (int i = 0; i < 32; i += 8) {
-      const int z = z0 + ty + i, iw = w0 + tx;
-      if (z < rows && iw < nw) tile[ty + i][tx] = src[(int64_t)z * src_zs + col * nw + iw];
+    for (int i = 0; i < TZ / 8; i++) { /* all loads of the tile first */
+      const int z = z0 + ty + 8 * i, iw = w0 + tx;
+      v[i] = (z < rows && iw < nw) ? src[(int64_t)z * src_zs + col * nw + iw] : 0.0;
     }
+#pragma unroll
+    for (int i = 0; i < TZ / 8; i++) tile[ty + 8 * i][tx] = v[i];
     __syncthreads();
 #pragma unroll
-    for (int i = 0; i < 32; i += 8) {
-      const int iw = w0 + ty + i, z = z0 + tx;
-      if (z < rows && iw < nw) dst[((int64_t)iw * ld_col + c_off + col) * rows + z] = tile[tx][ty + i];
+    for (int j = 0; j < TZ / 8; j++) {
+      const int lw = ty + 8 * (j >> 1), zz = tx + 32 * (j & 1);
+      const int iw = w0 + lw, z = z0 + zz;
+      if (z < rows && iw < nw) dst[((int64_t)iw * ld_col + c_off + col) * rows + z] = tile[zz][lw];
     }
     __syncthreads();
   }
@@ -109,7 +137,7 @@ __global__ void __launch_bounds__(256) k_lambda_to_reference(const double *__res
 cudaError_t launch_lambda_to_reference(const double *src, int64_t src_zs, double *dst, int64_t ld_col, int64_t c_off,
                                        int64_t nb, int rows, int nw, cudaStream_t s) {
   if (nb <= 0) return cudaSuccess;
-  const dim3 grid((unsigned)((nw + 31) / 32), (unsigned)((rows + 31) / 32), (unsigned)(nb < 65535 ? nb : 65535));
+  const dim3 grid((unsigned)((nw + 31) / 32), (unsigned)((rows + TZ - 1) / TZ), (unsigned)(nb < 65535 ? nb : 65535));
   k_lambda_to_reference<<<grid, dim3(32, 8), 0, s>>>(src, src_zs, dst, ld_col, c_off, nb, rows, nw);
   return cudaGetLastError();
 }

@@ -87,6 +87,7 @@ extern "C" void oco_destroy(oco_ctx *c) {
   if (c->copy) cudaStreamSynchronize(c->copy);
   c->lam.release();
   c->lam32.release();
+  c->trapw.release();
   c->pil.release();
   c->scratch.release();
   c->tmpU.release();
@@ -237,6 +238,16 @@ extern "C" int oco_set_wavelengths(oco_ctx *c, const double *wa, int32_t nw) {
   CU(cudaMemcpy(c->lam.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
   CU(c->lam32.ensure(tab32.size() * sizeof(float)));
   CU(cudaMemcpy(c->lam32.p, tab32.data(), tab32.size() * sizeof(float), cudaMemcpyHostToDevice));
+  /* trapezoid weights over the grid as given (cm): w_i = (wa_{i+1} - wa_{i-1}) / 2, halved
+   * differences at the ends; a single wavelength integrates to 0 */
+  std::vector<double> tw((size_t)nw, 0.0);
+  for (int i = 0; i + 1 < nw; i++) {
+    const double h = 0.5 * ((wa[i + 1] - wa[i]) * 1e-8);
+    tw[(size_t)i] += h;
+    tw[(size_t)i + 1] += h;
+  }
+  CU(c->trapw.ensure(tw.size() * sizeof(double)));
+  CU(cudaMemcpy(c->trapw.p, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice));
   c->wa.assign(wa, wa + nw);
   c->nw = nw;
   return OCO_OK;
@@ -674,6 +685,20 @@ extern "C" int oco_optical_depth_device(oco_ctx *c, const oco_params *p, const d
   a.target = target_tau;
   CU(cudaSetDevice(c->device));
   CU(launch_optical_depth(a, epilogue_blocks(c, a.ncol * a.nw), (cudaStream_t)stream));
+  c->launches++;
+  return OCO_OK;
+}
+
+extern "C" int oco_integrated_flux_device(oco_ctx *c, const oco_params *p, const double *V, double *F, void *stream) {
+  if (!c) return oco_set_err(nullptr, OCO_EINVAL, "NULL context");
+  if (!p || p->nx < 1 || p->ny < 1 || p->nw < 1) return oco_set_err(c, OCO_EINVAL, "bad block dimensions");
+  if (p->nw != c->nw)
+    return oco_set_err(c, OCO_EINVAL, "nw = %d but the context's wavelength grid has %d", p->nw, c->nw);
+  if (!V || !F) return oco_set_err(c, OCO_EINVAL, "V and F are required");
+  const int64_t ncol = (int64_t)p->nx * p->ny;
+  CU(cudaSetDevice(c->device));
+  CU(launch_integrated_flux(V, c->trapw.as<double>(), ncol, p->nw, ncol, F, epilogue_blocks(c, ncol),
+                            (cudaStream_t)stream));
   c->launches++;
   return OCO_OK;
 }

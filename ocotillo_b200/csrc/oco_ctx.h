@@ -54,6 +54,7 @@ struct oco_ctx {
   int nw = 0;
   std::vector<double> wa;
   DevBuf lam, lam32;
+  DevBuf trapw; /* trapezoid weights of the wavelength grid, cm (oco_integrated_flux_device) */
   /* workspace */
   DevBuf pil, scratch, work, status;
   Stage stage[2];

@@ -193,6 +193,9 @@ struct EpilogueArgs {
 };
 cudaError_t launch_intensities(const EpilogueArgs &a, int blocks, cudaStream_t s);
 cudaError_t launch_optical_depth(const EpilogueArgs &a, int blocks, cudaStream_t s);
+/* F[col] = sum_iw w[iw] * V[iw * ld_col + col] for col < ncol, iw in increasing order. */
+cudaError_t launch_integrated_flux(const double *V, const double *w, int64_t ncol, int nw, int64_t ld_col, double *F,
+                                   int blocks, cudaStream_t s);
 /* Copies a lambda-fastest chunk plane set (src[z * src_zs + col * nw + iw], rows z values)
  * into reference-layout arrays (dst[(iw * ld_col + c_off + col) * rows + z]). */
 cudaError_t launch_lambda_to_reference(const double *src, int64_t src_zs, double *dst, int64_t ld_col, int64_t c_off,

@@ -115,6 +115,7 @@ def load_library(path=None):
         "oco_synchronize": (I, [V]),
         "oco_kernel_launches": (ctypes.c_int64, [V]),
         "oco_check_bounded_wait": (I, [V, ctypes.c_int64]),
+        "oco_integrated_flux_device": (I, [V, P, V, V, V]),
         "oco_intensities_device": (I, [V, P, V, V, V, V, V]),
         "oco_optical_depth_device": (I, [V, P, V, V, D, V, V, V]),
         "oco_set_profiling": (I, [V, I]),
@@ -347,6 +348,23 @@ class Engine:
         p = lambda t: ctypes.c_void_p(t.data_ptr()) if t is not None else None
         self._check(self.lib.oco_optical_depth_device(self.ctx, ctypes.byref(prm), p(kappa), p(rho), float(target_tau),
                                                       p(tau), p(photo), ctypes.c_void_p(stream.cuda_stream)))
+
+    def integrated_flux_device(self, V, shape, out=None, stream=None):
+        """Wavelength-integrated emergent flux (trapezoid rule over the context's wavelength
+        grid, lambda in cm) of an emergent-flux plane V (nw, nx, ny) on the device, as a
+        (nx, ny) float64 tensor."""
+        import torch
+        if stream is None:
+            stream = torch.cuda.current_stream(V.device)
+        nx, ny = shape[0], shape[1]
+        nw = V.numel() // (nx * ny)
+        if out is None:
+            out = torch.empty((nx, ny), dtype=torch.float64, device=V.device)
+        prm = self.params((nx, ny, 2), nw, 1.0)
+        self._check(self.lib.oco_integrated_flux_device(self.ctx, ctypes.byref(prm), ctypes.c_void_p(V.data_ptr()),
+                                                        ctypes.c_void_p(out.data_ptr()),
+                                                        ctypes.c_void_p(stream.cuda_stream)))
+        return out
 
     def check_bounded_wait(self, spin_limit=100):
         """Return code of the bounded-wait diagnostic (OCO_ETIMEDOUT = -6 expected)."""

@@ -44,3 +44,34 @@ def test_intensities_and_optical_depth(layout):
     ref_photo = np.where(reached.any(axis=2), reached.argmax(axis=2), -1)
     assert np.array_equal(photo.cpu().numpy().reshape(nw, ncol), ref_photo)
     e.close()
+
+
+def test_integrated_flux():
+    """Wavelength-integrated emergent flux: the trapezoid rule over the wavelength grid (cm) of
+    the Vtop plane, against numpy's trapezoid on the same plane (summation orders differ, so
+    1e-13 relative)."""
+    import torch
+    from ocotillo_b200 import Engine, OcoError, workloads
+    e = Engine(0)
+    rho, T, dz = workloads.agn_block(5, 7, 64, seed=18)
+    wa = workloads.log_wavelengths(97)
+    e.set_wavelengths(wa)
+    nx, ny, nz = rho.shape
+    dev = torch.device("cuda:0")
+    vt = torch.empty((len(wa), nx, ny), dtype=torch.float64, device=dev)
+    r, t = torch.from_numpy(rho).to(dev), torch.from_numpy(T).to(dev)
+    e.solve_block_device(r, t, dz, {"Vtop": vt}, form="mixed", layout=0)
+    F = e.integrated_flux_device(vt, (nx, ny))
+    e.synchronize()
+    v = vt.cpu().numpy()
+    ref = np.trapezoid(v, x=wa * 1e-8, axis=0)
+    got = F.cpu().numpy()
+    assert got.shape == (nx, ny)
+    assert np.all(np.abs(got - ref) <= 1e-13 * np.abs(v).sum(axis=0) * (wa[-1] - wa[0]) * 1e-8)
+    with pytest.raises(OcoError):  # plane of another grid size
+        e.integrated_flux_device(vt[:10], (nx, ny))
+    e.set_wavelengths(wa[:1])
+    one = e.integrated_flux_device(vt[:1].contiguous(), (nx, ny))
+    e.synchronize()
+    assert np.array_equal(one.cpu().numpy(), np.zeros((nx, ny)))
+    e.close()
