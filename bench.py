@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=1.5, help="job arrivals per second")
     ap.add_argument("--batch-cols", type=int, default=8192)
     ap.add_argument("--no-c3", action="store_true", help="skip the precision-config (c3) measurement")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving (c5) measurement")
     return ap.parse_args()
 
 
@@ -629,6 +630,7 @@ def main():
         torch.cuda.empty_cache()
         extra["batch"] = measure_batch(a, eng, dev)
         torch.cuda.empty_cache()
+    if world == 1 and not a.no_extra and not a.no_serve:
         specs = workloads.serving_stream(a.serve_jobs, a.serve_rate, seed=5)
         arrays = [workloads.job_arrays_device(sp, dev) for sp in specs]
         torch.cuda.synchronize(dev)
@@ -641,8 +643,8 @@ def main():
             extra["serving"][form] = measure_serving(a, dev, form, specs, arrays)
         del arrays
         torch.cuda.empty_cache()
-        if not a.no_c3:
-            extra["precision_c3"] = measure_precision_c3(a, eng, dev)
+    if world == 1 and not a.no_extra and not a.no_c3:
+        extra["precision_c3"] = measure_precision_c3(a, eng, dev)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
