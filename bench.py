@@ -290,7 +290,7 @@ class Grid:
         by nw wavelengths).  Algorithmic flops per point: the reference's census, 97 (90
         add/mul + 7 divisions; transcendentals not counted)."""
         nz, nw = self.nz, self.nw
-        rec = 26 * 8.0 if form != "mixed" else 52 * 4.0
+        rec = 26 * 8.0 if form != "mixed" else 64 * 4.0
         bytes_pt = 8.0 * (self.mz / nz) + 16.0 + rec / nw
         launch_ms = m["solve_ms"] / max(m["nsolve"], 1)
         pts_launch = m["pts_step"] * steps / max(m["nsolve"], 1)

@@ -21,7 +21,7 @@
 namespace oco {
 using namespace oco::mx;
 
-constexpr int MZC = 24;            /* z records per staged chunk (24 x 208 B) */
+constexpr int MZC = 20;            /* z records per staged chunk (20 x 256 B) */
 constexpr int MWARPS = 4;          /* warps per 128-thread block */
 constexpr long long kMSpinLimit = 1ll << 26;
 #ifndef OCO_MIXED_PREFETCH

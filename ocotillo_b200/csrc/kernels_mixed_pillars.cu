@@ -3,7 +3,7 @@
  *
  *   k_pillars_mixed        one thread per (column, z): Saha ionization and the z-only factors
  *                          in FP64, written as the FP32 log2 record of mixed_core.h (MixedZ,
- *                          208 B; large logarithms as integer + fraction).
+ *                          256 B; large logarithms as integer + fraction).
  *   k_pillars_mixed_batch  the same for the columns of a ragged batch.
  *
  * Compiled with -fmad=false like the FP64 kernels: the Saha quadratic

@@ -58,8 +58,7 @@ namespace mx {
  * exponent needs it to ~1e-12). */
 enum MixedZ {
   MZ_TH = 0,        /* theta = 5040/T */
-  MZ_R,             /* 15 ratios E_n/E_n0 for n0 = 1..5, n = n0+1..6 (linear) */
-  MZ_PU = MZ_R + 15, /* log2(ionf * Unsold integral) [2] */
+  MZ_PU,            /* log2(ionf * Unsold integral) [2] */
   MZ_PE = MZ_PU + 2, /* log2(ionf * exp(-chi_n/kT)), n = 1..6 [2 each] */
   MZ_LHM = MZ_PE + 12, /* log2(hm_bf_factor * ionf) [2] */
   MZ_LAFF = MZ_LHM + 2, /* log2(ionf ne k T) [2] */
@@ -75,17 +74,23 @@ enum MixedZ {
   MZ_T1,            /* 1/T */
   MZ_DFT1,          /* damping_factor_const / T, high part */
   MZ_DFT1L,         /* low part */
-  MZ_END,
-  MZN = 52          /* 208 B (padded to 16 B) */
+  MZ_R,             /* level ratios E_n/E_n0 by first level n0 = 1..6: row n0 at MZ_R + rrow(n0)
+                       holds 1, E_{n0+1}/E_n0, ..., E_6/E_n0 (linear); 21 values + 5 zeros, so
+                       that six consecutive values can be read from any row */
+  MZ_END = MZ_R + 26,
+  MZN = 64          /* 256 B */
 };
+/* start of row n0 (1..6) of the level-ratio table: sum over m < n0 of (7 - m) */
+MX_HD int rrow(int n0) { return (n0 - 1) * 7 - ((n0 - 1) * n0) / 2; }
 static_assert(MZ_END <= MZN && MZN % 4 == 0, "mixed record layout");
 
 /* Per-wavelength FP32 record (device layout [field][nw]); [2] as in MixedZ. */
 enum MixedL {
   ML_CL2 = 0,  /* chi * log2(10) */
   ML_LAW,      /* log2(AHbf * wa^3) [2] */
-  ML_G1 = ML_LAW + 2, /* g(lambda,n) * n^-3, n = 1..6 */
-  ML_N0 = ML_G1 + 6,  /* first level with g > 0 (1..6), 7 if none */
+  ML_GS = ML_LAW + 2, /* g(lambda,n) n^-3 from the first level n0 with g > 0: n = n0..6, then 0 [6] */
+  ML_ROFF = ML_GS + 6, /* MixedZ offset of row n0 of the level-ratio table (MZ_R + rrow(n0)) */
+  ML_PEOFF,    /* MixedZ offset of log2(ionf E_n0) (MZ_PE + 2 (n0 - 1)); MZ_PU when no level has g > 0 */
   ML_LS,       /* log2(s_coeff) if wa < 16000 else -1000 [2] */
   ML_FC = ML_LS + 2, /* (f1 - 26) log2(10) [2] */
   ML_F2 = ML_FC + 2, /* f2 log2(10) */
@@ -184,9 +189,11 @@ MX_HD void pillar(double r, double t, double fully_ionized_T, float *o) {
   }
   const double lionf = ionf > 0.0 ? oco_log(ionf) * kLog2e : (double)kNeg;
   o[MZ_TH] = (float)(theta);
-  int q = 0;
-  for (int n0 = 1; n0 <= 5; n0++)
-    for (int n = n0 + 1; n <= 6; n++) o[MZ_R + q++] = oco_exp(-((chi[n] - chi[n0]) * ktemp1));
+  for (int n0 = 1; n0 <= 6; n0++) {
+    o[MZ_R + rrow(n0)] = 1.0f;
+    for (int n = n0 + 1; n <= 6; n++) o[MZ_R + rrow(n0) + (n - n0)] = oco_exp(-((chi[n] - chi[n0]) * ktemp1));
+  }
+  for (int k2 = MZ_R + 21; k2 < MZ_END; k2++) o[k2] = 0.0f;
   /* Unsold: 0.5 kT/Ry (exp(-chi_6/kT) - exp(-Ry/kT)) = 0.5 kT/Ry e^{-chi_6/kT} (1 - e^{-(Ry-chi_6)/kT}) */
   double lu = oco_log((0.5 * (k_cgs * t)) * RydbergEnergy1) - chi[6] * ktemp1 +
               oco_log(1.0 - oco_exp(-((RydbergEnergy - chi[6]) * ktemp1)));
@@ -226,11 +233,11 @@ MX_HD void lambda_record(const LamIn &L, float *o) {
   o[ML_CL2] = (float)(L.chi * kLog2_10);
   put_l2(oco_log(AHbf * L.wa3) * kLog2e, o + ML_LAW);
   int n0 = 7;
-  for (int n = 6; n >= 1; n--) {
-    o[ML_G1 + n - 1] = (float)L.gn[n - 1];
+  for (int n = 6; n >= 1; n--)
     if (L.gn[n - 1] > 0.0) n0 = n;
-  }
-  o[ML_N0] = (float)n0;
+  for (int t = 0; t < 6; t++) o[ML_GS + t] = (n0 + t <= 6) ? (float)L.gn[n0 + t - 1] : 0.0f;
+  o[ML_ROFF] = (float)(MZ_R + (n0 <= 6 ? rrow(n0) : 0));
+  o[ML_PEOFF] = (float)(n0 <= 6 ? MZ_PE + 2 * (n0 - 1) : MZ_PU);
   put_l2((L.hmon != 0.0 && L.s > 0.0) ? oco_log(L.s) * kLog2e : (double)kNeg, o + ML_LS);
   put_l2((L.f1 - 26.0) * kLog2_10, o + ML_FC);
   o[ML_F2] = (float)(L.f2 * kLog2_10);
@@ -251,10 +258,10 @@ MX_HD void lambda_record(const LamIn &L, float *o) {
 /* Wavelength constants held in registers by the solve; *i members are the integer parts of
  * the large logarithms (value = member + member_i). */
 struct Lam32 {
-  float cl2, law, lawi, g[6], ls, lsi_, fc, fci, f2, f3, lal0w, lal0wi, gff, chi1, lnnu9, hnuk, l3nu, l3nui;
+  float cl2, law, lawi, gs[6], ls, lsi_, fc, fci, f2, f3, lal0w, lal0wi, gff, chi1, lnnu9, hnuk, l3nu, l3nui;
   float ch, cl;   /* log2(e)/lambda_cm = ch + cl */
   float lsi, lsf; /* log2(2 h c^2 lambda_cm^-5) = lsi + lsf, lsi an integer */
-  int n0;
+  int roff, peoff; /* MixedZ offsets of the level-ratio row and of log2(ionf E_n0) */
 };
 /* Lam32 from a record laid out as MixedL (field f at t[f * stride]). */
 template <class Get>
@@ -262,8 +269,9 @@ MX_HD void lam32_from(Lam32 &L, Get t) {
   L.cl2 = t(ML_CL2);
   L.law = t(ML_LAW);
   L.lawi = t(ML_LAW + 1);
-  for (int q = 0; q < 6; q++) L.g[q] = t(ML_G1 + q);
-  L.n0 = (int)t(ML_N0);
+  for (int q = 0; q < 6; q++) L.gs[q] = t(ML_GS + q);
+  L.roff = (int)t(ML_ROFF);
+  L.peoff = (int)t(ML_PEOFF);
   L.ls = t(ML_LS);
   L.lsi_ = t(ML_LS + 1);
   L.fc = t(ML_FC);
@@ -335,24 +343,15 @@ MX_HD Opac32 opacity(const Rec &Z, const Lam32 &L) {
   /* stim = 1 - 10^(-chi theta) (c_o :171) */
   const float t10 = L.cl2 * Z[MZ_TH];
   const float ls = (t10 > 40.0f) ? 0.0f : log2_one_minus_exp2neg(t10);
-  /* H bound-free (c_o :233-244): AHbf wa^3 stim ionf (Unsold + E_n0 sm) */
+  /* H bound-free (c_o :233-244): AHbf wa^3 stim ionf (Unsold + E_n0 sm), sm = sum over
+   * t = 0..5 of g_{n0+t} E_{n0+t}/E_n0: six FMAs down row n0 of the ratio table (levels below
+   * n0 have g = 0 and drop out; past level 6 the weights are 0) */
   float ai = Z[MZ_PU + 1], af = Z[MZ_PU];
-  const int n0 = L.n0;
-  if (n0 <= 6) {
-    float sm = L.g[0];
+  float sm = 0.0f;
 #pragma unroll
-    for (int n = 2; n <= 6; n++) sm = (n == n0) ? L.g[n - 1] : sm; /* L.g[n0-1] without local memory */
-    int q = 0;
-    const int off = (n0 == 1) ? 0 : (n0 == 2) ? 5 : (n0 == 3) ? 9 : (n0 == 4) ? 12 : 14;
-#pragma unroll
-    for (int n = 2; n <= 6; n++) {
-      if (n > n0) {
-        sm += L.g[n - 1] * Z[MZ_R + off + q];
-        q++;
-      }
-    }
-    const int pe = MZ_PE + 2 * (n0 - 1);
-    const float ef = Z[pe], ei = Z[pe + 1];
+  for (int t = 0; t < 6; t++) sm = fmaf(L.gs[t], Z[L.roff + t], sm);
+  {
+    const float ef = Z[L.peoff], ei = Z[L.peoff + 1]; /* log2(ionf E_n0); = MZ_PU (d = 0) if no level */
     /* log2(Unsold) - log2(E_n0), both times ionf; the larger one sets the scale */
     const float d = (ai - ei) + (af - ef);
     const bool ug = d >= 0.0f;

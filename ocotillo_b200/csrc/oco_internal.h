@@ -216,8 +216,8 @@ int solve_fp64_max_blocks_per_sm(int form, int grey, int threads);
 cudaError_t launch_bounded_wait_check(long long limit, unsigned long long *status, cudaStream_t s);
 
 /* Mixed-precision kernels (kernels_mixed.cu). */
-constexpr int MIXED_ZN = 52; /* floats per mixed record */
-constexpr int MIXED_LN = 28; /* fields of the mixed wavelength table */
+constexpr int MIXED_ZN = 64; /* floats per mixed record */
+constexpr int MIXED_LN = 29; /* fields of the mixed wavelength table */
 cudaError_t launch_pillars_mixed(const double *rho, const double *T, int64_t ncol, int nz, double fully_ionized_T,
                                  float *rec, cudaStream_t s);
 cudaError_t launch_solve_mixed(const MixedArgs &a, int blocks, int threads, cudaStream_t s);
