@@ -366,6 +366,28 @@ def flux_error(g, form_a, form_b, eps=1e-7, seed=7):
                                 "equivalent_rho_perturbation_max": backward.max().item() if backward.numel() else None}}
 
 
+def intensity_error(g, form_a="mixed", form_b="stable"):
+    """Relative difference of the mean intensity U (every z, ghost zones included, every item)
+    of form_a against form_b on a grid that fits one chunk (its fields stay on the device)."""
+    import torch
+    assert g.nchunk == 1
+
+    def field(form):
+        g.step(form, fields=True)
+        g.sync()
+        return g.sets[0]["U"].clone()
+
+    ub, ua = field(form_b), field(form_a)
+    ok = torch.isfinite(ub) & (ub != 0)
+    rel = ((ua - ub).abs() / ub.abs())[ok]
+    sub = rel.float()[torch.randperm(rel.numel(), device=rel.device)[:1 << 24]]
+    res = {"reference_form": form_b, "values": int(rel.numel()), "p50": torch.quantile(sub, 0.5).item(),
+           "p99": torch.quantile(sub, 0.99).item(), "max": rel.max().item(),
+           "frac_above_1e-4": (rel > 1e-4).double().mean().item()}
+    del ub, ua, rel, sub
+    return res
+
+
 def flux_error_vs_plain(g, agree=1e-8):
     """Mixed emergent flux against the reference-form (plain) FP64 flux where that flux is
     itself accurate: items whose plain and stable FP64 fluxes agree to `agree` relative.  (In
@@ -488,7 +510,8 @@ def measure_precision_c3(a, eng, dev):
            "mixed_ms_per_step": mm["total_ms"] / steps, "plain_ms_per_step": mp["total_ms"] / steps,
            "error_sample": "32x32 columns of the same construction, all z and lambda",
            "emergent_flux_rel_err": flux_error(gs, "mixed", "stable"),
-           "emergent_flux_rel_err_vs_plain": flux_error_vs_plain(gs)}
+           "emergent_flux_rel_err_vs_plain": flux_error_vs_plain(gs),
+           "mean_intensity_rel_err": intensity_error(gs)}
     del gs
     torch.cuda.empty_cache()
     return res
@@ -565,6 +588,15 @@ def main():
                           "emergent_flux_rel_err_vs_plain": flux_error_vs_plain(g),
                           "roofline": g.roofline(mixed_m, a.steps, "mixed")}
         extra["plain_fp64_value"] = plain_v
+        import copy
+        sa = copy.copy(a)
+        sa.nx = sa.ny = 32
+        sa.chunk_cols, sa.layout = 1024, "lambda"
+        gs = Grid(sa, eng, dev, rank)
+        extra["mixed"]["mean_intensity_rel_err"] = dict(
+            intensity_error(gs), sample="32x32 columns of the same construction (seed 2), all z and lambda")
+        del gs
+        torch.cuda.empty_cache()
 
     # ---- e2e: host arrays through oco_solve_block (pinned), one batch of columns per step
     e2e = None
