@@ -158,7 +158,8 @@ __device__ __forceinline__ MItem block_item(const MixedArgs &a, int64_t cl, int 
   return it;
 }
 
-/* One (column, wavelength) item.  Scratch: one float4 per z at s4[z * ss] (see the forward
+/* One (column, wavelength) item.  Scratch: one float4 per z at s4[z * ss], each warp's levels
+ * contiguous (ss = 32), so that a warp reads and writes one sequential stream (see the forward
  * sweep).  An inactive lane runs the forward sweep (to keep a staged warp in step) and writes
  * nothing. */
 template <class PA>
@@ -349,7 +350,7 @@ __global__ void __launch_bounds__(128) k_solve_mixed_staged(const MixedArgs a) {
   const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int ntiles = (a.nw + 31) / 32;
   const unsigned long long ntasks = (unsigned long long)a.ncol * ntiles;
-  float4 *s4 = a.s4 + slot * 32 + lane;
+  float4 *s4 = a.s4 + slot * 32 * (int64_t)a.nz + lane; /* the warp's scratch: [z][lane], contiguous */
   MStaged pa;
   pa.buf = s_rec[wib];
   pa.bar0 = msmem(&s_bar[wib][0]);
@@ -374,7 +375,7 @@ __global__ void __launch_bounds__(128) k_solve_mixed_staged(const MixedArgs a) {
     const bool active = iw_raw < a.nw;
     const int iw = active ? iw_raw : a.nw - 1;
     pa.begin(a.rec + cl * (int64_t)a.nz * MZN);
-    msolve_item(block_item(a, cl, iw), active, pa, s4, a.slot_stride);
+    msolve_item(block_item(a, cl, iw), active, pa, s4, 32);
     if (__any_sync(0xffffffffu, pa.failed)) {
       if (lane == 0) atomicOr(&a.status[2], 1ull);
       pa.wait(0);
@@ -389,7 +390,7 @@ __global__ void __launch_bounds__(128) k_solve_mixed(const MixedArgs a) {
   const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nitems = a.ncol * a.nw;
   const unsigned long long ntasks = (unsigned long long)((nitems + 31) / 32);
-  float4 *s4 = a.s4 + slot * 32 + lane;
+  float4 *s4 = a.s4 + slot * 32 * (int64_t)a.nz + lane; /* the warp's scratch: [z][lane], contiguous */
   for (;;) {
     unsigned long long task = 0;
     if (lane == 0) task = atomicAdd(a.work, 1ull);
@@ -400,7 +401,7 @@ __global__ void __launch_bounds__(128) k_solve_mixed(const MixedArgs a) {
       const int64_t cl = item / a.nw;
       const int iw = (int)(item - cl * a.nw);
       MDirect pa{a.rec + cl * (int64_t)a.nz * MZN};
-      msolve_item(block_item(a, cl, iw), true, pa, s4, a.slot_stride);
+      msolve_item(block_item(a, cl, iw), true, pa, s4, 32);
     }
   }
 }
@@ -460,7 +461,7 @@ __global__ void __launch_bounds__(128) k_batch_mixed_staged(const MixedBatchArgs
   __shared__ __align__(8) unsigned long long s_bar[MWARPS][2];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  float4 *s4 = b.s4 + slot * 32 + lane;
+  float4 *s4 = b.s4 + slot * 32 * (int64_t)b.max_nz + lane; /* the warp's scratch: [z][lane], contiguous */
   MStaged pa;
   pa.buf = s_rec[wib];
   pa.bar0 = msmem(&s_bar[wib][0]);
@@ -485,7 +486,7 @@ __global__ void __launch_bounds__(128) k_batch_mixed_staged(const MixedBatchArgs
     const int iw = active ? iw_raw : c.nw - 1;
     pa.nz = c.nz;
     pa.begin(b.rec + c.rec_off * MZN);
-    msolve_item(batch_item(b, c, iw), active, pa, s4, b.slot_stride);
+    msolve_item(batch_item(b, c, iw), active, pa, s4, 32);
     if (__any_sync(0xffffffffu, pa.failed)) {
       if (lane == 0) atomicOr(&b.status[2], 1ull);
       pa.wait(0);
@@ -501,7 +502,7 @@ __global__ void __launch_bounds__(128) k_batch_mixed_staged(const MixedBatchArgs
 __global__ void __launch_bounds__(128) k_batch_mixed_packed(const MixedBatchArgs b) {
   const int lane = threadIdx.x & 31;
   const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  float4 *s4 = b.s4 + slot * 32 + lane;
+  float4 *s4 = b.s4 + slot * 32 * (int64_t)b.max_nz + lane; /* the warp's scratch: [z][lane], contiguous */
   for (;;) {
     unsigned long long task = 0;
     if (lane == 0) task = atomicAdd(b.work, 1ull);
@@ -520,7 +521,7 @@ __global__ void __launch_bounds__(128) k_batch_mixed_packed(const MixedBatchArgs
       const MBatchCol c = b.cols[__ldg(b.order + lo)];
       const int iw = (int)(item - __ldg(b.item_pre + lo));
       MDirect pa{b.rec + c.rec_off * MZN};
-      msolve_item(batch_item(b, c, iw), true, pa, s4, b.slot_stride);
+      msolve_item(batch_item(b, c, iw), true, pa, s4, 32);
     }
   }
 }

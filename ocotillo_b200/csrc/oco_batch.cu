@@ -80,6 +80,7 @@ static MixedBatchArgs batch_args(const oco_batch *b) {
   a.layout = b->layout;
   a.s4 = b->scratch.as<float4>();
   a.slot_stride = b->slots;
+  a.max_nz = b->max_nz;
   a.work = b->work.as<unsigned long long>();
   a.status = b->status.as<unsigned long long>();
   return a;

@@ -112,7 +112,7 @@ struct MixedArgs {
   double *Vtop, *Vbot;
   int64_t ld_col, c_off;
   int layout;
-  float4 *s4; /* scratch [nz][slots]: |gamma| or q, 1/kappa, u mantissa, u exponent (int bits) */
+  float4 *s4; /* scratch [warp slot][nz][32]: |gamma| or q, 1/kappa, u mantissa, u exponent (int bits) */
   int64_t slot_stride;
   unsigned long long *work;
   unsigned long long *status;
@@ -144,8 +144,9 @@ struct MixedBatchArgs {
   int64_t ncol, ntasks, nitems;
   double *U, *K, *V, *Vtop, *Vbot;
   int layout;
-  float4 *s4;
+  float4 *s4;        /* scratch [warp slot][max_nz][32] */
   int64_t slot_stride;
+  int max_nz;
   unsigned long long *work;
   unsigned long long *status;
 };
