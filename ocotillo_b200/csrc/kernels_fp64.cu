@@ -371,7 +371,7 @@ struct BlockItem {
   __device__ __forceinline__ int64_t vz() const { return a.V_zs; }
   __device__ __forceinline__ double *vtop() const { return a.Vtop ? a.Vtop + pidx() : nullptr; }
   __device__ __forceinline__ double *vbot() const { return a.Vbot ? a.Vbot + pidx() : nullptr; }
-  __device__ __forceinline__ int64_t ss() const { return a.slot_stride; }
+  __device__ __forceinline__ int64_t ss() const { return 32; }
   __device__ __forceinline__ unsigned long long *status() const { return a.status; }
   __device__ __forceinline__ unsigned long long id() const {
     return (unsigned long long)((a.c_off + cl) * a.nw + w);
@@ -618,10 +618,11 @@ __global__ void __launch_bounds__(128) k_solve(const SolveArgs a) {
   const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nitems = a.ncol * a.nw;
   const unsigned long long ntasks = (unsigned long long)((nitems + 31) / 32);
-  double *gam = a.gam + slot * 32 + lane;
-  double *uu = a.uu + slot * 32 + lane;
-  double *o1 = a.o1 + slot * 32 + lane;
-  double *qs = a.q + slot * 32 + lane;
+  const int64_t wbase = slot * 32 * (int64_t)a.nz + lane; /* each warp's scratch [z][lane], contiguous */
+  double *gam = a.gam + wbase;
+  double *uu = a.uu + wbase;
+  double *o1 = a.o1 + wbase;
+  double *qs = a.q + wbase;
   for (;;) {
     unsigned long long task = 0;
     if (lane == 0) task = atomicAdd(a.work, 1ull);
@@ -647,10 +648,11 @@ __global__ void __launch_bounds__(128, 4) k_solve_staged(const SolveArgs a) {
   const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int ntiles = (a.nw + 31) / 32;
   const unsigned long long ntasks = (unsigned long long)a.ncol * ntiles;
-  double *gam = a.gam + slot * 32 + lane;
-  double *uu = a.uu + slot * 32 + lane;
-  double *o1 = a.o1 + slot * 32 + lane;
-  double *qs = a.q + slot * 32 + lane;
+  const int64_t wbase = slot * 32 * (int64_t)a.nz + lane; /* each warp's scratch [z][lane], contiguous */
+  double *gam = a.gam + wbase;
+  double *uu = a.uu + wbase;
+  double *o1 = a.o1 + wbase;
+  double *qs = a.q + wbase;
   StagedPillars pa;
   pa.buf = s_pil[wib];
   pa.bar0 = smem_addr(&s_bar[wib][0]);
@@ -712,7 +714,7 @@ struct BatchItem {
   __device__ __forceinline__ int64_t vz() const { return uz(); }
   __device__ __forceinline__ double *vtop() const { return b.Vtop ? b.Vtop + __ldg(&c->flux_off) + w : nullptr; }
   __device__ __forceinline__ double *vbot() const { return b.Vbot ? b.Vbot + __ldg(&c->flux_off) + w : nullptr; }
-  __device__ __forceinline__ int64_t ss() const { return b.slot_stride; }
+  __device__ __forceinline__ int64_t ss() const { return 32; }
   __device__ __forceinline__ unsigned long long *status() const { return b.status; }
   __device__ __forceinline__ unsigned long long id() const { return ((unsigned long long)col << 32) | (unsigned)w; }
 };
@@ -725,10 +727,11 @@ __global__ void __launch_bounds__(128, 4) k_batch_fp64_staged(const FP64BatchArg
   __shared__ __align__(8) unsigned long long s_bar[WARPS_PER_BLOCK][2];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  double *gam = b.gam + slot * 32 + lane;
-  double *uu = b.uu + slot * 32 + lane;
-  double *o1 = b.o1 + slot * 32 + lane;
-  double *qs = b.q + slot * 32 + lane;
+  const int64_t wbase = slot * 32 * (int64_t)b.max_nz + lane; /* each warp's scratch [z][lane], contiguous */
+  double *gam = b.gam + wbase;
+  double *uu = b.uu + wbase;
+  double *o1 = b.o1 + wbase;
+  double *qs = b.q + wbase;
   StagedPillars pa;
   pa.buf = s_pil[wib];
   pa.bar0 = smem_addr(&s_bar[wib][0]);

@@ -106,6 +106,7 @@ static FP64BatchArgs fp64_args(const oco_batch *b) {
   a.o1 = sc + 2 * plane;
   a.q = sc + 3 * plane;
   a.slot_stride = b->slots;
+  a.max_nz = b->max_nz;
   a.work = b->work.as<unsigned long long>();
   a.status = b->status.as<unsigned long long>();
   return a;

@@ -87,8 +87,8 @@ struct SolveArgs {
   double *Vtop, *Vbot; /* [iw*ld_col + c_off + cl] */
   int64_t ld_col, c_off;
   int layout;
-  /* Scratch [nz][nslot*32]: forward-sweep gamma, u, 1/kappa and (stable form) q of each
-   * warp slot. */
+  /* Scratch [warp slot][nz][32] each (slot_stride*nz values): forward-sweep gamma, u,
+   * 1/kappa and (stable form) q, one contiguous block per warp. */
   double *gam, *uu, *o1, *q;
   int64_t slot_stride; /* = nslot*32 */
   unsigned long long *work;   /* persistent-kernel work counter (warp tasks) */
@@ -160,8 +160,9 @@ struct FP64BatchArgs {
   int64_t ntasks;
   double *U, *K, *V, *Vtop, *Vbot;
   int layout;
-  double *gam, *uu, *o1, *q; /* scratch [max_nz][slots] each */
+  double *gam, *uu, *o1, *q; /* scratch [warp slot][max_nz][32] each */
   int64_t slot_stride;
+  int max_nz;
   unsigned long long *work;
   unsigned long long *status; /* [0] zero pivots, [1] first (column << 32 | wavelength), [2] timeout */
 };
