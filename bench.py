@@ -317,7 +317,7 @@ PUBLISHED_POINTS_PER_S = 1e6 / 0.14415
 # kernel, from one ncu --set full capture of a 1024-column launch of this grid (outputs 3.2 GB,
 # larger than L2), scaled to a launch by its points: profiles/k_solve_staged_plain_agn_32x32x512x256.txt
 # and profiles/k_solve_mixed_staged_agn_32x32x512x256.txt.
-TRAFFIC_BYTES_PER_POINT = {"plain": 71.8, "mixed": 56.9}
+TRAFFIC_BYTES_PER_POINT = {"plain": 72.2, "mixed": 56.8}
 
 
 def flux_error(g, form_a, form_b, eps=1e-7, seed=7):
