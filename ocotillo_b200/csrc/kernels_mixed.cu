@@ -31,8 +31,6 @@ constexpr long long kMSpinLimit = 1ll << 26;
 #define OCO_MIXED_L2_AHEAD 8 /* reverse-sweep steps between the L2 prefetch and the load of a scratch level */
 #endif
 
-__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
-
 /* Shared-memory record accessor. */
 struct MRec {
   const float *p;
@@ -286,11 +284,14 @@ __device__ __forceinline__ void msolve_item(const MItem &it, bool active, PA &pa
     constexpr int PF = OCO_MIXED_PREFETCH;
     for (; k >= PF - 1; k -= PF) { /* scratch loads of PF steps hoisted off the serial chain */
       float4 w[PF];
-      /* the scratch level OCO_MIXED_L2_AHEAD steps ahead into L2 (it was written a whole
-       * forward sweep ago and has usually left L2) */
-#pragma unroll
-      for (int q = 0; q < PF; q++)
-        if (k - q >= OCO_MIXED_L2_AHEAD) prefetch_l2(s4 + (int64_t)(k - q - OCO_MIXED_L2_AHEAD) * ss);
+      /* the PF scratch levels OCO_MIXED_L2_AHEAD steps ahead into L2, one bulk request from lane
+       * 0 (the warp's levels are contiguous; they were written a whole forward sweep ago and
+       * have usually left L2) */
+      if (k - PF + 1 - OCO_MIXED_L2_AHEAD >= 0 && (threadIdx.x & 31) == 0) /* PF levels, one bulk request */
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(__cvta_generic_to_global(
+                         s4 + (int64_t)(k - PF + 1 - OCO_MIXED_L2_AHEAD) * ss)),
+                     "r"((uint32_t)(PF * 32 * sizeof(float4)))
+                     : "memory");
 #pragma unroll
       for (int q = 0; q < PF; q++) w[q] = s4[(int64_t)(k - q) * ss];
 #pragma unroll
