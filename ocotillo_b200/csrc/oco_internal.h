@@ -90,7 +90,7 @@ struct SolveArgs {
   /* Scratch [warp slot][nz][32] each (slot_stride*nz values): forward-sweep gamma, u,
    * 1/kappa and (stable form) q, one contiguous block per warp. */
   double *gam, *uu, *o1, *q;
-  int64_t slot_stride; /* = nslot*32 */
+  int64_t slot_stride; /* resident threads the scratch is sized for (each warp's block is 32*nz) */
   unsigned long long *work;   /* persistent-kernel work counter (warp tasks) */
   unsigned long long *status; /* [0] zero-pivot count, [1] first bad item (min), [2] timeout flag */
 };
@@ -113,7 +113,7 @@ struct MixedArgs {
   int64_t ld_col, c_off;
   int layout;
   float4 *s4; /* scratch [warp slot][nz][32]: |gamma| or q, 1/kappa, u mantissa, u exponent (int bits) */
-  int64_t slot_stride;
+  int64_t slot_stride; /* resident threads the scratch is sized for */
   unsigned long long *work;
   unsigned long long *status;
 };
@@ -145,7 +145,7 @@ struct MixedBatchArgs {
   double *U, *K, *V, *Vtop, *Vbot;
   int layout;
   float4 *s4;        /* scratch [warp slot][max_nz][32] */
-  int64_t slot_stride;
+  int64_t slot_stride; /* resident threads the scratch is sized for */
   int max_nz;
   unsigned long long *work;
   unsigned long long *status;
@@ -161,7 +161,7 @@ struct FP64BatchArgs {
   double *U, *K, *V, *Vtop, *Vbot;
   int layout;
   double *gam, *uu, *o1, *q; /* scratch [warp slot][max_nz][32] each */
-  int64_t slot_stride;
+  int64_t slot_stride; /* resident threads the scratch is sized for */
   int max_nz;
   unsigned long long *work;
   unsigned long long *status; /* [0] zero pivots, [1] first (column << 32 | wavelength), [2] timeout */
