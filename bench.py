@@ -145,7 +145,7 @@ def run_reference(a):
     rho, T, dz = workloads.agn_block(a.nx, a.ny, a.nz, seed=2)
     wa = workloads.log_wavelengths(a.nw)
     procs = os.cpu_count() or 1
-    cols = max(procs, min(a.cpu_cols // 4, a.nx * a.ny))
+    cols = min(max(procs, a.cpu_cols // 4), a.nx * a.ny)  # the sample never exceeds the grid
     import multiprocessing as mp
     nz = a.nz
     flat_r, flat_t = rho.reshape(-1, nz), T.reshape(-1, nz)
@@ -156,7 +156,8 @@ def run_reference(a):
         for step in range(a.warmup + a.steps):
             c0 = (step * cols) % (a.nx * a.ny - cols + 1)
             parts = np.array_split(np.arange(c0, c0 + cols), procs)
-            jobs = [(flat_r[p].reshape(len(p), 1, nz), flat_t[p].reshape(len(p), 1, nz), wa, dz) for p in parts]
+            jobs = [(flat_r[p].reshape(len(p), 1, nz), flat_t[p].reshape(len(p), 1, nz), wa, dz) for p in parts
+                    if len(p)]
             t0 = time.perf_counter()
             pool.map(_cpu_worker, jobs)
             if step >= a.warmup:
@@ -176,7 +177,7 @@ def run_reference(a):
 
 
 def config_dict(a, form):
-    return {"workload": "plain FP64 non-grey AGN grid, 256x256 columns, nz=512, nw=256",
+    return {"workload": f"plain FP64 non-grey AGN grid, {a.nx}x{a.ny} columns, nz={a.nz}, nw={a.nw}",
             "nx": a.nx, "ny": a.ny, "nz": a.nz, "nw": a.nw, "lambda": "100 A - 10 um log-spaced",
             "form": form, "l2": "inputs and outputs larger than L2 (no flush needed)"}
 
