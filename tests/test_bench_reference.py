@@ -1,6 +1,7 @@
 """The benchmark's reference arm (`bench.py --impl reference`: the CPU restatement of the
-reference loop on the host cores) prints one JSON line with the fields the driver reads, on a
-small grid so that it runs in seconds."""
+reference loop on the host cores) prints one JSON line with the benchmark's fields (value,
+unit, CPU-baseline description, end-to-end entry), checked here on a small grid so that it
+runs in seconds."""
 import json
 import os
 import subprocess
