@@ -1,0 +1,48 @@
+// Host build of the mixed form's arithmetic (mixed_core.h: records, wavelength record, opacity,
+// rows and the extended-exponent Thomas solve) for the CPU tests: libm exp2f/log2f stand in for
+// the GPU's ex2/lg2.approx, everything else is the same code the kernels inline.
+#include <vector>
+
+#include "mixed_core.h"
+#include "oco_internal.h"
+
+using namespace oco;
+
+// U[(iw*ncol + c)*(nz+6) + z], K and V [(iw*ncol + c)*nz + z]; rho, T [c*nz + z]; waves in Angstrom.
+extern "C" void mixed_host_solve(const double *rho, const double *T, const double *wa, int ncol, int nz, int nw,
+                                 double dz, double fully_ionized_T, double *U, double *K, double *V) {
+  std::vector<double> tab((size_t)NL * nw);
+  fill_lambda_table(wa, nw, tab.data());
+  std::vector<float> Z((size_t)nz * mx::MZN), work((size_t)8 * nz);
+  std::vector<double> dwork((size_t)nz + 6);
+  for (int c = 0; c < ncol; c++) {
+    for (int z = 0; z < nz; z++) mx::pillar(rho[(size_t)c * nz + z], T[(size_t)c * nz + z], fully_ionized_T, &Z[(size_t)z * mx::MZN]);
+    for (int iw = 0; iw < nw; iw++) {
+      auto t = [&](int f) { return tab[(size_t)f * nw + iw]; };
+      mx::LamIn li;
+      li.chi = t(L_CHI);
+      li.gff = t(L_GFF);
+      li.chi1 = t(L_CHI1);
+      li.wa3 = t(L_WA3);
+      li.s = t(L_SCOEF);
+      li.hmon = t(L_HMON);
+      li.f1 = t(L_F1);
+      li.f2 = t(L_F2);
+      li.f3 = t(L_F3);
+      for (int q = 0; q < 6; q++) li.gn[q] = t(L_GN1 + q);
+      li.nu9 = t(L_NU9);
+      li.l3nu = t(L_L3NU);
+      li.hnuk = t(L_HNUK);
+      li.wcm1 = t(L_WCM1);
+      li.sw5 = t(L_SW5);
+      float lr[mx::MLN];
+      mx::lambda_record(li, lr);
+      mx::Lam32 L;
+      mx::lam32_from(L, [&](int f) { return lr[f]; });
+      auto zat = [&](int z) { return &Z[(size_t)z * mx::MZN]; };
+      const size_t item = (size_t)iw * ncol + c;
+      mx::solve_item_host(zat, L, nz, dz, work.data(), dwork.data(), U + item * (nz + 6), K + item * nz,
+                          V + item * nz);
+    }
+  }
+}

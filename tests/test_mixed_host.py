@@ -1,0 +1,71 @@
+"""The mixed form's arithmetic (mixed_core.h) compiled for the host, against the stable FP64
+oracle at the mixed form's tolerances: kappa 3e-5, U 5e-4, emergent flux 1e-4 (relative).  The
+GPU kernels inline the same functions (with the SFU's ex2/lg2 for libm's exp2f/log2f), so this
+catches a regression in the arithmetic without a GPU."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "ocotillo_b200")
+BUILD = os.path.join(ROOT, "tests", "_build")
+P = ctypes.POINTER(ctypes.c_double)
+
+
+@pytest.fixture(scope="module")
+def host_lib():
+    lib = os.path.join(PKG, "liboco_b200.so")
+    if not os.path.exists(lib):
+        pytest.fail("liboco_b200.so is missing: build it with `python -m ocotillo_b200.build`")
+    os.makedirs(BUILD, exist_ok=True)
+    out = os.path.join(BUILD, "libmixed_host.so")
+    src = os.path.join(ROOT, "tests", "mixed_host.cpp")
+    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-I", os.path.join(PKG, "csrc"),
+           "-I", "/usr/local/cuda/include", "-o", out, src, f"-L{PKG}", "-l:liboco_b200.so", f"-Wl,-rpath,{PKG}"]
+    subprocess.run(cmd, check=True, capture_output=True)
+    h = ctypes.CDLL(out)
+    h.mixed_host_solve.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                   ctypes.c_double, P, P, P]
+    return h
+
+
+def _solve(h, rho, T, wa, dz):
+    ncol, nz = rho.shape
+    nw = len(wa)
+    U = np.zeros(nw * ncol * (nz + 6))
+    K = np.zeros(nw * ncol * nz)
+    V = np.zeros(nw * ncol * nz)
+    p = lambda a: a.ctypes.data_as(P)
+    h.mixed_host_solve(p(np.ascontiguousarray(rho)), p(np.ascontiguousarray(T)), p(wa), ncol, nz, nw, dz, 2e4,
+                       p(U), p(K), p(V))
+    return U.reshape(nw, ncol, nz + 6), K.reshape(nw, ncol, nz), V.reshape(nw, ncol, nz)
+
+
+@pytest.mark.parametrize("case", ["agn", "athena"])
+def test_mixed_host_against_stable_oracle(host_lib, oracle, case):
+    from ocotillo_b200 import workloads
+    if case == "agn":
+        rho, T, dz = workloads.agn_block(2, 3, 160, seed=31)
+        wa = workloads.log_wavelengths(48)
+    else:
+        rng = np.random.default_rng(32)
+        cols = [workloads.athena_column(120, rng, sigma_dex=0.3) for _ in range(4)]
+        rho = np.stack([c[0] for c in cols]).reshape(4, 1, 120)
+        T = np.stack([c[1] for c in cols]).reshape(4, 1, 120)
+        dz = cols[0][2]
+        wa = workloads.log_wavelengths(40, 900.0, 40000.0)
+    nx, ny, nz = rho.shape
+    U, K, V = _solve(host_lib, rho.reshape(-1, nz), T.reshape(-1, nz), wa, dz)
+    ref = oracle.solve_block(rho, T, wa, dz, form=oracle.FORM_STABLE, backend="ocomath")
+    nw = len(wa)
+    rU = ref["U"].reshape(nw, nx * ny, nz + 6)
+    rK = ref["kappa"].reshape(nw, nx * ny, nz)
+    rV = ref["V"].reshape(nw, nx * ny, nz)
+    rel = lambda a, b: np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
+    assert rel(K, rK).max() <= 3e-5
+    assert rel(U, rU).max() <= 5e-4
+    for end in (-1, 0):
+        assert rel(V[..., end], rV[..., end]).max() <= 1e-4, end
