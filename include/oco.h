@@ -189,8 +189,8 @@ const char *oco_noalloc_last_error(void);
  * No counterpart in the reference, whose loop runs one block with one nz and one wavelength
  * grid: a batch is a set of independent columns, each with its own nz, dz and wavelength
  * grid (for instance columns of several snapshots), solved by one persistent launch fed from
- * a device work queue and replayed as a CUDA graph.  Mixed form only.  Per column the
- * arithmetic is that of oco_solve_block_device with p->form = OCO_FORM_MIXED.
+ * a device work queue and replayed as a CUDA graph.  Per column the arithmetic is that of
+ * oco_solve_block_device with p->form set to the batch's form (plain, stable or mixed).
  *
  * Array layout (device arrays, element offsets given per column):
  *   rho, T      nz values from in_off (z fastest), read-only

@@ -65,3 +65,49 @@ def test_no_alloc_rejects_bad_sizes_before_touching_a_device():
     prm = OcoParams(1, 1, 1, 8, 1e13, 0.4, 2e4, 0, 0, 0, 0)  # nz = 1
     assert lib.oco_solve_block_noalloc(ctypes.byref(prm), None, ctypes.c_void_p(1), ctypes.c_void_p(1),
                                        ctypes.c_void_p(1), None, None, None, None, None) == -1
+
+
+def test_every_ctypes_struct_matches_its_c_layout(tmp_path):
+    """Each ctypes mirror in engine.py has the C struct's size and every field's offset."""
+    from ocotillo_b200 import engine
+    pairs = {"oco_params": engine.OcoParams, "oco_batch_column": engine.OcoBatchColumn,
+             "oco_batch_info": engine.OcoBatchInfo, "oco_server_config": engine.OcoServerConfig,
+             "oco_job": engine.OcoJob, "oco_job_status": engine.OcoJobStatus,
+             "oco_deck_info": engine.OcoDeckInfo}
+    lines = []
+    for cname, cls in pairs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f in cls._fields_:
+            lines.append(f'printf("{cname} {f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "oco.h"\nint main(void){'
+                   + "".join(lines) + "return 0;}\n")
+    exe = tmp_path / "layout"
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)])
+    c = {}
+    for ln in subprocess.check_output([str(exe)]).decode().splitlines():
+        s, f, v = ln.split()
+        c[(s, f)] = int(v)
+    for cname, cls in pairs.items():
+        assert ctypes.sizeof(cls) == c[(cname, "size")], cname
+        for f in cls._fields_:
+            assert getattr(cls, f[0]).offset == c[(cname, f[0])], (cname, f[0])
+
+
+def test_dense_batch_offsets_are_prefix_sums():
+    from ocotillo_b200 import dense_batch_offsets
+    nz = [2, 512, 37, 1024]
+    nw = [1, 256, 3, 17]
+    o = dense_batch_offsets(nz, nw)
+    in_off, u_off, kv_off, f_off = [0], [0], [0], [0]
+    for a, b in zip(nz, nw):
+        in_off.append(in_off[-1] + a)
+        u_off.append(u_off[-1] + (a + 6) * b)
+        kv_off.append(kv_off[-1] + a * b)
+        f_off.append(f_off[-1] + b)
+    assert list(o["in_off"]) == in_off[:-1] and o["n_in"] == in_off[-1]
+    assert list(o["u_off"]) == u_off[:-1] and o["n_u"] == u_off[-1]
+    assert list(o["kv_off"]) == kv_off[:-1] and o["n_kv"] == kv_off[-1]
+    assert list(o["flux_off"]) == f_off[:-1] and o["n_flux"] == f_off[-1]
+    one = dense_batch_offsets([5], [4])
+    assert list(one["u_off"]) == [0] and one["n_u"] == 44 and one["n_flux"] == 4
