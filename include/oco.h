@@ -198,7 +198,8 @@ const char *oco_noalloc_last_error(void);
  *               OCO_LAYOUT_REFERENCE, [z][lambda] for OCO_LAYOUT_LAMBDA_FASTEST
  *   kappa, V    from kv_off: nz x nw values, same order as U
  *   Vtop, Vbot  from flux_off: nw values (V at z index nz and 1)
- * Output ranges of different columns must not overlap. */
+ * Output ranges of different columns must not overlap (oco_batch_bind checks this for the
+ * arrays it is given); offsets are at most 2^56. */
 typedef struct oco_batch oco_batch;
 
 typedef struct oco_batch_column {
@@ -241,7 +242,8 @@ int oco_batch_create(oco_ctx *ctx, const oco_batch_column *cols, int64_t ncol, c
 
 /* Binds the device arrays (element counts for the bounds check of every column's ranges)
  * and captures the batch's launches into a CUDA graph.  U, kappa, V, Vtop, Vbot may be NULL
- * (not stored; their count is then ignored).  Rebinding recaptures. */
+ * (not stored; their count is then ignored).  OCO_EINVAL when a bound output array's
+ * ranges of two columns overlap (the message names the pair).  Rebinding recaptures. */
 int oco_batch_bind(oco_batch *batch, const double *rho, const double *T, int64_t n_in, double *U,
                    int64_t n_u, double *kappa, double *V, int64_t n_kv, double *Vtop, double *Vbot,
                    int64_t n_flux);

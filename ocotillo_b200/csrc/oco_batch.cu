@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "../../include/oco.h"
+#include "batch_layout.h"
 #include "mixed_core.h"
 #include "oco_ctx.h"
 #include "oco_internal.h"
@@ -46,6 +47,9 @@ struct oco_batch {
   int64_t ncol = 0, npoints = 0, nrec = 0, nitems = 0, ntasks_tile = 0, ntasks_packed = 0;
   int max_nz = 0, max_nw = 0;
   int64_t need_in = 0, need_u = 0, need_kv = 0, need_flux = 0; /* element counts the arrays must hold */
+  /* first pair of columns whose output ranges overlap, per array family (U; kappa and V;
+     Vtop and Vbot), {-1, -1} if none: binding an array of an overlapping family fails */
+  int64_t overlap[3][2] = {{-1, -1}, {-1, -1}, {-1, -1}};
   DevBuf cols, rec_pre, tasks, order, item_pre, lam, rec, scratch, work, status;
   int64_t slots = 0; /* scratch slots (threads of the largest persistent grid) */
   int tiling = OCO_TILING_WARP_COLUMN, bps = 1, max_bps[2] = {1, 1}; /* max_bps 0: tiling not available */
@@ -208,10 +212,11 @@ extern "C" int oco_batch_create(oco_ctx *c, const oco_batch_column *cols, int64_
   std::vector<double> tab;
   for (int64_t i = 0; i < ncol; i++) {
     const oco_batch_column &q = cols[i];
-    if (q.nz < 2 || q.nw < 1 || !(q.dz > 0.0) || !std::isfinite(q.dz) || q.in_off < 0 || q.u_off < 0 ||
-        q.kv_off < 0 || q.flux_off < 0 || q.wave_off < 0 || q.wave_off + q.nw > nwaves)
+    const auto off_ok = [](int64_t o) { return o >= 0 && o <= kBatchMaxOffset; };
+    if (q.nz < 2 || q.nw < 1 || !(q.dz > 0.0) || !std::isfinite(q.dz) || !off_ok(q.in_off) || !off_ok(q.u_off) ||
+        !off_ok(q.kv_off) || !off_ok(q.flux_off) || q.wave_off < 0 || q.wave_off > nwaves - q.nw)
       return oco_set_err(c, OCO_EINVAL,
-                         "oco_batch_create: column %lld: need nz >= 2, nw >= 1, dz > 0, offsets >= 0 and "
+                         "oco_batch_create: column %lld: need nz >= 2, nw >= 1, dz > 0, 0 <= offsets <= 2^56 and "
                          "wave_off + nw <= nwaves",
                          (long long)i);
     auto key = std::make_pair(q.wave_off, q.nw);
@@ -257,6 +262,19 @@ extern "C" int oco_batch_create(oco_ctx *c, const oco_batch_column *cols, int64_
     b->need_flux = std::max(b->need_flux, q.flux_off + q.nw);
   }
   b->nrec = rpre[(size_t)ncol];
+  {
+    std::vector<int64_t> off((size_t)ncol), len((size_t)ncol);
+    for (int f = 0; f < 3; f++) {
+      for (int64_t i = 0; i < ncol; i++) {
+        const oco_batch_column &q = cols[i];
+        off[(size_t)i] = f == 0 ? q.u_off : f == 1 ? q.kv_off : q.flux_off;
+        len[(size_t)i] = f == 0 ? (int64_t)(q.nz + 6) * q.nw : f == 1 ? (int64_t)q.nz * q.nw : q.nw;
+      }
+      const auto pr = first_overlap(off, len);
+      b->overlap[f][0] = pr.first;
+      b->overlap[f][1] = pr.second;
+    }
+  }
 
   /* work lists, longest column first */
   std::vector<int32_t> order((size_t)ncol);
@@ -332,6 +350,12 @@ extern "C" int oco_batch_bind(oco_batch *b, const double *rho, const double *T, 
     return oco_set_err(c, OCO_EINVAL, "oco_batch_bind: kappa and V need %lld elements", (long long)b->need_kv);
   if ((Vtop || Vbot) && n_flux < b->need_flux)
     return oco_set_err(c, OCO_EINVAL, "oco_batch_bind: Vtop and Vbot need %lld elements", (long long)b->need_flux);
+  const bool bound_family[3] = {U != nullptr, kappa || V, Vtop || Vbot};
+  static const char *family[3] = {"U", "kappa/V", "Vtop/Vbot"};
+  for (int f = 0; f < 3; f++)
+    if (bound_family[f] && b->overlap[f][0] >= 0)
+      return oco_set_err(c, OCO_EINVAL, "oco_batch_bind: columns %lld and %lld have overlapping %s ranges",
+                         (long long)b->overlap[f][0], (long long)b->overlap[f][1], family[f]);
   CU(cudaSetDevice(c->device));
   if (b->pending) CU(cudaStreamSynchronize(b->last));
   b->rho = rho;

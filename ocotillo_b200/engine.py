@@ -383,10 +383,13 @@ class Engine:
         self._check(self.lib.oco_kernel_times(self.ctx, ctypes.byref(a), ctypes.byref(b), ctypes.byref(n)))
         return a.value, b.value, n.value
 
-    def batch(self, nz, nw, dz, waves, wave_off, layout=LAYOUT_LAMBDA_FASTEST, fully_ionized_T=2e4, form="mixed"):
-        """A ragged batch of len(nz) columns packed densely (see dense_batch_offsets): column i
-        has nz[i] levels, spacing dz[i] and the nw[i] wavelengths waves[wave_off[i]:...]."""
-        return Batch(self, nz, nw, dz, waves, wave_off, layout, fully_ionized_T, form)
+    def batch(self, nz, nw, dz, waves, wave_off, layout=LAYOUT_LAMBDA_FASTEST, fully_ionized_T=2e4, form="mixed",
+              offsets=None):
+        """A ragged batch of len(nz) columns: column i has nz[i] levels, spacing dz[i] and the
+        nw[i] wavelengths waves[wave_off[i]:...]; form is "plain", "stable" or "mixed".  The
+        arrays are packed densely (dense_batch_offsets) unless offsets gives the per-column
+        element offsets {"in_off", "u_off", "kv_off", "flux_off"} of the caller's packing."""
+        return Batch(self, nz, nw, dz, waves, wave_off, layout, fully_ionized_T, form, offsets)
 
 
 def dense_batch_offsets(nz, nw):
@@ -403,18 +406,39 @@ def dense_batch_offsets(nz, nw):
             "n_in": int(p_in[-1]), "n_u": int(p_u[-1]), "n_kv": int(p_kv[-1]), "n_flux": int(p_f[-1])}
 
 
+def batch_offsets(nz, nw, in_off, u_off, kv_off, flux_off):
+    """A caller's packing of a batch's arrays in the form dense_batch_offsets returns: the
+    per-column offsets and, per array, the element count that holds every column's range."""
+    nz = np.asarray(nz, dtype=np.int64)
+    nw = np.asarray(nw, dtype=np.int64)
+    o = {k: np.asarray(v, dtype=np.int64).copy() for k, v in
+         (("in_off", in_off), ("u_off", u_off), ("kv_off", kv_off), ("flux_off", flux_off))}
+    if any(v.shape != nz.shape for v in o.values()):
+        raise ValueError("batch_offsets: one offset per column")
+    o["n_in"] = int((o["in_off"] + nz).max())
+    o["n_u"] = int((o["u_off"] + (nz + 6) * nw).max())
+    o["n_kv"] = int((o["kv_off"] + nz * nw).max())
+    o["n_flux"] = int((o["flux_off"] + nw).max())
+    return o
+
+
 class Batch:
     """Ragged batch (include/oco.h, oco_batch_*): independent columns of different nz, dz
     and wavelength grids, solved by one persistent launch replayed as a CUDA graph.  Arrays
-    are torch CUDA float64 tensors packed as dense_batch_offsets describes; per column U is
-    [z][lambda] (LAYOUT_LAMBDA_FASTEST) or [lambda][z] (LAYOUT_REFERENCE)."""
+    are torch CUDA float64 tensors packed as dense_batch_offsets describes (or as the caller's
+    offsets give, see batch_offsets); per column U is [z][lambda] (LAYOUT_LAMBDA_FASTEST) or
+    [lambda][z] (LAYOUT_REFERENCE)."""
 
-    def __init__(self, eng, nz, nw, dz, waves, wave_off, layout, fully_ionized_T, form):
+    def __init__(self, eng, nz, nw, dz, waves, wave_off, layout, fully_ionized_T, form, offsets=None):
         self.eng, self.lib = eng, eng.lib
         n = len(nz)
         self.nz = np.asarray(nz, dtype=np.int64)
         self.nw = np.asarray(nw, dtype=np.int64)
-        self.offsets = dense_batch_offsets(self.nz, self.nw)
+        if offsets is None:
+            self.offsets = dense_batch_offsets(self.nz, self.nw)
+        else:
+            self.offsets = batch_offsets(self.nz, self.nw, offsets["in_off"], offsets["u_off"], offsets["kv_off"],
+                                         offsets["flux_off"])
         cols = (OcoBatchColumn * n)()
         o = self.offsets
         for i in range(n):

@@ -111,3 +111,17 @@ def test_dense_batch_offsets_are_prefix_sums():
     assert list(o["flux_off"]) == f_off[:-1] and o["n_flux"] == f_off[-1]
     one = dense_batch_offsets([5], [4])
     assert list(one["u_off"]) == [0] and one["n_u"] == 44 and one["n_flux"] == 4
+
+
+def test_batch_offsets_of_a_caller_packing():
+    from ocotillo_b200 import batch_offsets, dense_batch_offsets
+    nz, nw = [2, 512, 37], [1, 256, 3]
+    d = dense_batch_offsets(nz, nw)
+    same = batch_offsets(nz, nw, d["in_off"], d["u_off"], d["kv_off"], d["flux_off"])
+    assert all(np.array_equal(same[k], d[k]) if k.endswith("_off") else same[k] == d[k] for k in d)
+    # reverse order with gaps: every total is the furthest end, not the sum
+    o = batch_offsets(nz, nw, [700, 100, 0], [10, 0, 200000], [0, 5, 1000], [9, 4, 0])
+    assert o["n_in"] == 702 and o["n_u"] == 200000 + 43 * 3 and o["n_kv"] == 5 + 512 * 256
+    assert o["n_flux"] == 4 + 256
+    with pytest.raises(ValueError):
+        batch_offsets(nz, nw, [0, 1], [0, 0, 0], [0, 0, 0], [0, 0, 0])

@@ -236,6 +236,60 @@ def test_batch_rejects_bad_descriptors(engine):
     b.close()
 
 
+def test_batch_caller_offsets_and_overlap(engine):
+    """A caller's packing (columns in reverse order, NaN-filled gaps between them) gives every
+    column the bits of the dense packing; an output family whose column ranges overlap is
+    refused at bind when that array is bound, and accepted when it is not."""
+    import torch
+    from ocotillo_b200 import OcoError, dense_batch_offsets, LAYOUT_LAMBDA_FASTEST
+    d = _small_batch(seed=12)
+    nz, nw = d["nz"], d["nw"]
+    n = len(nz)
+    dense = dense_batch_offsets(nz, nw)
+    sizes = {"in_off": nz, "u_off": (nz + 6) * nw, "kv_off": nz * nw, "flux_off": nw}
+    off = {}
+    for k, s in sizes.items():
+        pos, o = 3, np.zeros(n, dtype=np.int64)
+        for i in reversed(range(n)):
+            o[i] = pos
+            pos += int(s[i]) + 5
+        off[k] = o
+    ref, _, _, out0 = _make(engine, d, LAYOUT_LAMBDA_FASTEST, form="plain")
+    _run_fp64(ref)
+
+    b = engine.batch(nz, nw, d["dz"], d["waves"], d["wave_off"], form="plain", offsets=off)
+    rho = np.full(b.offsets["n_in"], np.nan)
+    T = np.full(b.offsets["n_in"], np.nan)
+    for i in range(n):
+        src, dst = int(dense["in_off"][i]), int(off["in_off"][i])
+        rho[dst:dst + nz[i]] = d["rho"][src:src + nz[i]]
+        T[dst:dst + nz[i]] = d["T"][src:src + nz[i]]
+    dev = torch.device("cuda:0")
+    rho, T = torch.from_numpy(rho).to(dev), torch.from_numpy(T).to(dev)
+    out = b.alloc(dev)
+    b.bind(rho, T, out)
+    _run_fp64(b)
+    for i in range(n):
+        for name in ("U", "kappa", "V", "Vtop", "Vbot"):
+            assert _same(b.column(out, i, name), ref.column(out0, i, name).cpu().numpy()), (i, name)
+    b.close()
+
+    bad = {k: v.copy() for k, v in off.items()}
+    bad["u_off"][4] = bad["u_off"][5] + 1  # column 4's U range starts inside column 5's
+    bo = engine.batch(nz, nw, d["dz"], d["waves"], d["wave_off"], form="plain", offsets=bad)
+    with pytest.raises(OcoError) as e:
+        bo.bind(rho, T, bo.alloc(dev))
+    assert "columns 4 and 5 have overlapping U ranges" in str(e.value)
+    part = bo.alloc(dev, want=("kappa", "V", "Vtop", "Vbot"))
+    bo.bind(rho, T, part)
+    _run_fp64(bo)
+    for i in range(n):
+        for name in ("kappa", "V", "Vtop", "Vbot"):
+            assert _same(bo.column(part, i, name), ref.column(out0, i, name).cpu().numpy()), (i, name)
+    bo.close()
+    ref.close()
+
+
 @pytest.mark.parametrize("form,layout", [("plain", 0), ("plain", 1), ("stable", 0), ("stable", 1)])
 def test_batch_fp64_bitwise_block_solve(engine, form, layout):
     d = _small_batch(seed=16)
