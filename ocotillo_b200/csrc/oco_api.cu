@@ -259,6 +259,8 @@ static int check_params(oco_ctx *c, const oco_params *p) {
   if (p->nx < 1 || p->ny < 1 || p->nz < 2 || p->nw < 1)
     return oco_set_err(c, OCO_EINVAL, "bad dimensions nx=%d ny=%d nz=%d nw=%d (need nz >= 2)", p->nx, p->ny,
                    p->nz, p->nw);
+  if (!block_elements_fit(p->nx, p->ny, p->nz, p->nw))
+    return oco_set_err(c, OCO_EINVAL, "block too large: nx*ny*nw*(nz+6) exceeds 2^56 elements");
   if (p->lgrey && p->nw != 1)
     return oco_set_err(c, OCO_EGREY, "For Grey RT use only one wavelength. Switch nw=1 in resolution.in");
   if (!p->lgrey && (c->nw != p->nw))
@@ -267,7 +269,7 @@ static int check_params(oco_ctx *c, const oco_params *p) {
     return oco_set_err(c, OCO_EINVAL, "unknown form %d", p->form);
   if (p->layout != OCO_LAYOUT_REFERENCE && p->layout != OCO_LAYOUT_LAMBDA_FASTEST)
     return oco_set_err(c, OCO_EINVAL, "unknown layout %d", p->layout);
-  if (!(p->dz > 0.0)) return oco_set_err(c, OCO_EINVAL, "dz must be positive");
+  if (!(p->dz > 0.0) || !std::isfinite(p->dz)) return oco_set_err(c, OCO_EINVAL, "dz must be positive and finite");
   return OCO_OK;
 }
 

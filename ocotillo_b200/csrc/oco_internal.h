@@ -11,6 +11,13 @@
 
 namespace oco {
 
+/* Whether a block's largest array (U, nx*ny*nw*(nz+6) elements) stays within 2^56 elements,
+ * the limit the entry points accept: every element index and byte count of the host code and
+ * the kernels then fits int64.  Computed in double, whose rounding only blurs the bound. */
+inline bool block_elements_fit(int nx, int ny, int nz, int nw) {
+  return (double)nx * (double)ny * (double)nw * ((double)nz + 6.0) <= 72057594037927936.0;
+}
+
 /* Per-(column, z) quantities written by the pillar kernel and read by the solve kernels:
  * the wavelength-independent part of the reference's per-(z, lambda) work
  * (gas_state.f90:30-110 plus every factor of continuous_opacity.f90 that depends on z

@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -78,7 +79,9 @@ extern "C" int oco_solve_block_noalloc(const oco_params *p, const double *wa_ang
     return fail(OCO_EINVAL, "oco_solve_block_noalloc supports the plain and stable FP64 forms only");
   if (p->layout != OCO_LAYOUT_REFERENCE && p->layout != OCO_LAYOUT_LAMBDA_FASTEST)
     return fail(OCO_EINVAL, "unknown layout %d", p->layout);
-  if (!(p->dz > 0.0)) return fail(OCO_EINVAL, "dz must be positive");
+  if (!(p->dz > 0.0) || !std::isfinite(p->dz)) return fail(OCO_EINVAL, "dz must be positive and finite");
+  if (!block_elements_fit(p->nx, p->ny, p->nz, p->nw))
+    return fail(OCO_EINVAL, "block too large: nx*ny*nw*(nz+6) exceeds 2^56 elements");
   if (!p->lgrey && !wa_angstrom) return fail(OCO_ENOWAVES, "wavelengths are required");
   if (p->nz > OCO_NOALLOC_MAX_NZ || p->nw > OCO_NOALLOC_MAX_NW)
     return fail(OCO_EINVAL, "oco_solve_block_noalloc: nz=%d nw=%d exceed the static workspace limits nz <= %d, nw <= %d",

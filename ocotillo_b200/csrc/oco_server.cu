@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstdarg>
 #include <cstdio>
@@ -408,9 +409,14 @@ extern "C" int oco_server_create(const oco_server_config *cfg, oco_server **out)
 
 extern "C" int oco_server_submit(oco_server *s, const oco_job *job, int64_t *job_id) {
   if (!s || !job || !job_id) return serr(OCO_EINVAL, "oco_server_submit: NULL argument");
-  if (job->nx < 1 || job->ny < 1 || job->nz < 2 || job->nw < 1 || !(job->dz > 0.0) || !job->rho || !job->T ||
-      !job->waves)
-    return serr(OCO_EINVAL, "oco_server_submit: bad job (need nx, ny >= 1, nz >= 2, nw >= 1, dz > 0, arrays)");
+  if (job->nx < 1 || job->ny < 1 || job->nz < 2 || job->nw < 1 || !(job->dz > 0.0) || !std::isfinite(job->dz) ||
+      !job->rho || !job->T || !job->waves)
+    return serr(OCO_EINVAL, "oco_server_submit: bad job (need nx, ny >= 1, nz >= 2, nw >= 1, finite dz > 0, arrays)");
+  if (!oco::block_elements_fit(job->nx, job->ny, job->nz, job->nw))
+    return serr(OCO_EINVAL, "oco_server_submit: job too large: nx*ny*nw*(nz+6) exceeds 2^56 elements");
+  for (int i = 0; i < job->nw; i++)
+    if (!(job->waves[i] > 0.0) || !std::isfinite(job->waves[i]))
+      return serr(OCO_EINVAL, "oco_server_submit: wavelength %d is not positive and finite", i);
   if (job->form != OCO_FORM_PLAIN && job->form != OCO_FORM_STABLE && job->form != OCO_FORM_MIXED)
     return serr(OCO_EINVAL, "oco_server_submit: unknown form %d", job->form);
   auto j = std::make_unique<Job>();

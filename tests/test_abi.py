@@ -67,6 +67,21 @@ def test_no_alloc_rejects_bad_sizes_before_touching_a_device():
                                        ctypes.c_void_p(1), None, None, None, None, None) == -1
 
 
+@pytest.mark.parametrize("dims,dz,msg", [((2**31 - 1, 2**31 - 1, 4096, 4096), 1e13, b"exceeds 2^56"),
+                                         ((2**20, 2**20, 4096, 4096), 1e13, b"exceeds 2^56"),
+                                         ((1, 1, 8, 8), float("inf"), b"finite"),
+                                         ((1, 1, 8, 8), float("nan"), b"finite")])
+def test_no_alloc_rejects_oversized_blocks_and_bad_dz(dims, dz, msg):
+    """Element counts beyond 2^56 (which would wrap int64 index arithmetic) and a non-finite dz
+    are refused before any device work."""
+    from ocotillo_b200.engine import load_library, OcoParams
+    lib = load_library()
+    prm = OcoParams(*dims, dz, 0.4, 2e4, 0, 0, 0, 0)
+    one = ctypes.c_void_p(1)
+    assert lib.oco_solve_block_noalloc(ctypes.byref(prm), None, one, one, one, None, None, None, None, None) == -1
+    assert msg in lib.oco_noalloc_last_error()
+
+
 def test_every_ctypes_struct_matches_its_c_layout(tmp_path):
     """Each ctypes mirror in engine.py has the C struct's size and every field's offset."""
     from ocotillo_b200 import engine

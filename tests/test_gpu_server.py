@@ -104,6 +104,14 @@ def test_server_rejects_and_shuts_down():
     with pytest.raises(OcoError) as e:
         srv.submit(rho, T, wa, dz)  # footprint above the budget: never admissible
     assert e.value.code == -8
+    bad_wa = wa.copy()
+    bad_wa[3] = float("nan")
+    with pytest.raises(OcoError) as e:
+        srv.submit(rho, T, bad_wa, dz)  # refused at submission, not failed later
+    assert e.value.code == -1 and "wavelength 3" in str(e.value)
+    with pytest.raises(OcoError) as e:
+        srv.submit(rho, T, wa, float("inf"))
+    assert e.value.code == -1
     srv.close()
     # shutting down with one job running and three queued: the queued ones are dropped, the
     # running one finishes, and the call returns
