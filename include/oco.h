@@ -36,7 +36,8 @@ extern "C" {
 
 /* Return codes.  The first group mirrors the reference's 'print ... ; stop' sites. */
 #define OCO_OK 0
-#define OCO_EINVAL (-1)      /* bad argument or dimension (nz < 2, nw < 1, NULL input) */
+#define OCO_EINVAL (-1)      /* bad argument or dimension (nz < 2, nw < 1, NULL input, dz not
+                                positive and finite, nx*ny*nw*(nz+6) above 2^56 elements) */
 #define OCO_ENOMEM (-2)      /* allocation failed; flux_feautrier.f90:95-104 */
 #define OCO_EZEROPIVOT (-3)  /* a Thomas pivot was exactly 0; auxiliary.f90:27-39 */
 #define OCO_EGREY (-4)       /* grey RT with nw != 1; flux_feautrier.f90:84-87 */
