@@ -140,3 +140,41 @@ def test_batch_offsets_of_a_caller_packing():
     assert o["n_flux"] == 4 + 256
     with pytest.raises(ValueError):
         batch_offsets(nz, nw, [0, 1], [0, 0, 0], [0, 0, 0], [0, 0, 0])
+
+
+def _c_kind(t):
+    t = t.strip()
+    if "*" in t:
+        return "ptr"
+    t = re.sub(r"\bconst\b", "", t).split()[0]
+    return {"int": "i32", "int32_t": "i32", "int64_t": "i64", "double": "f64", "void": "void"}[t]
+
+
+def _py_kind(t):
+    if t is None:
+        return "void"
+    if t in (ctypes.c_void_p, ctypes.c_char_p) or isinstance(t, type(ctypes.POINTER(ctypes.c_int))):
+        return "ptr"
+    return {ctypes.c_int32: "i32", ctypes.c_int64: "i64", ctypes.c_double: "f64"}[t]
+
+
+def test_ctypes_signatures_match_the_header():
+    """Every function the header declares has a ctypes signature in the binding with the same
+    number of arguments and the same kind (pointer, int32, int64, double) of each, and the same
+    return kind: a mismatch would pass garbage through the ABI without any error."""
+    from ocotillo_b200 import load_library
+    lib = load_library()
+    text = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "oco.h")).read(), flags=re.S)
+    proto = re.compile(r"^\s*((?:const\s+)?[A-Za-z_][A-Za-z0-9_]*\s*\**)\s*(oco_[a-z0-9_]+)\s*\(([^)]*)\)\s*;", re.M)
+    seen = 0
+    for m in proto.finditer(text):
+        ret, name, params = m.group(1), m.group(2), m.group(3)
+        params = [] if params.strip() in ("", "void") else params.split(",")
+        want = [_c_kind(re.sub(r"\b[A-Za-z_][A-Za-z0-9_]*\s*$", "", p) if "*" not in p.split()[-1] else p)
+                for p in params]
+        f = getattr(lib, name)
+        assert f.argtypes is not None, f"{name}: no ctypes signature"
+        assert [_py_kind(a) for a in f.argtypes] == want, name
+        assert _py_kind(f.restype) == _c_kind(ret), name
+        seen += 1
+    assert seen == len(declared_functions())
