@@ -86,6 +86,10 @@ extern "C" int oco_solve_block_noalloc(const oco_params *p, const double *wa_ang
   if (p->nz > OCO_NOALLOC_MAX_NZ || p->nw > OCO_NOALLOC_MAX_NW)
     return fail(OCO_EINVAL, "oco_solve_block_noalloc: nz=%d nw=%d exceed the static workspace limits nz <= %d, nw <= %d",
                 p->nz, p->nw, OCO_NOALLOC_MAX_NZ, OCO_NOALLOC_MAX_NW);
+  if (!p->lgrey)
+    for (int i = 0; i < p->nw; i++)
+      if (!(wa_angstrom[i] > 0.0) || !std::isfinite(wa_angstrom[i]))
+        return fail(OCO_EINVAL, "wavelength %d is not positive and finite", i);
   const int grey = p->lgrey ? 1 : 0;
   const int nz = p->nz, nw = p->nw;
   cudaStream_t s = (cudaStream_t)stream;

@@ -82,6 +82,18 @@ def test_no_alloc_rejects_oversized_blocks_and_bad_dz(dims, dz, msg):
     assert msg in lib.oco_noalloc_last_error()
 
 
+def test_no_alloc_rejects_bad_wavelengths_before_touching_a_device():
+    from ocotillo_b200.engine import load_library, OcoParams
+    lib = load_library()
+    prm = OcoParams(1, 1, 8, 4, 1e13, 0.4, 2e4, 0, 0, 0, 0)
+    one = ctypes.c_void_p(1)
+    for bad in (0.0, -5000.0, float("nan"), float("inf")):
+        wa = np.array([3000.0, 4000.0, bad, 6000.0])
+        assert lib.oco_solve_block_noalloc(ctypes.byref(prm), wa.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                           one, one, one, None, None, None, None, None) == -1
+        assert b"wavelength 2" in lib.oco_noalloc_last_error()
+
+
 def test_every_ctypes_struct_matches_its_c_layout(tmp_path):
     """Each ctypes mirror in engine.py has the C struct's size and every field's offset."""
     from ocotillo_b200 import engine
