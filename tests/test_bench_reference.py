@@ -1,7 +1,7 @@
 """The benchmark's reference arm (`bench.py --impl reference`: the CPU restatement of the
 reference loop on the host cores) prints one JSON line with the benchmark's fields (value,
 unit, CPU-baseline description, end-to-end entry), checked here on a small grid so that it
-runs in seconds."""
+runs in seconds; and the summary of the clock samples taken during the timed region."""
 import json
 import os
 import subprocess
@@ -24,3 +24,34 @@ def test_reference_arm_json_line():
     assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     e = d["e2e"]
     assert e["value"] == d["value"] and e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
+
+
+class _Done:
+    def terminate(self):
+        pass
+
+    def wait(self):
+        return 0
+
+
+def _clocks_from(rows):
+    sys.path.insert(0, ROOT)
+    import bench
+    c = bench.Clocks(0)
+    c.f.write("".join(r + "\n" for r in rows))
+    c.p = _Done()
+    return c.stop()
+
+
+def test_clock_record_summary():
+    """The clock record of the timed region (nvidia-smi samples): median SM clock, max clock,
+    the throttle reasons seen Active in any sample, malformed lines skipped."""
+    s = _clocks_from(["0, 1965, 1965, 900.50, 0x0, Not Active, Not Active, Not Active, Not Active",
+                      "0, 1900, 1965, 990.10, 0x4, Not Active, Not Active, Not Active, Active",
+                      "garbage",
+                      "0, 1950, 1965, [N/A], 0x0, Not Active, Not Active, Not Active, Not Active"])
+    assert s["sm_mhz"] == 1950.0 and s["sm_max_mhz"] == 1965.0 and s["samples"] == 3
+    assert s["reasons"] == ["sw_power_cap"] and s["power_w_max"] == 990.1
+    s = _clocks_from(["0, 1500, 1965, [N/A], 0x0, Active, Not Active, Active, Not Active"])
+    assert s["reasons"] == ["hw_slowdown", "sw_thermal_slowdown"] and s["power_w_max"] is None
+    assert _clocks_from([])["reasons"] == ["no samples"]
