@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "../../include/oco.h"
+#include "fortran_records.h"
 
 namespace {
 
@@ -255,33 +256,12 @@ std::string list_int_real(int i, double v) {
   return out;
 }
 
-/* One Fortran unformatted sequential record (gfortran): 4-byte length markers around the
- * data; records above 2147483639 bytes are split into subrecords whose leading marker is
- * negative when more follow and whose trailing marker is negative when one precedes. */
-bool write_record(FILE *fp, const void *data, size_t bytes) {
-  const size_t kMax = 2147483639u;
-  const char *p = (const char *)data;
-  size_t left = bytes;
-  bool first = true;
-  do {
-    const size_t len = left > kMax ? kMax : left;
-    const bool last = (left - len) == 0;
-    const int32_t lead = last ? (int32_t)len : -(int32_t)len;
-    const int32_t trail = first ? (int32_t)len : -(int32_t)len;
-    if (fwrite(&lead, 4, 1, fp) != 1) return false;
-    if (len && fwrite(p, 1, len, fp) != len) return false;
-    if (fwrite(&trail, 4, 1, fp) != 1) return false;
-    p += len;
-    left -= len;
-    first = false;
-  } while (left > 0);
-  return true;
-}
-
+/* A file holding one Fortran unformatted sequential record of n doubles (gfortran markers and
+ * subrecords, fortran_records.h). */
 bool write_record_file(const std::string &path, const double *a, size_t n) {
   FILE *fp = fopen(path.c_str(), "wb");
   if (!fp) return false;
-  const bool ok = write_record(fp, a, n * sizeof(double));
+  const bool ok = oco::write_fortran_record(fp, a, n * sizeof(double));
   return (fclose(fp) == 0) && ok;
 }
 

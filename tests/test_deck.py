@@ -70,3 +70,40 @@ def test_fortran_records_roundtrip(tmp_path):
         f.write((4).to_bytes(4, "little", signed=True) + b[3:] + (-4).to_bytes(4, "little", signed=True))
     recs = read_fortran_records(str(p))
     assert recs == [a, b]
+
+
+@pytest.fixture(scope="module")
+def record_writer():
+    import ctypes
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    build = os.path.join(root, "tests", "_build")
+    os.makedirs(build, exist_ok=True)
+    out = os.path.join(build, "libfortran_records_host.so")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-I", os.path.join(root, "ocotillo_b200", "csrc"),
+                    "-o", out, os.path.join(root, "tests", "fortran_records_host.cpp")], check=True, capture_output=True)
+    h = ctypes.CDLL(out)
+    h.append_fortran_record.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_size_t]
+    return h
+
+
+def test_fortran_record_writer_splits_into_subrecords(record_writer, tmp_path):
+    """The writer the deck uses for its binary outputs, with a small subrecord limit standing in
+    for gfortran's 2147483639 bytes: exact markers of a split record, and every size and limit
+    read back by the reader."""
+    from ocotillo_b200 import read_fortran_records
+    le = lambda v: int(v).to_bytes(4, "little", signed=True)
+    p = tmp_path / "split.bin"
+    assert record_writer.append_fortran_record(str(p).encode(), b"abcdefg", 7, 3) == 0
+    assert p.read_bytes() == (le(-3) + b"abc" + le(3) + le(-3) + b"def" + le(-3) + le(1) + b"g" + le(-1))
+    q = tmp_path / "whole.bin"
+    assert record_writer.append_fortran_record(str(q).encode(), b"abcdefg", 7, 2147483639) == 0
+    assert q.read_bytes() == le(7) + b"abcdefg" + le(7)
+    rng = np.random.default_rng(3)
+    for max_sub in (1, 3, 8, 1000):
+        f = tmp_path / f"m{max_sub}.bin"
+        payloads = [rng.bytes(int(n)) for n in (0, 1, 7, 8, 9, 100, 257)]
+        for b in payloads:
+            assert record_writer.append_fortran_record(str(f).encode(), b, len(b), max_sub) == 0
+        assert read_fortran_records(str(f)) == payloads, max_sub
+    assert record_writer.append_fortran_record(str(tmp_path / "bad.bin").encode(), b"x", 1, 0) == 1
