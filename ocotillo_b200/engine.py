@@ -223,7 +223,7 @@ def read_fortran_records(path):
 def calc_wavelength(w1, w0, nw):
     """Linear grid of continuous_opacity.f90:37-62 (argument order as there)."""
     lib = load_library()
-    wa = np.empty(nw)
+    wa = np.empty(max(int(nw), 0))  # nw < 1 reaches the library's check (OCO_EINVAL)
     rc = lib.oco_calc_wavelength(float(w1), float(w0), int(nw), _ptr(wa))
     if rc:
         raise OcoError(rc, lib.oco_last_error(None).decode())

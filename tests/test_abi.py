@@ -47,6 +47,11 @@ def test_calc_wavelength_without_gpu():
     from ocotillo_b200 import calc_wavelength
     assert list(calc_wavelength(5000.0, 3000.0, 5)) == [3000.0, 3500.0, 4000.0, 4500.0, 5000.0]
     assert list(calc_wavelength(5000.0, 3000.0, 1)) == [3000.0]
+    from ocotillo_b200 import OcoError
+    for nw in (0, -3):
+        with pytest.raises(OcoError) as e:
+            calc_wavelength(5000.0, 3000.0, nw)
+        assert e.value.code == -1
 
 
 def test_create_fails_cleanly_without_gpu():
