@@ -157,8 +157,32 @@ def load_library(path=None):
 def _ptr(a):
     if a is None:
         return None
-    assert a.dtype == np.float64 and a.flags.c_contiguous
+    if not isinstance(a, np.ndarray) or a.dtype != np.float64 or not a.flags.c_contiguous:
+        raise ValueError("need a C-contiguous float64 numpy array")
     return a.ctypes.data_as(_DP)
+
+
+def _need_host(name, a, numel):
+    """A host array handed to the library: C-contiguous float64 of exactly numel elements (a
+    shorter one would be read or written past its end)."""
+    if not isinstance(a, np.ndarray) or a.dtype != np.float64 or not a.flags.c_contiguous:
+        raise ValueError(f"{name}: need a C-contiguous float64 numpy array")
+    if a.size != numel:
+        raise ValueError(f"{name}: {a.size} elements where the block has {numel}")
+
+
+def _need_tensor(name, t, numel, device, dtype=None):
+    """A device array handed to a kernel: a contiguous CUDA tensor of exactly numel elements of
+    dtype (float64 by default) on the context's device.  A wrong size would let the kernel read
+    or write past the caller's allocation, so it is refused here, before anything is launched."""
+    import torch
+    dtype = dtype or torch.float64
+    if t.numel() != numel:
+        raise ValueError(f"{name}: {t.numel()} elements where the block has {numel}")
+    if t.dtype != dtype or not t.is_contiguous():
+        raise ValueError(f"{name}: need a contiguous {dtype} tensor")
+    if not t.is_cuda or t.device.index != int(device):
+        raise ValueError(f"{name}: need a tensor on cuda:{int(device)}")
 
 
 def format_e(v, w=15, d=5):
@@ -278,6 +302,8 @@ class Engine:
         are returned with out['zero_pivot'] = True instead."""
         rho = np.ascontiguousarray(rho, dtype=np.float64)
         T = np.ascontiguousarray(T, dtype=np.float64)
+        if rho.ndim != 3 or T.shape != rho.shape:
+            raise ValueError(f"rho and T: need one shape (nx, ny, nz), got {rho.shape} and {T.shape}")
         nx, ny, nz = rho.shape
         nw = 1 if lgrey else self.nw
         out = dict(out or {})
@@ -286,6 +312,10 @@ class Engine:
         for k in set(want):
             if k not in out:
                 out[k] = np.empty(shapes[k])
+        if nw >= 1:  # without wavelength tables the library reports OCO_ENOWAVES
+            for k in shapes:
+                if out.get(k) is not None:
+                    _need_host(k, out[k], int(np.prod(shapes[k])))
         prm = self.params(rho.shape, nw, dz, fully_ionized_T, lgrey, sigma_grey, form)
         rc = self.lib.oco_solve_block(self.ctx, ctypes.byref(prm), _ptr(rho), _ptr(T), _ptr(out.get("U")),
                                       _ptr(out.get("kappa")), _ptr(out.get("V")), _ptr(out.get("Vtop")),
@@ -301,10 +331,20 @@ class Engine:
         (default: torch's current stream).  `out` maps any of 'U', 'kappa', 'V', 'Vtop', 'Vbot'
         to preallocated tensors of the layout's shapes (absent names are not stored)."""
         import torch
+        if rho.dim() != 3:
+            raise ValueError(f"rho: need shape (nx, ny, nz), got {tuple(rho.shape)}")
         nx, ny, nz = rho.shape
         nw = 1 if lgrey else self.nw
-        for t in [rho, T] + [v for v in out.values() if v is not None]:
-            assert t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()
+        cols = nx * ny
+        _need_tensor("rho", rho, cols * nz, self.device)
+        _need_tensor("T", T, cols * nz, self.device)
+        sizes = {"U": nw * cols * (nz + 6), "kappa": nw * cols * nz, "V": nw * cols * nz, "Vtop": nw * cols,
+                 "Vbot": nw * cols}
+        for k, v in out.items():
+            if k not in sizes:
+                raise ValueError(f"out: unknown array {k!r} (U, kappa, V, Vtop, Vbot)")
+            if v is not None and nw >= 1:  # without wavelength tables the library reports OCO_ENOWAVES
+                _need_tensor(k, v, sizes[k], self.device)
         if stream is None:
             stream = torch.cuda.current_stream(rho.device)
         prm = self.params(rho.shape, nw, dz, fully_ionized_T, lgrey, sigma_grey, form, layout)
@@ -327,6 +367,13 @@ class Engine:
         shape (nx, ny, nz) with nw wavelengths; `out` maps 'Ip' and/or 'Im' to tensors shaped
         like V."""
         import torch
+        nx, ny, nz = shape
+        n = nw * nx * ny * nz
+        _need_tensor("U", U, nw * nx * ny * (nz + 6), self.device)
+        _need_tensor("V", V, n, self.device)
+        for k in ("Ip", "Im"):
+            if out.get(k) is not None:
+                _need_tensor(k, out[k], n, self.device)
         if stream is None:
             stream = torch.cuda.current_stream(U.device)
         prm = self.params(shape, nw, 1.0, layout=layout)
@@ -340,10 +387,20 @@ class Engine:
         """tau = cumsum_z(kappa rho dz) and the photosphere index (first z with tau >= target,
         -1 if none) on torch CUDA tensors of a solved block; rho (nx, ny, nz)."""
         import torch
-        if stream is None:
-            stream = torch.cuda.current_stream(kappa.device)
+        if rho.dim() != 3:
+            raise ValueError(f"rho: need shape (nx, ny, nz), got {tuple(rho.shape)}")
         nx, ny, nz = rho.shape
         nw = kappa.numel() // (nx * ny * nz)
+        if nw < 1 or kappa.numel() != nw * nx * ny * nz:
+            raise ValueError(f"kappa: {kappa.numel()} elements is not nw * {nx * ny * nz} for the block of rho")
+        _need_tensor("kappa", kappa, kappa.numel(), self.device)
+        _need_tensor("rho", rho, nx * ny * nz, self.device)
+        if tau is not None:
+            _need_tensor("tau", tau, kappa.numel(), self.device)
+        if photo is not None:
+            _need_tensor("photo", photo, nw * nx * ny, self.device, dtype=torch.int32)
+        if stream is None:
+            stream = torch.cuda.current_stream(kappa.device)
         prm = self.params((nx, ny, nz), nw, dz, layout=layout)
         p = lambda t: ctypes.c_void_p(t.data_ptr()) if t is not None else None
         self._check(self.lib.oco_optical_depth_device(self.ctx, ctypes.byref(prm), p(kappa), p(rho), float(target_tau),
@@ -354,12 +411,16 @@ class Engine:
         grid, lambda in cm) of an emergent-flux plane V (nw, nx, ny) on the device, as a
         (nx, ny) float64 tensor."""
         import torch
-        if stream is None:
-            stream = torch.cuda.current_stream(V.device)
         nx, ny = shape[0], shape[1]
         nw = V.numel() // (nx * ny)
+        if nw < 1 or V.numel() != nw * nx * ny:
+            raise ValueError(f"V: {V.numel()} elements is not nw * {nx * ny} for a ({nx}, {ny}) plane")
+        _need_tensor("V", V, V.numel(), self.device)
         if out is None:
             out = torch.empty((nx, ny), dtype=torch.float64, device=V.device)
+        _need_tensor("out", out, nx * ny, self.device)
+        if stream is None:
+            stream = torch.cuda.current_stream(V.device)
         prm = self.params((nx, ny, 2), nw, 1.0)
         self._check(self.lib.oco_integrated_flux_device(self.ctx, ctypes.byref(prm), ctypes.c_void_p(V.data_ptr()),
                                                         ctypes.c_void_p(out.data_ptr()),
@@ -554,20 +615,24 @@ class Server:
             raise OcoError(rc, self.lib.oco_server_last_error().decode())
 
     @staticmethod
-    def _addr(a):
+    def _addr(name, a):
         if isinstance(a, np.ndarray):
-            assert a.dtype == np.float64 and a.flags.c_contiguous
+            if a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError(f"{name}: need a C-contiguous float64 numpy array")
             return a.ctypes.data
-        assert a.is_cuda and a.is_contiguous() and str(a.dtype) == "torch.float64"
+        if not (getattr(a, "is_cuda", False) and a.is_contiguous() and str(a.dtype) == "torch.float64"):
+            raise ValueError(f"{name}: need a C-contiguous float64 numpy array or contiguous float64 CUDA tensor")
         return a.data_ptr()
 
     def submit(self, rho, T, waves, dz, form="mixed", fully_ionized_T=2e4, want_fields=False):
         """Queues a job; returns its id.  rho and T are referenced until the job is fetched."""
+        if len(rho.shape) != 3 or tuple(T.shape) != tuple(rho.shape):
+            raise ValueError(f"rho and T: need one shape (nx, ny, nz), got {tuple(rho.shape)} and {tuple(T.shape)}")
         nx, ny, nz = rho.shape
         w = np.ascontiguousarray(np.atleast_1d(waves), dtype=np.float64)
         job = OcoJob(nx, ny, nz, w.size, float(dz), float(fully_ionized_T),
                      _FORMS[form] if isinstance(form, str) else int(form), int(bool(want_fields)),
-                     self._addr(rho), self._addr(T), w.ctypes.data)
+                     self._addr("rho", rho), self._addr("T", T), w.ctypes.data)
         jid = ctypes.c_int64()
         self._check(self.lib.oco_server_submit(self.h, ctypes.byref(job), ctypes.byref(jid)))
         self._jobs[jid.value] = (rho, T, (nx, ny, nz, w.size), bool(want_fields))
