@@ -217,7 +217,8 @@ class Grid:
         self.T = torch.from_numpy(self.T_h).to(dev).reshape(self.ncol, nz)
         self.layout = LAYOUT_REFERENCE if a.layout == "reference" else LAYOUT_LAMBDA_FASTEST
         self.CH = min(a.chunk_cols, self.ncol)
-        assert self.ncol % self.CH == 0, "chunk must divide the grid"
+        if self.ncol % self.CH:
+            raise SystemExit(f"--chunk-cols {self.CH} must divide the grid's {self.ncol} columns")
         self.nchunk = self.ncol // self.CH
         mk = lambda shape: torch.empty(shape, dtype=torch.float64, device=dev)
         CH, mz = self.CH, self.mz
@@ -372,7 +373,8 @@ def intensity_error(g, form_a="mixed", form_b="stable"):
     """Relative difference of the mean intensity U (every z, ghost zones included, every item)
     of form_a against form_b on a grid that fits one chunk (its fields stay on the device)."""
     import torch
-    assert g.nchunk == 1
+    if g.nchunk != 1:
+        raise ValueError("intensity_error: the grid must fit one chunk")
 
     def field(form):
         g.step(form, fields=True)
