@@ -48,6 +48,8 @@ def solve_sharded(solve, rho, T, rank, world, group=None):
     rank as numpy arrays."""
     import torch
     nx, ny, _ = rho.shape
+    if nx * ny < world:  # every rank sees the same shapes, so all refuse before any collective
+        raise ValueError(f"{nx * ny} columns cannot give each of {world} ranks one")
     r, t, _ = local_columns(rho, T, rank, world)
     out = solve(r, t)
     res = {}

@@ -69,6 +69,22 @@ def test_column_range_partitions():
             assert rs[0][0] == 0 and rs[-1][1] == ncol
             assert all(a[1] == b[0] for a, b in zip(rs, rs[1:]))
             assert max(c1 - c0 for c0, c1 in rs) - min(c1 - c0 for c0, c1 in rs) <= 1
+    with pytest.raises(ValueError):
+        column_range(10, 2, 2)
+
+
+def test_more_ranks_than_columns_refused_before_any_collective():
+    """A rank without columns could not join the gather with a plane of the right height, so
+    every rank refuses (no process group needed: nothing collective has started)."""
+    from ocotillo_b200.shard import solve_sharded
+    rho = np.ones((1, 3, 8))
+
+    def solve(r, t):
+        raise AssertionError("must not be reached")
+
+    for rank in range(4):
+        with pytest.raises(ValueError, match="3 columns"):
+            solve_sharded(solve, rho, rho, rank, 4)
 
 
 def test_sharded_solve_matches_single_solve():
