@@ -16,6 +16,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -222,22 +223,18 @@ void oco::fill_mixed_lambda_table(const double *tab, int nw, float *tab32) {
   }
 }
 
-extern "C" int oco_set_wavelengths(oco_ctx *c, const double *wa, int32_t nw) {
+/* Every host table is built before the context changes, so a failed host allocation leaves
+ * the previous grid in place. */
+static int set_wavelengths(oco_ctx *c, const double *wa, int32_t nw) {
   if (!c) return oco_set_err(nullptr, OCO_EINVAL, "oco_set_wavelengths: NULL context");
   if (!wa || nw < 1) return oco_set_err(c, OCO_EINVAL, "oco_set_wavelengths: nw < 1 or NULL wa");
   for (int i = 0; i < nw; i++)
     if (!(wa[i] > 0.0) || !std::isfinite(wa[i]))
       return oco_set_err(c, OCO_EINVAL, "oco_set_wavelengths: wavelength %d is not positive", i);
-  CU(cudaSetDevice(c->device));
   std::vector<double> tab((size_t)NL * nw, 0.0);
   fill_lambda_table(wa, nw, tab.data());
-  CU(cudaStreamSynchronize(c->stream));
   std::vector<float> tab32((size_t)mx::MLN * nw);
   fill_mixed_lambda_table(tab.data(), nw, tab32.data());
-  CU(c->lam.ensure(tab.size() * sizeof(double)));
-  CU(cudaMemcpy(c->lam.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
-  CU(c->lam32.ensure(tab32.size() * sizeof(float)));
-  CU(cudaMemcpy(c->lam32.p, tab32.data(), tab32.size() * sizeof(float), cudaMemcpyHostToDevice));
   /* trapezoid weights over the grid as given (cm): w_i = (wa_{i+1} - wa_{i-1}) / 2, halved
    * differences at the ends; a single wavelength integrates to 0 */
   std::vector<double> tw((size_t)nw, 0.0);
@@ -246,11 +243,26 @@ extern "C" int oco_set_wavelengths(oco_ctx *c, const double *wa, int32_t nw) {
     tw[(size_t)i] += h;
     tw[(size_t)i + 1] += h;
   }
+  std::vector<double> wcopy(wa, wa + nw);
+  CU(cudaSetDevice(c->device));
+  CU(cudaStreamSynchronize(c->stream));
+  CU(c->lam.ensure(tab.size() * sizeof(double)));
+  CU(cudaMemcpy(c->lam.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CU(c->lam32.ensure(tab32.size() * sizeof(float)));
+  CU(cudaMemcpy(c->lam32.p, tab32.data(), tab32.size() * sizeof(float), cudaMemcpyHostToDevice));
   CU(c->trapw.ensure(tw.size() * sizeof(double)));
   CU(cudaMemcpy(c->trapw.p, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice));
-  c->wa.assign(wa, wa + nw);
+  c->wa.swap(wcopy);
   c->nw = nw;
   return OCO_OK;
+}
+
+extern "C" int oco_set_wavelengths(oco_ctx *c, const double *wa, int32_t nw) {
+  try {
+    return set_wavelengths(c, wa, nw);
+  } catch (const std::bad_alloc &) {
+    return oco_set_err(c, OCO_ENOMEM, "oco_set_wavelengths: out of host memory for %d wavelengths", nw);
+  }
 }
 
 static int check_params(oco_ctx *c, const oco_params *p) {

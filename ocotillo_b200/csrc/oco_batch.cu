@@ -25,6 +25,7 @@
 #include <cmath>
 #include <map>
 #include <memory>
+#include <new>
 #include <numeric>
 #include <utility>
 #include <vector>
@@ -175,9 +176,8 @@ static int check_status(oco_batch *b, bool report_pivots = true) {
   return OCO_OK;
 }
 
-extern "C" int oco_batch_create(oco_ctx *c, const oco_batch_column *cols, int64_t ncol, const double *waves,
-                                int64_t nwaves, int32_t form, int32_t layout, double fully_ionized_T,
-                                oco_batch **out) {
+static int batch_create(oco_ctx *c, const oco_batch_column *cols, int64_t ncol, const double *waves, int64_t nwaves,
+                        int32_t form, int32_t layout, double fully_ionized_T, oco_batch **out) {
   if (!c) return oco_set_err(nullptr, OCO_EINVAL, "oco_batch_create: NULL context");
   if (!out) return oco_set_err(c, OCO_EINVAL, "oco_batch_create: out is NULL");
   *out = nullptr;
@@ -337,6 +337,19 @@ extern "C" int oco_batch_create(oco_ctx *c, const oco_batch_column *cols, int64_
   b->info.max_nw = b->max_nw;
   *out = guard.release();
   return OCO_OK;
+}
+
+/* Host work lists grow with ncol and nw: a failed allocation is OCO_ENOMEM (the partly built
+ * batch is released by its guard while the exception unwinds), never an exception through
+ * the C ABI. */
+extern "C" int oco_batch_create(oco_ctx *c, const oco_batch_column *cols, int64_t ncol, const double *waves,
+                                int64_t nwaves, int32_t form, int32_t layout, double fully_ionized_T,
+                                oco_batch **out) {
+  try {
+    return batch_create(c, cols, ncol, waves, nwaves, form, layout, fully_ionized_T, out);
+  } catch (const std::bad_alloc &) {
+    return oco_set_err(c, OCO_ENOMEM, "oco_batch_create: out of host memory for %lld columns", (long long)ncol);
+  }
 }
 
 extern "C" int oco_batch_bind(oco_batch *b, const double *rho, const double *T, int64_t n_in, double *U, int64_t n_u,

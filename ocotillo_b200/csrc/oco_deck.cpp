@@ -18,7 +18,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
 #include <map>
+#include <memory>
+#include <new>
 #include <string>
 #include <sys/stat.h>
 #include <vector>
@@ -304,6 +307,9 @@ int load_deck(const char *deck_dir, const char *snapshot, Deck &d) {
   d.snapshot = (snapshot && snapshot[0]) ? snapshot : "0000";
   std::map<std::string, long> rv;
   if (!resolution(d.dir + "/resolution.in", rv)) return derr(OCO_EIO, "cannot read %s/resolution.in", d.dir.c_str());
+  for (const auto &kv : rv)
+    if (kv.second < INT32_MIN || kv.second > INT32_MAX)
+      return derr(OCO_EDIM, "resolution.in: %s = %ld is out of range", kv.first.c_str(), kv.second);
   d.nw = (int)rget(rv, "nw", 0);
   d.nx = (int)rget(rv, "nx", 0);
   d.ny = (int)rget(rv, "ny", 0);
@@ -317,6 +323,8 @@ int load_deck(const char *deck_dir, const char *snapshot, Deck &d) {
   d.nyloc = (int)rget(rv, "nyloc", d.ny / d.nprocy);
   if (d.nw < 1 || d.nz < 2 || d.nxloc < 1 || d.nyloc < 1)
     return derr(OCO_EDIM, "resolution.in: need nw >= 1, nz >= 2, nxloc, nyloc >= 1");
+  if ((double)d.nxloc * d.nyloc * d.nw * (d.nz + 6.0) > 72057594037927936.0) /* the library's 2^56 limit */
+    return derr(OCO_EDIM, "resolution.in: nxloc*nyloc*nw*(nz+6) exceeds 2^56 elements");
   std::string text;
   if (!slurp(d.dir + "/input.in", text)) return derr(OCO_EIO, "cannot read %s/input.in", d.dir.c_str());
   Group g;
@@ -570,8 +578,8 @@ extern "C" void oco_format_e(double v, int32_t w, int32_t d, char *out) {
   memcpy(out + pad, body.c_str(), body.size() + 1);
 }
 
-extern "C" int oco_deck_block_inputs(const char *deck_dir, const char *snapshot, int32_t iprocx, int32_t iprocy,
-                                     oco_deck_info *info, double *rho, double *T, double *wa, double *z) {
+static int deck_block_inputs(const char *deck_dir, const char *snapshot, int32_t iprocx, int32_t iprocy,
+                             oco_deck_info *info, double *rho, double *T, double *wa, double *z) {
   if (!info) return derr(OCO_EINVAL, "oco_deck_block_inputs: info is NULL");
   Deck d;
   int rc = load_deck(deck_dir, snapshot, d);
@@ -596,8 +604,8 @@ extern "C" int oco_deck_block_inputs(const char *deck_dir, const char *snapshot,
   return OCO_OK;
 }
 
-extern "C" int oco_run_deck(const char *deck_dir, const char *snapshot, const char *out_dir, int32_t form,
-                            int32_t device, int32_t write_binary) {
+static int run_deck(const char *deck_dir, const char *snapshot, const char *out_dir, int32_t form, int32_t device,
+                    int32_t write_binary) {
   Deck d;
   int rc = load_deck(deck_dir, snapshot, d);
   if (rc) return rc;
@@ -608,11 +616,8 @@ extern "C" int oco_run_deck(const char *deck_dir, const char *snapshot, const ch
   if (!make_dirs(out)) return derr(OCO_EIO, "cannot create %s", out.c_str());
   oco_ctx *ctx = nullptr;
   if ((rc = oco_create(&ctx, device))) return derr(rc, "%s", oco_last_error(nullptr));
-  if (!d.lgrey && (rc = oco_set_wavelengths(ctx, d.wa.data(), d.nw))) {
-    derr(rc, "%s", oco_last_error(ctx));
-    oco_destroy(ctx);
-    return rc;
-  }
+  const std::unique_ptr<oco_ctx, void (*)(oco_ctx *)> ctx_guard(ctx, oco_destroy); /* every return path */
+  if (!d.lgrey && (rc = oco_set_wavelengths(ctx, d.wa.data(), d.nw))) return derr(rc, "%s", oco_last_error(ctx));
   const int nz = d.nz, nw = d.nw, mz = nz + 2 * kNg;
   const size_t ncol = (size_t)d.nxloc * d.nyloc;
   std::vector<double> rho(ncol * nz), T(ncol * nz), z((size_t)mz, 0.0);
@@ -695,8 +700,31 @@ extern "C" int oco_run_deck(const char *deck_dir, const char *snapshot, const ch
       }
     }
   }
-  oco_destroy(ctx);
   return rc ? rc : zero_pivot_rc;
+}
+
+/* The C entry points: host allocations sized by the deck can fail, and an exception must not
+ * cross the C ABI, so it becomes an error code. */
+extern "C" int oco_deck_block_inputs(const char *deck_dir, const char *snapshot, int32_t iprocx, int32_t iprocy,
+                                     oco_deck_info *info, double *rho, double *T, double *wa, double *z) {
+  try {
+    return deck_block_inputs(deck_dir, snapshot, iprocx, iprocy, info, rho, T, wa, z);
+  } catch (const std::bad_alloc &) {
+    return derr(OCO_ENOMEM, "oco_deck_block_inputs: out of host memory");
+  } catch (const std::exception &e) {
+    return derr(OCO_EINVAL, "oco_deck_block_inputs: %s", e.what());
+  }
+}
+
+extern "C" int oco_run_deck(const char *deck_dir, const char *snapshot, const char *out_dir, int32_t form,
+                            int32_t device, int32_t write_binary) {
+  try {
+    return run_deck(deck_dir, snapshot, out_dir, form, device, write_binary);
+  } catch (const std::bad_alloc &) {
+    return derr(OCO_ENOMEM, "oco_run_deck: out of host memory");
+  } catch (const std::exception &e) {
+    return derr(OCO_EINVAL, "oco_run_deck: %s", e.what());
+  }
 }
 
 extern "C" const char *oco_deck_last_error(void) { return g_deck_err.c_str(); }

@@ -28,8 +28,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <deque>
+#include <exception>
 #include <memory>
 #include <mutex>
+#include <new>
 #include <string>
 #include <thread>
 #include <unordered_map>
@@ -397,12 +399,19 @@ extern "C" int oco_server_create(const oco_server_config *cfg, oco_server **out)
   srv->device = cfg->device;
   if (cfg->chunk_points > 0) srv->chunk_points = cfg->chunk_points;
   if (const char *t = getenv("OCO_SERVER_TRACE")) srv->trace = t[0] == '1';
-  const int rc = setup_server(srv, cfg);
+  int rc;
+  try { /* host allocations grow with max_jobs; thread creation can fail */
+    rc = setup_server(srv, cfg);
+    if (!rc) srv->th = std::thread([srv] { srv->loop(); });
+  } catch (const std::bad_alloc &) {
+    rc = serr(OCO_ENOMEM, "oco_server_create: out of host memory");
+  } catch (const std::exception &e) {
+    rc = serr(OCO_EINVAL, "oco_server_create: %s", e.what());
+  }
   if (rc) {
     free_server(srv);
     return rc;
   }
-  srv->th = std::thread([srv] { srv->loop(); });
   *out = srv;
   return OCO_OK;
 }
@@ -419,7 +428,13 @@ extern "C" int oco_server_submit(oco_server *s, const oco_job *job, int64_t *job
       return serr(OCO_EINVAL, "oco_server_submit: wavelength %d is not positive and finite", i);
   if (job->form != OCO_FORM_PLAIN && job->form != OCO_FORM_STABLE && job->form != OCO_FORM_MIXED)
     return serr(OCO_EINVAL, "oco_server_submit: unknown form %d", job->form);
-  auto j = std::make_unique<Job>();
+  std::unique_ptr<Job> j;
+  try {
+    j = std::make_unique<Job>();
+    j->waves.assign(job->waves, job->waves + job->nw);
+  } catch (const std::bad_alloc &) {
+    return serr(OCO_ENOMEM, "oco_server_submit: out of host memory");
+  }
   j->p.nx = job->nx;
   j->p.ny = job->ny;
   j->p.nz = job->nz;
@@ -433,18 +448,28 @@ extern "C" int oco_server_submit(oco_server *s, const oco_job *job, int64_t *job
   j->want_fields = job->want_fields ? 1 : 0;
   j->rho_in = job->rho;
   j->T_in = job->T;
-  j->waves.assign(job->waves, job->waves + job->nw);
   j->bytes = footprint(j->p, j->want_fields, &j->input_bytes);
   std::lock_guard<std::mutex> g(s->mu);
   if (s->closing) return serr(OCO_ECLOSED, "oco_server_submit: the server is shutting down");
   if ((double)j->bytes > s->budget)
     return serr(OCO_EADMIT, "oco_server_submit: footprint %.3g GB exceeds the admission budget %.3g GB",
                 (double)j->bytes / 1e9, s->budget / 1e9);
-  j->id = s->next_id++;
+  const int64_t id = s->next_id;
+  j->id = id;
   j->t_submit = now_s();
-  *job_id = j->id;
-  s->queue.push_back(j.get());
-  s->jobs.emplace(j->id, std::move(j));
+  try { /* the job table owns the job before the queue refers to it, and loses it if queueing fails */
+    auto it = s->jobs.emplace(id, std::move(j)).first;
+    try {
+      s->queue.push_back(it->second.get());
+    } catch (...) {
+      s->jobs.erase(it);
+      throw;
+    }
+  } catch (const std::bad_alloc &) {
+    return serr(OCO_ENOMEM, "oco_server_submit: out of host memory");
+  }
+  s->next_id++;
+  *job_id = id;
   s->cv.notify_all();
   return OCO_OK;
 }

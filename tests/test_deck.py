@@ -1,6 +1,6 @@
 """The deck layer (input construction, Ew.d editing, Fortran records) on the CPU, against the
 oracle's restatement of the reference's driver: the same bytes for every deck's root-block
-inputs, the same text for every formatted value."""
+inputs, the same text for every formatted value; and its refusals of bad decks as error codes."""
 import os
 import shutil
 
@@ -107,3 +107,39 @@ def test_fortran_record_writer_splits_into_subrecords(record_writer, tmp_path):
             assert record_writer.append_fortran_record(str(f).encode(), b, len(b), max_sub) == 0
         assert read_fortran_records(str(f)) == payloads, max_sub
     assert record_writer.append_fortran_record(str(tmp_path / "bad.bin").encode(), b"x", 1, 0) == 1
+
+
+@pytest.mark.parametrize("edit,what", [("nz=10", "nz=3000000000"), ("nx=1,ny=1,nz=10", "nx=16777216,ny=16777216,nz=4096"),
+                                       ("nw=2", "nw=-5")])
+def test_deck_refuses_out_of_range_resolution(tmp_path, edit, what):
+    """Dimensions beyond int32, beyond the library's 2^56-element block limit, or negative come
+    back as OCO_EDIM before anything is allocated."""
+    from ocotillo_b200 import OcoError, deck_block_inputs
+    d = tmp_path / "agn"
+    shutil.copytree(os.path.join(SAMPLES, "NongreyAGN"), d)
+    txt = open(d / "resolution.in").read()
+    assert edit in txt
+    open(d / "resolution.in", "w").write(txt.replace(edit, what))
+    with pytest.raises(OcoError) as e:
+        deck_block_inputs(str(d))
+    assert e.value.code == -10, e.value
+
+
+def test_run_deck_without_gpu_fails_cleanly(tmp_path):
+    """Without a device the deck run reads the deck, creates the output folder and returns the
+    context's error code (no exception crosses the C ABI, nothing is left behind but the folder)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from ocotillo_b200 import OcoError, run_deck
+    with pytest.raises(OcoError) as e:
+        run_deck(os.path.join(SAMPLES, "NongreyAGN"), out_dir=str(tmp_path / "out"))
+    assert e.value.code == -5
+    assert os.listdir(tmp_path / "out") == []
+    d = tmp_path / "agn"
+    shutil.copytree(os.path.join(SAMPLES, "NongreyAGN"), d)
+    txt = open(d / "resolution.in").read().replace("nz=10", "nz=1")
+    open(d / "resolution.in", "w").write(txt)
+    with pytest.raises(OcoError) as e:
+        run_deck(str(d), out_dir=str(tmp_path / "out2"))
+    assert e.value.code == -10
