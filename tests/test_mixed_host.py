@@ -69,3 +69,22 @@ def test_mixed_host_against_stable_oracle(host_lib, oracle, case):
     assert rel(U, rU).max() <= 5e-4
     for end in (-1, 0):
         assert rel(V[..., end], rV[..., end]).max() <= 1e-4, end
+
+
+@pytest.mark.parametrize("rho0", [1e-11, 1e-9, 1e-7])
+def test_mixed_host_across_precision_config_densities(host_lib, oracle, rho0):
+    """The precision workload draws rho0 log-uniform in [1e-11, 1e-7]: its ends and middle, at the
+    mixed form's tolerances against the stable FP64 oracle."""
+    from ocotillo_b200 import workloads
+    rho, T, dz = workloads.agn_block(2, 2, 160, seed=41, rho0=rho0)
+    wa = workloads.log_wavelengths(48)
+    nx, ny, nz = rho.shape
+    nw = len(wa)
+    U, K, V = _solve(host_lib, rho.reshape(-1, nz), T.reshape(-1, nz), wa, dz)
+    ref = oracle.solve_block(rho, T, wa, dz, form=oracle.FORM_STABLE, backend="ocomath")
+    rel = lambda a, b: np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
+    assert rel(K, ref["kappa"].reshape(nw, nx * ny, nz)).max() <= 3e-5
+    assert rel(U, ref["U"].reshape(nw, nx * ny, nz + 6)).max() <= 5e-4
+    rV = ref["V"].reshape(nw, nx * ny, nz)
+    for end in (-1, 0):
+        assert rel(V[..., end], rV[..., end]).max() <= 1e-4, end
