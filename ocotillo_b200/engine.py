@@ -523,7 +523,15 @@ class Batch:
         return {k: torch.empty(n[k], dtype=torch.float64, device=device) for k in want}
 
     def bind(self, rho, T, out):
-        """Binds device inputs (dense rho, T) and outputs (dict of U, kappa, V, Vtop, Vbot)."""
+        """Binds device inputs (dense rho, T) and outputs (dict of U, kappa, V, Vtop, Vbot).
+        The library checks every column's range against the element counts passed here; the
+        arrays themselves must be float64 CUDA tensors on the engine's device."""
+        for k in out:
+            if k not in ("U", "kappa", "V", "Vtop", "Vbot"):
+                raise ValueError(f"out: unknown array {k!r} (U, kappa, V, Vtop, Vbot)")
+        for name, t in (("rho", rho), ("T", T)) + tuple(out.items()):
+            if t is not None:
+                _need_tensor(name, t, t.numel(), self.eng.device)
         o = self.offsets
 
         def p(t):

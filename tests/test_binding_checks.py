@@ -84,3 +84,18 @@ def test_server_submit_refuses_mismatched_inputs():
         s.submit(np.ones((2, 2, 8)), np.ones((2, 2, 9)), [5000.0], 1e13)
     with pytest.raises(ValueError, match="C-contiguous float64"):
         s.submit(np.ones((2, 2, 8), dtype=np.float32), np.ones((2, 2, 8)), [5000.0], 1e13)
+
+
+def test_batch_bind_refuses_host_and_float32_tensors(eng):
+    """The library bounds every column's range by the element counts it is given, which are
+    only meaningful for float64 device arrays: anything else is refused in the binding."""
+    from ocotillo_b200.engine import Batch
+    b = Batch.__new__(Batch)
+    b.eng, b.lib, b.offsets = eng, eng.lib, None
+    x = torch.ones(64, dtype=torch.float64)
+    with pytest.raises(ValueError, match="rho: need a tensor on cuda:0"):
+        b.bind(x, x, {})
+    with pytest.raises(ValueError, match="rho: need a contiguous torch.float64"):
+        b.bind(x.float(), x, {})
+    with pytest.raises(ValueError, match="unknown array 'Vtp'"):
+        b.bind(x, x, {"Vtp": x})
