@@ -143,3 +143,23 @@ def test_run_deck_without_gpu_fails_cleanly(tmp_path):
     with pytest.raises(OcoError) as e:
         run_deck(str(d), out_dir=str(tmp_path / "out2"))
     assert e.value.code == -10
+
+
+def test_deck_executable_arguments_and_errors(tmp_path):
+    """The command-line driver: a bad form or option exits 2 with its usage, a deck that cannot
+    be read exits 1 with the library's message, and without a device the run exits 1 after
+    reading the deck."""
+    import subprocess
+    import ocotillo_b200
+    exe = os.path.join(os.path.dirname(ocotillo_b200.__file__), "flux_feautrier_b200")
+    run = lambda *args: subprocess.run([exe, *args], capture_output=True, text=True, timeout=120)
+    r = run("--form", "quad")
+    assert r.returncode == 2 and "unknown form quad" in r.stderr
+    r = run("--bogus")
+    assert r.returncode == 2 and "usage:" in r.stderr
+    r = run("--deck", str(tmp_path))
+    assert r.returncode == 1 and "resolution.in" in r.stderr
+    import torch
+    if not torch.cuda.is_available():
+        r = run("--deck", os.path.join(SAMPLES, "NongreyAGN"), "--out", str(tmp_path / "out"))
+        assert r.returncode == 1 and r.stderr.strip()
