@@ -195,3 +195,17 @@ def test_ctypes_signatures_match_the_header():
         assert _py_kind(f.restype) == _c_kind(ret), name
         seen += 1
     assert seen == len(declared_functions())
+
+
+def test_server_create_refuses_bad_config_and_fails_cleanly_without_gpu():
+    from ocotillo_b200 import OcoError, Server
+    for kw in ({"max_jobs": 0}, {"max_nz": -1}, {"budget_bytes": -1.0}, {"chunk_points": -5},
+               {"reserve_bytes": -1.0}):
+        with pytest.raises(OcoError) as e:
+            Server(0, **kw)
+        assert e.value.code == -1, kw
+    import torch
+    if not torch.cuda.is_available():
+        with pytest.raises(OcoError) as e:
+            Server(0, max_jobs=2)
+        assert e.value.code == -5
