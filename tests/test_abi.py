@@ -1,5 +1,6 @@
 """The C-ABI library loads without a GPU and exports every function include/*.h declares;
-the ctypes struct matches the C layout; calls that need no device work on the CPU."""
+every ctypes struct and signature matches the header; calls that need no device work on the
+CPU, and argument checks refuse before any device work."""
 import ctypes
 import glob
 import os
