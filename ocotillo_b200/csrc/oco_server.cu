@@ -164,7 +164,12 @@ void oco_server::fail(Job *j, int code, const std::string &msg) {
   j->msg = msg;
   j->inputs_consumed = 1;
   j->t_done = now_s();
-  if (j->slot >= 0) slots[(size_t)j->slot].job = nullptr;
+  if (j->slot >= 0) { /* its events are complete after the synchronize: back to the slot's pool */
+    Slot &sl = slots[(size_t)j->slot];
+    sl.pool.insert(sl.pool.end(), j->inflight.begin(), j->inflight.end());
+    sl.job = nullptr;
+  }
+  j->inflight.clear();
   j->slot = -1;
   cv_done.notify_all();
 }
