@@ -55,3 +55,21 @@ def test_clock_record_summary():
     s = _clocks_from(["0, 1500, 1965, [N/A], 0x0, Active, Not Active, Active, Not Active"])
     assert s["reasons"] == ["hw_slowdown", "sw_thermal_slowdown"] and s["power_w_max"] is None
     assert _clocks_from([])["reasons"] == ["no samples"]
+
+
+def test_reference_arm_under_torchrun_two_ranks():
+    """Launched as the multi-GPU bench is (torchrun, two ranks), rank 0 alone runs the reference
+    arm and prints its one line; the other rank exits 0 without work."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"),
+           "--impl", "reference", "--gpus", "2", "--nx", "2", "--ny", "2", "--steps", "3", "--warmup", "3"]
+    r = subprocess.run(cmd, capture_output=True, text=True, cwd=ROOT, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.strip().startswith("{")]
+    assert len(lines) == 1, r.stdout
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
