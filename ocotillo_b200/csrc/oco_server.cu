@@ -80,6 +80,7 @@ struct Job {
   std::vector<double> waves;
   /* state (guarded by the server mutex) */
   int state = OCO_JOB_QUEUED, error = OCO_OK, inputs_consumed = 0;
+  bool fetching = false; /* one oco_server_fetch owns the done job's arrays */
   std::string msg;
   int64_t bytes = 0, input_bytes = 0;
   double t_submit = 0, t_admit = 0, t_done = 0;
@@ -511,18 +512,8 @@ extern "C" int oco_server_wait(oco_server *s, int64_t id, double timeout_s) {
   return OCO_OK;
 }
 
-extern "C" int oco_server_fetch(oco_server *s, int64_t id, double *Vtop, double *Vbot, double *U, double *kappa,
-                                double *V) {
-  if (!s) return serr(OCO_EINVAL, "oco_server_fetch: NULL server");
-  Job *j = nullptr;
-  {
-    std::lock_guard<std::mutex> g(s->mu);
-    auto it = s->jobs.find(id);
-    if (it == s->jobs.end()) return serr(OCO_EINVAL, "oco_server_fetch: unknown job %lld", (long long)id);
-    j = it->second.get();
-    if (j->state == OCO_JOB_FAILED) return serr(j->error, "job %lld failed: %s", (long long)id, j->msg.c_str());
-    if (j->state != OCO_JOB_DONE) return serr(OCO_EAGAIN, "oco_server_fetch: job %lld not done", (long long)id);
-  }
+/* Copies a done job's results into the caller's host arrays (any may be NULL). */
+static int copy_results(oco_server *s, const Job *j, double *Vtop, double *Vbot, double *U, double *kappa, double *V) {
   const int64_t ncol = (int64_t)j->p.nx * j->p.ny;
   const size_t nfl = (size_t)ncol * j->p.nw * sizeof(double);
   const size_t nkv = (size_t)ncol * j->p.nw * j->p.nz * sizeof(double);
@@ -534,9 +525,31 @@ extern "C" int oco_server_fetch(oco_server *s, int64_t id, double *Vtop, double 
   if (kappa && j->K) SCU(cudaMemcpyAsync(kappa, j->K, nkv, cudaMemcpyDeviceToHost, s->misc));
   if (V && j->V) SCU(cudaMemcpyAsync(V, j->V, nkv, cudaMemcpyDeviceToHost, s->misc));
   SCU(cudaStreamSynchronize(s->misc));
-  if ((U && !j->U) || (kappa && !j->K) || (V && !j->V))
+  return OCO_OK;
+}
+
+extern "C" int oco_server_fetch(oco_server *s, int64_t id, double *Vtop, double *Vbot, double *U, double *kappa,
+                                double *V) {
+  if (!s) return serr(OCO_EINVAL, "oco_server_fetch: NULL server");
+  Job *j = nullptr;
+  {
+    std::lock_guard<std::mutex> g(s->mu);
+    auto it = s->jobs.find(id);
+    if (it == s->jobs.end()) return serr(OCO_EINVAL, "oco_server_fetch: unknown job %lld", (long long)id);
+    j = it->second.get();
+    if (j->state == OCO_JOB_FAILED) return serr(j->error, "job %lld failed: %s", (long long)id, j->msg.c_str());
+    if (j->state != OCO_JOB_DONE) return serr(OCO_EAGAIN, "oco_server_fetch: job %lld not done", (long long)id);
+    if (j->fetching) return serr(OCO_EAGAIN, "oco_server_fetch: job %lld is being fetched by another call", (long long)id);
+    j->fetching = true;
+  }
+  const int rc = copy_results(s, j, Vtop, Vbot, U, kappa, V);
+  if (!rc && ((U && !j->U) || (kappa && !j->K) || (V && !j->V)))
     serr(OCO_OK, "oco_server_fetch: job %lld kept no fields; only the emergent flux was copied", (long long)id);
   std::lock_guard<std::mutex> g(s->mu);
+  if (rc) { /* the job stays done and fetchable */
+    j->fetching = false;
+    return rc;
+  }
   for (double **p : {&j->Vtop, &j->Vbot, &j->U, &j->K, &j->V})
     if (*p) {
       cudaFreeAsync(*p, s->misc);
