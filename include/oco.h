@@ -341,7 +341,8 @@ int oco_server_wait(oco_server *server, int64_t job_id, double timeout_s);
 
 /* Copies a done job's results into host arrays (reference layout: Vtop, Vbot (ny, nx, nw);
  * U (nz+6, ny, nx, nw), kappa and V (nz, ny, nx, nw) when the job kept its fields; any may be
- * NULL), then releases the job and its device memory. */
+ * NULL), then releases the job and its device memory.  OCO_EAGAIN while the job is not done or
+ * another call is fetching it; a failed copy leaves the job done and fetchable. */
 int oco_server_fetch(oco_server *server, int64_t job_id, double *Vtop, double *Vbot, double *U, double *kappa,
                      double *V);
 
