@@ -402,6 +402,7 @@ extern "C" int oco_batch_tune(oco_batch *b) {
       if (bps >= 1) cands.push_back({t, bps, 0.0f});
     }
   if (cands.size() > 16) cands.resize(16);
+  const int tiling0 = b->tiling, bps0 = b->bps; /* the captured graph's setting, kept on failure */
   int rc = OCO_OK;
   bool warm = false;
   for (auto &k : cands) {
@@ -425,7 +426,11 @@ extern "C" int oco_batch_tune(oco_batch *b) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (rc) return rc;
+  if (rc) {
+    b->tiling = tiling0;
+    b->bps = bps0;
+    return rc;
+  }
   const Cand *best = &cands[0];
   for (auto &k : cands)
     if (k.ms < best->ms) best = &k;
