@@ -261,7 +261,9 @@ int oco_batch_set_tiling(oco_batch *batch, int32_t tiling, int32_t blocks_per_sm
 
 /* Replays the batch's graph on `stream` (a cudaStream_t; NULL is the CUDA default stream):
  * records, then every (column, wavelength) item.  Returns after enqueueing; the bound inputs
- * must stay valid and the outputs untouched until the stream reaches this work. */
+ * must stay valid and the outputs untouched until the stream reaches this work.  Replays share
+ * the batch's work queue, so a replay on another stream than the pending one waits for it on
+ * the device (an event; the host does not block). */
 int oco_batch_run(oco_batch *batch, void *stream);
 
 /* Waits for the last oco_batch_run; returns OCO_ETIMEDOUT if a bounded wait in the kernel

@@ -63,6 +63,7 @@ struct oco_batch {
   cudaGraphExec_t exec = nullptr;
   cudaStream_t last = nullptr;
   bool pending = false;
+  cudaEvent_t after_last = nullptr; /* orders a replay on another stream after the pending one */
   oco_batch_info info{};
 };
 
@@ -468,6 +469,11 @@ extern "C" int oco_batch_run(oco_batch *b, void *stream) {
   if (!b->bound || !b->exec) return oco_set_err(c, OCO_EINVAL, "oco_batch_run: bind the arrays first");
   CU(cudaSetDevice(c->device));
   cudaStream_t s = (cudaStream_t)stream;
+  if (b->pending && b->last != s) { /* replays share the work queue: no overlap across streams */
+    if (!b->after_last) CU(cudaEventCreateWithFlags(&b->after_last, cudaEventDisableTiming));
+    CU(cudaEventRecord(b->after_last, b->last));
+    CU(cudaStreamWaitEvent(s, b->after_last, 0));
+  }
   CU(cudaGraphLaunch(b->exec, s));
   b->last = s;
   b->pending = true;
@@ -497,12 +503,13 @@ extern "C" int oco_batch_get_info(const oco_batch *b, oco_batch_info *info) {
 extern "C" void oco_batch_destroy(oco_batch *b) {
   if (!b) return;
   if (b->c) cudaSetDevice(b->c->device);
-  if (b->pending && b->last) cudaStreamSynchronize(b->last);
+  if (b->pending) cudaStreamSynchronize(b->last); /* a null stream is the default stream */
   if (b->cap) cudaStreamSynchronize(b->cap);
   drop_graph(b);
   for (DevBuf *d : {&b->cols, &b->rec_pre, &b->tasks, &b->order, &b->item_pre, &b->lam, &b->rec, &b->scratch,
                     &b->work, &b->status})
     d->release();
+  if (b->after_last) cudaEventDestroy(b->after_last);
   if (b->cap) cudaStreamDestroy(b->cap);
   delete b;
 }
