@@ -290,6 +290,28 @@ def test_batch_caller_offsets_and_overlap(engine):
     ref.close()
 
 
+def test_batch_replays_alternating_streams(engine):
+    """Replays share the batch's work queue: one on another stream than the pending one is
+    ordered after it on the device, and every replay gives the same bits."""
+    import torch
+    d = _small_batch(seed=13)
+    b, _, _, out = _make(engine, d, 0, form="plain")
+    _run_fp64(b)
+    ref = {k: v.cpu().numpy().copy() for k, v in out.items()}
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    for k in out:
+        out[k].fill_(float("nan"))
+    torch.cuda.synchronize()
+    for _ in range(3):
+        b.run(stream=s1)
+        b.run(stream=s2)
+    _run_fp64(b)
+    torch.cuda.synchronize()
+    for k in out:
+        assert _same(out[k], ref[k]), k
+    b.close()
+
+
 @pytest.mark.parametrize("form,layout", [("plain", 0), ("plain", 1), ("stable", 0), ("stable", 1)])
 def test_batch_fp64_bitwise_block_solve(engine, form, layout):
     d = _small_batch(seed=16)
