@@ -116,7 +116,9 @@ int oco_solve_block(oco_ctx *ctx, const oco_params *p, const double *rho, const 
 /* Same loop on DEVICE arrays (p->layout selects the output layout), enqueued on `stream`
  * (a cudaStream_t; NULL is the CUDA default stream); returns after enqueueing.  Zero pivots are
  * reported by the next oco_synchronize.  Any output may be NULL.  The inputs must stay
- * valid and the outputs untouched until the stream reaches this work. */
+ * valid and the outputs untouched until the stream reaches this work.  The context's work
+ * buffers serve one call at a time: a call on another stream than a pending one waits for it
+ * on the device (an event; the host does not block). */
 int oco_solve_block_device(oco_ctx *ctx, const oco_params *p, const double *rho,
                            const double *T, double *U, double *kappa, double *V,
                            double *Vtop, double *Vbot, void *stream);

@@ -84,6 +84,7 @@ extern "C" int oco_create(oco_ctx **out, int device) {
 extern "C" void oco_destroy(oco_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->device);
+  if (c->status_pending) cudaStreamSynchronize(c->status_stream); /* a device-array call in flight */
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->copy) cudaStreamSynchronize(c->copy);
   c->lam.release();
@@ -114,6 +115,7 @@ extern "C" void oco_destroy(oco_ctx *c) {
       cudaEventDestroy(pr.second);
     }
   for (auto e : c->ev_pool) cudaEventDestroy(e);
+  if (c->order_ev) cudaEventDestroy(c->order_ev);
   delete c;
 }
 
@@ -524,6 +526,13 @@ extern "C" int oco_solve_block_device(oco_ctx *c, const oco_params *p, const dou
   if (!rho || !T) return oco_set_err(c, OCO_EINVAL, "rho and T are required");
   CU(cudaSetDevice(c->device));
   cudaStream_t s = (cudaStream_t)stream; /* NULL is the CUDA default stream */
+  if (c->status_pending && c->status_stream != s) {
+    /* the context's records, Thomas scratch and status serve one call at a time: a call on
+       another stream waits for the pending one on the device (the host does not block) */
+    if (!c->order_ev) CU(cudaEventCreateWithFlags(&c->order_ev, cudaEventDisableTiming));
+    CU(cudaEventRecord(c->order_ev, c->status_stream));
+    CU(cudaStreamWaitEvent(s, c->order_ev, 0));
+  }
   const int64_t ncol = (int64_t)p->nx * p->ny;
   const int64_t ch = chunk_columns(c, p, false, U != nullptr, kappa != nullptr, V != nullptr, Vtop || Vbot);
   CU(c->pil.ensure((size_t)ch * p->nz * record_bytes(p->form)));

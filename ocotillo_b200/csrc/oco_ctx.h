@@ -71,6 +71,7 @@ struct oco_ctx {
   bool status_pending = false;
   cudaStream_t status_stream = nullptr;
   oco_params status_params{};
+  cudaEvent_t order_ev = nullptr; /* orders a device call on another stream after the pending one */
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_solve, ev_pil;
   cudaEvent_t take_event() {

@@ -173,3 +173,30 @@ def test_chunked_solve_matches_single_chunk(engine, monkeypatch):
     small.close()
     for k in ("U", "kappa", "V", "Vtop", "Vbot"):
         assert_bitwise(a[k], b[k], k)
+
+
+def test_device_entry_alternating_streams(engine, oracle):
+    """Device-array calls share the context's records, scratch and layout temporaries: a call
+    on another stream than the pending one is ordered after it on the device, so calls
+    alternating between two streams each give the oracle's bits."""
+    import torch
+    from ocotillo_b200 import workloads
+    rho, T, dz = workloads.agn_block(16, 16, 128, seed=23)
+    wa = workloads.log_wavelengths(64)
+    engine.set_wavelengths(wa)
+    nx, ny, nz = rho.shape
+    nw = len(wa)
+    dev = torch.device("cuda:0")
+    r, t = torch.from_numpy(rho).to(dev), torch.from_numpy(T).to(dev)
+    mk = lambda *s: torch.full(s, float("nan"), dtype=torch.float64, device=dev)
+    outs = [{"U": mk(nw, nx, ny, nz + 6), "V": mk(nw, nx, ny, nz)} for _ in range(4)]
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    torch.cuda.synchronize()
+    for i, o in enumerate(outs):
+        engine.solve_block_device(r, t, dz, o, form="stable", layout=0, stream=s1 if i % 2 == 0 else s2)
+    torch.cuda.synchronize()
+    engine.synchronize()
+    ref = oracle.solve_block(rho, T, wa, dz, form=oracle.FORM_STABLE, backend="ocomath")
+    for i, o in enumerate(outs):
+        assert_bitwise(o["U"].cpu().numpy(), ref["U"], f"call {i} U")
+        assert_bitwise(o["V"].cpu().numpy(), ref["V"], f"call {i} V")
