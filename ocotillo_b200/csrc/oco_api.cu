@@ -248,6 +248,7 @@ static int set_wavelengths(oco_ctx *c, const double *wa, int32_t nw) {
   std::vector<double> wcopy(wa, wa + nw);
   CU(cudaSetDevice(c->device));
   CU(cudaStreamSynchronize(c->stream));
+  if (c->status_pending) CU(cudaStreamSynchronize(c->status_stream)); /* a device-array call may read the tables */
   CU(c->lam.ensure(tab.size() * sizeof(double)));
   CU(cudaMemcpy(c->lam.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
   CU(c->lam32.ensure(tab32.size() * sizeof(float)));
