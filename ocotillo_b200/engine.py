@@ -14,6 +14,7 @@ The device entry point also offers the lambda-fastest layout:
 """
 import ctypes
 import os
+import weakref
 
 import numpy as np
 
@@ -265,8 +266,11 @@ class Engine:
             raise OcoError(rc, self.lib.oco_last_error(None).decode())
         self.device = device
         self.nw = 0
+        self._batches = weakref.WeakSet()  # a batch refers to this context: closed before it
 
     def close(self):
+        for b in list(getattr(self, "_batches", ())):
+            b.close()
         if self.ctx:
             self.lib.oco_destroy(self.ctx)
             self.ctx = ctypes.c_void_p()
@@ -514,6 +518,7 @@ class Batch:
                                        float(fully_ionized_T), ctypes.byref(self.h))
         eng._check(rc)
         self.arrays = None
+        eng._batches.add(self)
 
     def alloc(self, device="cuda", want=("U", "kappa", "V", "Vtop", "Vbot")):
         """Allocates output tensors of the dense packing."""

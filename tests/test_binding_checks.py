@@ -99,3 +99,21 @@ def test_batch_bind_refuses_host_and_float32_tensors(eng):
         b.bind(x.float(), x, {})
     with pytest.raises(ValueError, match="unknown array 'Vtp'"):
         b.bind(x, x, {"Vtp": x})
+
+
+def test_engine_close_closes_its_batches_first(eng):
+    """A batch refers to its engine's context, so closing the engine closes its open batches
+    before the context goes."""
+    import weakref
+    from ocotillo_b200.engine import Batch
+    eng._batches = weakref.WeakSet()
+    closed = []
+
+    class FakeBatch(Batch):
+        def close(self):
+            closed.append(self)
+
+    fb = FakeBatch.__new__(FakeBatch)
+    eng._batches.add(fb)
+    eng.close()
+    assert closed == [fb]
