@@ -96,3 +96,45 @@ def test_pow10_fast_path_is_pow_of_ten(oracle):
     assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
     nan = oracle.mathcheck("ocomath", "pow10", np.array([np.nan]), np.array([np.nan]))
     assert np.isnan(nan).all()
+
+
+@pytest.fixture(scope="module")
+def exp_host():
+    import ctypes
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    build = os.path.join(root, "tests", "_build")
+    os.makedirs(build, exist_ok=True)
+    out = os.path.join(build, "libocomath_host.so")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-I",
+                    os.path.join(root, "ocotillo_b200", "csrc"), "-o", out, os.path.join(root, "tests", "ocomath_host.cpp")],
+                   check=True, capture_output=True)
+    h = ctypes.CDLL(out)
+    P = ctypes.POINTER(ctypes.c_double)
+    h.exp_fast_and_dd.argtypes = [P, P, ctypes.c_int64, P, ctypes.POINTER(ctypes.c_int32), P]
+    return h
+
+
+def test_exp_fast_phase_equals_full_exp_where_it_succeeds(exp_host):
+    """The plain kernels take the branch-free fast phase when it reports success and the full
+    correctly rounded exp otherwise: wherever it succeeds it must give the same bits.  Inputs
+    are double-double arguments (xl below half an ulp of xh) over the whole finite range and
+    near the ends, where the fast phase must decline rather than differ."""
+    import ctypes
+    rng = np.random.default_rng(11)
+    n = 400000
+    xh = np.concatenate([rng.uniform(-745.2, 709.8, n // 2), rng.uniform(-50.0, 50.0, n // 4),
+                         rng.uniform(-746.0, -700.0, n // 8), rng.uniform(700.0, 710.0, n // 8)])
+    xl = xh * rng.uniform(-1.0, 1.0, xh.size) * 2.0 ** -54
+    xl[::7] = 0.0
+    fast, dd = np.empty_like(xh), np.empty_like(xh)
+    ok = np.empty(xh.size, dtype=np.int32)
+    P = ctypes.POINTER(ctypes.c_double)
+    exp_host.exp_fast_and_dd(xh.ctypes.data_as(P), xl.ctypes.data_as(P), xh.size, fast.ctypes.data_as(P),
+                             ok.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), dd.ctypes.data_as(P))
+    good = ok.astype(bool)
+    inner = np.abs(xh) <= 700.0  # the fast phase declines only toward underflow and overflow
+    assert good[inner].mean() > 0.999, good[inner].mean()
+    assert np.array_equal(fast[good].view(np.uint64), dd[good].view(np.uint64)), np.count_nonzero(
+        fast[good].view(np.uint64) != dd[good].view(np.uint64))
