@@ -73,3 +73,23 @@ def test_reference_arm_under_torchrun_two_ranks():
     assert len(lines) == 1, r.stdout
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+
+
+def test_profile_commands_parse(monkeypatch):
+    """Every profile summary gives the bench command it was captured from; each must still be a
+    valid bench.py command line (the chunking of its grid included)."""
+    import glob
+    import re
+    sys.path.insert(0, ROOT)
+    import bench
+    found = 0
+    for f in glob.glob(os.path.join(ROOT, "profiles", "*.txt")):
+        text = open(f).read().replace("\\\n", " ")
+        for m in re.finditer(r"python bench\.py([^\n]*)", text):
+            argv = m.group(1).split()
+            monkeypatch.setattr(sys, "argv", ["bench.py"] + argv)
+            a = bench.parse()
+            ncol = a.nx * a.ny
+            assert ncol % min(a.chunk_cols, ncol) == 0, (f, argv)
+            found += 1
+    assert found >= 6
