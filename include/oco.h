@@ -176,9 +176,12 @@ int oco_check_bounded_wait(oco_ctx *ctx, int64_t spin_limit);
  * the process exits.  The caller passes the wavelengths (Angstrom), the device inputs and
  * the device outputs (layout p->layout).  No context, no cudaMalloc/cudaFree, no allocating
  * library call.  The first call on a device looks up the array's device address (do it
- * before any stream capture).  Calls share the array; calls whose GPU work overlaps race.
- * The call returns when its work on `stream` is done.  Limits: nz <= OCO_NOALLOC_MAX_NZ,
- * nw <= OCO_NOALLOC_MAX_NW, forms PLAIN and STABLE; larger sizes return OCO_EINVAL.
+ * before any stream capture).  Calls on a device share its array, so calls whose GPU work
+ * overlapped would race: each call holds a per-device lock until its work on `stream` is done,
+ * and returns only then (also on an error after work was enqueued).  Any of U, kappa, V, Vtop,
+ * Vbot may be NULL (not stored), as for oco_solve_block_device.  Limits: nz <=
+ * OCO_NOALLOC_MAX_NZ together with nw <= OCO_NOALLOC_MAX_NW always fit (the library checks this
+ * at compile time), forms PLAIN and STABLE; larger sizes return OCO_EINVAL.
  * Errors: oco_noalloc_last_error(). */
 #define OCO_NOALLOC_WORKSPACE_BYTES (32u << 20)
 #define OCO_NOALLOC_MAX_NZ 4096

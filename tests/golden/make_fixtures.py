@@ -7,7 +7,9 @@ for the Athena decks, the binary snapshot files under input_athena/.  These are 
 (data), copied byte for byte; the GPU box has no copy of the reference, so the tests read
 them from here.
 
-    python tests/golden/make_fixtures.py [reference_root]
+    python tests/golden/make_fixtures.py <reference_root>
+
+reference_root is the top directory of a checkout of the reference (the one holding samples/).
 """
 import os
 import shutil
@@ -18,7 +20,9 @@ KEEP = {"input.in", "resolution.in", "reference.out"}
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_fixtures.py <reference_root>")
+    ref = sys.argv[1]
     dst_root = os.path.join(os.path.dirname(os.path.abspath(__file__)), "samples")
     for deck in DECKS:
         src = os.path.join(ref, "samples", deck)
