@@ -17,18 +17,35 @@
 #include <stdlib.h>
 #include <string.h>
 
-#ifdef OCO_ORACLE_OCOMATH
+/* oreal: the arithmetic type of the per-column and per-(column, wavelength) work.  double in
+ * the glibc and ocomath back-ends; long double (x87 extended, 64-bit significand) in the
+ * longdouble back-end, which evaluates the same problem -- the same double inputs, wavelength
+ * tables and constants -- with 11 more bits per operation, to measure the rounding error of
+ * the double forms (the stable form in particular). */
+#ifdef OCO_ORACLE_LONGDOUBLE
+typedef long double oreal;
+#define MEXP(x) expl(x)
+#define MLOG(x) logl(x)
+#define MLOG10(x) log10l(x)
+#define MPOW(x, y) powl((x), (y))
+#define MSQRT(x) sqrtl(x)
+#define BACKEND 2
+#elif defined(OCO_ORACLE_OCOMATH)
 #include "ocomath.h"
+typedef double oreal;
 #define MEXP(x) oco_exp(x)
 #define MLOG(x) oco_log(x)
 #define MLOG10(x) oco_log10(x)
 #define MPOW(x, y) oco_pow((x), (y))
+#define MSQRT(x) sqrt(x)
 #define BACKEND 1
 #else
+typedef double oreal;
 #define MEXP(x) exp(x)
 #define MLOG(x) log(x)
 #define MLOG10(x) log10(x)
 #define MPOW(x, y) pow((x), (y))
+#define MSQRT(x) sqrt(x)
 #define BACKEND 0
 #endif
 
@@ -186,13 +203,13 @@ enum {
 };
 typedef struct {
   int nz;
-  double *f[P_NFIELDS];
-  double *mem;
+  oreal *f[P_NFIELDS];
+  oreal *mem;
 } opillar;
 
 static int pillar_alloc(opillar *p, int nz) {
   p->nz = nz;
-  p->mem = (double *)calloc((size_t)nz * P_NFIELDS, sizeof(double));
+  p->mem = (oreal *)calloc((size_t)nz * P_NFIELDS, sizeof(oreal));
   if (!p->mem) return ORACLE_ENOMEM;
   for (int k = 0; k < P_NFIELDS; k++) p->f[k] = p->mem + (size_t)k * nz;
   return ORACLE_OK;
@@ -201,20 +218,20 @@ static int pillar_alloc(opillar *p, int nz) {
 /* wavelength_independent_pillars + calc_hydrogen_ion_frac + solve_gas_state +
  * get_electron_pressure (gas_state.f90:30-110) + get_electron_thomson_scattering and
  * get_hydrogen_ion_bound_free (continuous_opacity.f90:143-163). */
-static void pillars(opillar *p, double fully_ionized_T) {
+static void pillars(opillar *p, oreal fully_ionized_T) {
   const int nz = p->nz;
-  double **f = p->f;
+  oreal **f = p->f;
   for (int i = 0; i < nz; i++) {
     f[P_RHO1][i] = 1.0 / f[P_RHO][i]; /* gas_state :34 */
     f[P_T1][i] = 1.0 / f[P_T][i];     /* :35 */
   }
   for (int i = 0; i < nz; i++) { /* calc_hydrogen_ion_frac :57-63 */
-    double T = f[P_T][i];
-    double constants = 2414683039571967.0 * MPOW(T, 1.5);
-    double exparg = (f[P_T1][i] * hydrogen_ionization_eV) * k1_eV;
-    double niine_ni = constants * MEXP(-exparg);
-    double c_ion = (mp * f[P_RHO1][i]) * niine_ni;
-    f[P_X][i] = 0.5 * (sqrt(c_ion * c_ion + 4.0 * c_ion) - c_ion);
+    oreal T = f[P_T][i];
+    oreal constants = 2414683039571967.0 * MPOW(T, 1.5);
+    oreal exparg = (f[P_T1][i] * hydrogen_ionization_eV) * k1_eV;
+    oreal niine_ni = constants * MEXP(-exparg);
+    oreal c_ion = (mp * f[P_RHO1][i]) * niine_ni;
+    f[P_X][i] = 0.5 * (MSQRT(c_ion * c_ion + 4.0 * c_ion) - c_ion);
   }
   for (int i = 0; i < nz; i++) /* :70-74 */
     if (f[P_T][i] > fully_ionized_T) f[P_X][i] = 1.0;
@@ -239,11 +256,11 @@ static void pillars(opillar *p, double fully_ionized_T) {
 }
 
 /* bremsstrahlung_absorptionCoeff, continuous_opacity.f90:281-300 (zprotons = 1.0) */
-static double bremsstrahlung(const opillar *p, int i, double frequency) {
-  double *const *f = p->f;
-  const double zprotons = 1.0;
-  double gaunt = MLOG(MEXP(5.960 - (sqrt3 * pi1) * MLOG((frequency * 1e-9) * MPOW(f[P_T][i] * 1e-4, -1.5))) + exp1);
-  double ln_physQuant = (((MLOG(f[P_NE][i] * (f[P_NHI][i] + f[P_NHII][i])) + 2.0 * MLOG(zprotons)) -
+static oreal bremsstrahlung(const opillar *p, int i, oreal frequency) {
+  oreal *const *f = p->f;
+  const oreal zprotons = 1.0;
+  oreal gaunt = MLOG(MEXP(5.960 - (sqrt3 * pi1) * MLOG((frequency * 1e-9) * MPOW(f[P_T][i] * 1e-4, -1.5))) + exp1);
+  oreal ln_physQuant = (((MLOG(f[P_NE][i] * (f[P_NHI][i] + f[P_NHII][i])) + 2.0 * MLOG(zprotons)) -
                           0.5 * MLOG(f[P_T][i])) - 3.0 * MLOG(frequency)) +
                         MLOG(1.0 - MEXP(-(((h_planck * frequency) * k1_cgs) * f[P_T1][i])));
   return (bremsstrahlung_constant * MEXP(ln_physQuant)) * gaunt;
@@ -252,45 +269,45 @@ static double bremsstrahlung(const opillar *p, int i, double frequency) {
 /* calc_opacity_and_albedo, continuous_opacity.f90:175-201, with get_kappa_H_bf (:203-246),
  * get_kappa_Hm_bf (:302-324), get_kappa_Hm_ff (:326-341), calc_kappa_H_ff (:248-279) and
  * get_source_function (:392-409).  kr is scratch of length nz. */
-static void opacity_and_albedo(opillar *p, const otab *t, int iw, double *kr) {
+static void opacity_and_albedo(opillar *p, const otab *t, int iw, oreal *kr) {
   const int nz = p->nz;
-  double **f = p->f;
-  const double chi = t->chi[iw], wa3 = t->wa3[iw];
+  oreal **f = p->f;
+  const oreal chi = t->chi[iw], wa3 = t->wa3[iw];
   for (int i = 0; i < nz; i++) f[P_STIM][i] = 1.0 - MPOW(10.0, -(chi * f[P_THETA][i])); /* :171 */
   for (int i = 0; i < nz; i++) {
     /* get_kappa_H_bf :233-244 */
-    double sm = 0.0;
-    double ktemp = k_cgs * f[P_T][i];
-    double ktemp1 = k1_cgs * f[P_T1][i];
+    oreal sm = 0.0;
+    oreal ktemp = k_cgs * f[P_T][i];
+    oreal ktemp1 = k1_cgs * f[P_T1][i];
     for (int n = 0; n < MDIM; n++) {
-      double n1 = t->n1_array[n];
+      oreal n1 = t->n1_array[n];
       sm = sm + (t->g[iw * MDIM + n] * (n1 * (n1 * n1))) * MEXP(-(t->chi_n[n] * ktemp1));
     }
-    double unsold = ((0.5 * ktemp) * RydbergEnergy1) *
+    oreal unsold = ((0.5 * ktemp) * RydbergEnergy1) *
                     (MEXP(-(t->chi_m * ktemp1)) - MEXP(-(RydbergEnergy * ktemp1)));
-    double kHbf = (((AHbf * f[P_STIM][i]) * f[P_IONF][i]) * wa3) * (unsold + sm);
+    oreal kHbf = (((AHbf * f[P_STIM][i]) * f[P_IONF][i]) * wa3) * (unsold + sm);
     /* get_kappa_Hm_bf :318-322 */
-    double kHmbf = (t->wa[iw] < 16000.0)
+    oreal kHmbf = (t->wa[iw] < 16000.0)
                        ? ((f[P_HMBF][i] * f[P_STIM][i]) * f[P_IONF][i]) * t->s_coeff[iw]
                        : 0.0;
     /* get_kappa_Hm_ff :337-339 */
-    double flam = ((t->f_coeff[iw * 3 + 0] + t->f_coeff[iw * 3 + 1] * f[P_LGT][i]) +
+    oreal flam = ((t->f_coeff[iw * 3 + 0] + t->f_coeff[iw * 3 + 1] * f[P_LGT][i]) +
                    t->f_coeff[iw * 3 + 2] * f[P_LGT2][i]) - 26.0;
-    double kHmff = (((f[P_IONF][i] * f[P_NE][i]) * k_cgs) * f[P_T][i]) * MPOW(10.0, flam);
+    oreal kHmff = (((f[P_IONF][i] * f[P_NE][i]) * k_cgs) * f[P_T][i]) * MPOW(10.0, flam);
     kr[i] = (((kHbf + kHmbf) + kHmff) + f[P_ESCAT][i]) * mp1; /* :188 */
     f[P_OMA][i] = ((kHbf + kHmbf) + kHmff) * mp1; /* absorption part of kr, stable form */
     f[P_OP][i] = kr[i] * f[P_RHO][i];                          /* :189 */
   }
   for (int i = 0; i < nz; i++) { /* calc_kappa_H_ff :261-277 */
     if ((1.0 - f[P_X][i]) > switch_ionfraction) {
-      double g_ff = 1.0 + t->gff_factor[iw] * (((f[P_THETA1][i] * log10e) * t->chi1[iw]) + 0.5);
-      double energyfactor = (((0.5 * log10e) * f[P_THETA1][i]) * Iev1) * MPOW(10.0, -(f[P_THETA][i] * Iev));
-      double kHff = ((((f[P_STIM][i] * f[P_IONF][i]) * alpha0) * wa3) * g_ff) * energyfactor;
+      oreal g_ff = 1.0 + t->gff_factor[iw] * (((f[P_THETA1][i] * log10e) * t->chi1[iw]) + 0.5);
+      oreal energyfactor = (((0.5 * log10e) * f[P_THETA1][i]) * Iev1) * MPOW(10.0, -(f[P_THETA][i] * Iev));
+      oreal kHff = ((((f[P_STIM][i] * f[P_IONF][i]) * alpha0) * wa3) * g_ff) * energyfactor;
       kr[i] = kr[i] + kHff * mp1;
       f[P_OMA][i] = f[P_OMA][i] + kHff * mp1;
       f[P_OP][i] = f[P_OP][i] + kr[i] * f[P_RHO][i];
     } else {
-      double ob = bremsstrahlung(p, i, t->nu[iw]);
+      oreal ob = bremsstrahlung(p, i, t->nu[iw]);
       f[P_OP][i] = f[P_OP][i] + ob;
       kr[i] = kr[i] + f[P_OP][i] * f[P_RHO1][i];
       f[P_OMA][i] = f[P_OMA][i] + f[P_OP][i] * f[P_RHO1][i];
@@ -303,19 +320,19 @@ static void opacity_and_albedo(opillar *p, const otab *t, int iw, double *kr) {
     f[P_OP2][i] = f[P_OP][i] * f[P_OP][i];       /* :197 */
   }
   for (int i = 0; i < nz; i++) { /* get_source_function :399-407 */
-    double damping = (t->damping_factor_const * f[P_T1][i]) * t->wcm1[iw];
+    oreal damping = (t->damping_factor_const * f[P_T1][i]) * t->wcm1[iw];
     if (damping > log_overflow_limit) damping = log_overflow_limit;
     f[P_S][i] = (t->source_function_const * t->w1cm5[iw]) / (MEXP(damping) - 1.0);
   }
 }
 
 /* grey_parameters, continuous_opacity.f90:377-390 */
-static void grey_parameters(opillar *p, double sigma_grey) {
-  double **f = p->f;
+static void grey_parameters(opillar *p, oreal sigma_grey) {
+  oreal **f = p->f;
   for (int i = 0; i < p->nz; i++) {
-    double T = f[P_T][i], T2 = T * T;
+    oreal T = f[P_T][i], T2 = T * T;
     f[P_S][i] = sigma_sb * (T2 * T2);
-    double alpha_grey = (3.68e22 * MPOW(T, -3.5)) * f[P_RHO][i];
+    oreal alpha_grey = (3.68e22 * MPOW(T, -3.5)) * f[P_RHO][i];
     f[P_OP][i] = (alpha_grey + sigma_grey) * f[P_RHO][i];
     f[P_ALB][i] = sigma_grey / (alpha_grey + sigma_grey);
     f[P_OMA][i] = alpha_grey / (alpha_grey + sigma_grey);
@@ -327,23 +344,23 @@ static void grey_parameters(opillar *p, double sigma_grey) {
 /* get_tridag_coefficients -> fill_center_coeffs + fill_boundary_coeffs,
  * auxiliary.f90:111-201.  ex receives the diagonal excess -(a+b+c) computed directly
  * (used only by the stable form). */
-static void tridag_coefficients(double *aa, double *bb, double *cc, double *dd, double *ex,
-                                const opillar *p, double dz, double dz2, double *kp, int stable) {
+static void tridag_coefficients(oreal *aa, oreal *bb, oreal *cc, oreal *dd, oreal *ex,
+                                const opillar *p, oreal dz, oreal dz2, oreal *kp, int stable) {
   const int nz = p->nz;
-  double *const *f = p->f;
+  oreal *const *f = p->f;
   for (int iz = 0; iz < nz - 1; iz++) kp[iz] = 0.5 * (f[P_OP][iz + 1] + f[P_OP][iz]); /* :147-149 */
   for (int iz = 1; iz < nz - 1; iz++) { /* :159-165; kappa_m(iz) == kappa_p(iz-1) */
-    double op = f[P_OP][iz];
+    oreal op = f[P_OP][iz];
     aa[iz] = f[P_OP2][iz] / kp[iz - 1];
     cc[iz] = f[P_OP2][iz] / kp[iz];
-    double oma = stable ? f[P_OMA][iz] : (1.0 - f[P_ALB][iz]);
-    double zeta = (dz2 * (op * (op * op))) * oma;
+    oreal oma = stable ? f[P_OMA][iz] : (1.0 - f[P_ALB][iz]);
+    oreal zeta = (dz2 * (op * (op * op))) * oma;
     bb[iz] = -((aa[iz] + cc[iz]) + zeta);
     dd[iz] = -(f[P_S][iz] * zeta);
     ex[iz] = zeta;
   }
   /* :187-197 */
-  double zeta = ((f[P_OP][0] * dz2) * (stable ? f[P_OMA][0] : (1.0 - f[P_ALB][0]))) * 0.25;
+  oreal zeta = ((f[P_OP][0] * dz2) * (stable ? f[P_OMA][0] : (1.0 - f[P_ALB][0]))) * 0.25;
   aa[0] = 0.0;
   bb[0] = -(((f[P_OP1][0] + dz) + zeta) * f[P_OP2][0]);
   cc[0] = f[P_OP][0];
@@ -360,10 +377,10 @@ static void tridag_coefficients(double *aa, double *bb, double *cc, double *dd, 
 
 /* tridag, auxiliary.f90:14-47.  Returns 0, or -1 on an exactly zero pivot (the reference
  * stops there; here the solve continues so that a status can be reported). */
-static int tridag(const double *a, const double *b, const double *c, const double *r, double *u,
-                  int n, double *gam) {
+static int tridag(const oreal *a, const oreal *b, const oreal *c, const oreal *r, oreal *u,
+                  int n, oreal *gam) {
   int bad = 0;
-  double bet = b[0];
+  oreal bet = b[0];
   if (bet == 0.0) bad = -1;
   u[0] = r[0] / bet;
   for (int j = 1; j < n; j++) {
@@ -381,15 +398,15 @@ static int tridag(const double *a, const double *b, const double *c, const doubl
  * also returns the differences D_j = U_j - U_{j+1} = u_j - q_j U_{j+1}, q_j = h_j/(c_j + h_j):
  * in optically thin layers |gamma| = 1 - q rounds to 1 and U_j - U_{j+1} is below the
  * resolution of U itself, while u_j and q_j U_{j+1} are of the size of the difference. */
-static int tridag_stable(const double *a, const double *c, const double *r, const double *e,
-                         double *u, int n, double *gam, double *q, double *D) {
+static int tridag_stable(const oreal *a, const oreal *c, const oreal *r, const oreal *e,
+                         oreal *u, int n, oreal *gam, oreal *q, oreal *D) {
   int bad = 0;
-  double h = e[0];
-  double bet = -(c[0] + h);
+  oreal h = e[0];
+  oreal bet = -(c[0] + h);
   if (bet == 0.0) bad = -1;
   u[0] = r[0] / bet;
   for (int j = 1; j < n; j++) {
-    double den = c[j - 1] + h;
+    oreal den = c[j - 1] + h;
     gam[j] = -(c[j - 1] / den);
     q[j - 1] = h / den;
     h = e[j] + (a[j] * h) / den;
@@ -398,7 +415,7 @@ static int tridag_stable(const double *a, const double *c, const double *r, cons
     u[j] = (r[j] - a[j] * u[j - 1]) / bet;
   }
   for (int j = n - 2; j >= 0; j--) {
-    double uf = u[j];
+    oreal uf = u[j];
     u[j] = uf - gam[j + 1] * u[j + 1];
     D[j] = uf - q[j] * u[j + 1];
   }
@@ -410,9 +427,9 @@ static int tridag_stable(const double *a, const double *c, const double *r, cons
  * ghost zones mirror the differences next to each boundary.  Same value as the stencil on
  * f in exact arithmetic; used by the stable form (nz >= 4), whose D_j are accurate where
  * the differences of U are not resolved. */
-static void calc_flux_diff(const double *D, opillar *p, double dz1, double *Dl) {
+static void calc_flux_diff(const oreal *D, opillar *p, oreal dz1, oreal *Dl) {
   const int nz = p->nz, n1 = 3;
-  double **pf = p->f;
+  oreal **pf = p->f;
   for (int m = n1; m <= nz + 1; m++) Dl[m] = D[m - n1];
   for (int i = 1; i <= 3; i++) {
     Dl[nz + 2 + i - 1] = Dl[nz + 2 - i];
@@ -420,16 +437,16 @@ static void calc_flux_diff(const double *D, opillar *p, double dz1, double *Dl) 
   }
   for (int j = 0; j < nz; j++) {
     int m = n1 + j;
-    double s1 = Dl[m - 1] + Dl[m];
-    double s2 = (s1 + Dl[m - 2]) + Dl[m + 1];
-    double s3 = (s2 + Dl[m - 3]) + Dl[m + 2];
-    double df = -((1.0 / 60.0) * (((45.0 * s1) - 9.0 * s2) + s3));
+    oreal s1 = Dl[m - 1] + Dl[m];
+    oreal s2 = (s1 + Dl[m - 2]) + Dl[m + 1];
+    oreal s3 = (s2 + Dl[m - 3]) + Dl[m + 2];
+    oreal df = -((1.0 / 60.0) * (((45.0 * s1) - 9.0 * s2) + s3));
     pf[P_FLUX][j] = ((-1.0 * pf[P_OP1][j]) * df) * dz1;
   }
 }
 
 /* update_ghosts, auxiliary.f90:49-62 (f has nz+6 entries, n1 = 3, n2 = nz+2 0-based) */
-static void update_ghosts(double *f, int nz) {
+static void update_ghosts(oreal *f, int nz) {
   const int n1 = 3, n2 = nz + 2;
   for (int i = 1; i <= 3; i++) {
     f[n1 - i] = 2.0 * f[n1] - f[n1 + i];
@@ -438,12 +455,12 @@ static void update_ghosts(double *f, int nz) {
 }
 
 /* der + calc_flux, auxiliary.f90:64-78 and :96-109 */
-static void calc_flux(const double *f, opillar *p, double dz1) {
+static void calc_flux(const oreal *f, opillar *p, oreal dz1) {
   const int n1 = 3;
-  double **pf = p->f;
+  oreal **pf = p->f;
   for (int i = 0; i < p->nz; i++) {
     int c = n1 + i;
-    double df = (1.0 / 60.0) * (((45.0 * (f[c + 1] - f[c - 1])) - 9.0 * (f[c + 2] - f[c - 2])) +
+    oreal df = (1.0 / 60.0) * (((45.0 * (f[c + 1] - f[c - 1])) - 9.0 * (f[c + 2] - f[c - 2])) +
                                 (f[c + 3] - f[c - 3]));
     pf[P_FLUX][i] = ((-1.0 * pf[P_OP1][i]) * df) * dz1;
   }
@@ -469,19 +486,21 @@ int oracle_solve_columns(const oracle_params *prm, const double *wa, const doubl
     otab_free(&t);
     return ORACLE_ENOMEM;
   }
-  double *work = (double *)calloc((size_t)nz * 10 + 2 * mz, sizeof(double));
+  oreal *work = (oreal *)calloc((size_t)nz * 10 + 2 * mz, sizeof(oreal));
   if (!work) {
     free(p.mem);
     otab_free(&t);
     return ORACLE_ENOMEM;
   }
-  double *a = work, *b = work + nz, *c = work + 2 * nz, *d = work + 3 * nz, *ex = work + 4 * nz;
-  double *kr = work + 5 * nz, *gam = work + 6 * nz, *kp = work + 7 * nz, *u = work + 8 * nz;
-  double *qv = work + 8 * nz + mz, *Dv = work + 9 * nz + mz, *Dl = work + 10 * nz + mz;
-  const double dz = prm->dz, dz1 = 1.0 / prm->dz, dz2 = prm->dz * prm->dz;
+  oreal *a = work, *b = work + nz, *c = work + 2 * nz, *d = work + 3 * nz, *ex = work + 4 * nz;
+  oreal *kr = work + 5 * nz, *gam = work + 6 * nz, *kp = work + 7 * nz, *u = work + 8 * nz;
+  oreal *qv = work + 8 * nz + mz, *Dv = work + 9 * nz + mz, *Dl = work + 10 * nz + mz;
+  const oreal dz = prm->dz, dz1 = (oreal)1.0 / dz, dz2 = dz * dz;
   for (int64_t col = col0; col < col1; col++) {
-    memcpy(p.f[P_RHO], rho + col * nz, (size_t)nz * sizeof(double));
-    memcpy(p.f[P_T], T + col * nz, (size_t)nz * sizeof(double));
+    for (int i = 0; i < nz; i++) {
+      p.f[P_RHO][i] = rho[col * nz + i];
+      p.f[P_T][i] = T[col * nz + i];
+    }
     pillars(&p, prm->fully_ionized_T);
     for (int iw = 0; iw < nw; iw++) {
       if (prm->lgrey)
@@ -501,9 +520,12 @@ int oracle_solve_columns(const oracle_params *prm, const double *wa, const doubl
       else
         calc_flux(u, &p, dz1);
       size_t item = (size_t)iw * (size_t)ncol + (size_t)col;
-      if (U) memcpy(U + item * mz, u, (size_t)mz * sizeof(double));
-      if (kappa) memcpy(kappa + item * nz, p.f[P_OP], (size_t)nz * sizeof(double));
-      if (V) memcpy(V + item * nz, p.f[P_FLUX], (size_t)nz * sizeof(double));
+      if (U)
+        for (int i = 0; i < mz; i++) U[item * mz + i] = (double)u[i];
+      if (kappa)
+        for (int i = 0; i < nz; i++) kappa[item * nz + i] = (double)p.f[P_OP][i];
+      if (V)
+        for (int i = 0; i < nz; i++) V[item * nz + i] = (double)p.f[P_FLUX][i];
     }
   }
   free(work);

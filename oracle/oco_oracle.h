@@ -8,11 +8,15 @@
  * The reference (Fortran 90, all REAL promoted to double by -fdefault-real-8) cannot be
  * compiled here (no Fortran compiler), so this file restates it in C99 with the same
  * operation order, no FMA contraction (-ffp-contract=off) and the reference's lowering of
- * integer powers.  Two math back-ends are built from the same source:
- *   - glibc    (OCO_ORACLE_OCOMATH undefined): exp/log/log10/pow from the C library, as
- *              the gfortran-built reference calls them;
- *   - ocomath  (OCO_ORACLE_OCOMATH defined): the project's correctly rounded functions,
- *              which the GPU kernels also use, for bit-for-bit comparisons.
+ * integer powers.  Three back-ends are built from the same source:
+ *   - glibc    (no macro): exp/log/log10/pow from the C library, as the gfortran-built
+ *              reference calls them;
+ *   - ocomath  (OCO_ORACLE_OCOMATH): the project's correctly rounded functions, which the GPU
+ *              kernels also use, for bit-for-bit comparisons;
+ *   - longdouble (OCO_ORACLE_LONGDOUBLE): the per-column and per-item work in long double
+ *              (x87 extended) arithmetic with glibc's long double functions, on the same double
+ *              inputs, wavelength tables and constants; it measures the rounding error of the
+ *              double forms (oracle_math_backend() returns 2).
  * Only calls inside the xy/lambda loop switch back-ends; the once-per-run wavelength tables
  * and the input construction (disk model, Athena reader) use glibc in both, as the product's
  * host code does.
@@ -53,7 +57,7 @@ typedef struct oracle_params {
   double fully_ionized_T;
 } oracle_params;
 
-/* 0 = glibc, 1 = ocomath. */
+/* 0 = glibc, 1 = ocomath, 2 = longdouble. */
 int oracle_math_backend(void);
 
 /* calc_wavelength, continuous_opacity.f90:37-62. */
