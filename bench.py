@@ -42,7 +42,7 @@ sys.path.insert(0, ROOT)
 METRIC = "mesh\u00b7\u03bb points/s + p50/p99 latency: mixed vs plain FP64, 1 B200, \u22641e-4 rel"
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -60,12 +60,27 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the mixed, batch and serving measurements")
-    ap.add_argument("--serve-jobs", type=int, default=12)
-    ap.add_argument("--serve-rate", type=float, default=1.5, help="job arrivals per second")
+    ap.add_argument("--serve-jobs", type=int, default=50, help="jobs per serving run (each rate of the sweep)")
     ap.add_argument("--batch-cols", type=int, default=8192)
     ap.add_argument("--no-c3", action="store_true", help="skip the precision-config (c3) measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving (c5) measurement")
-    return ap.parse_args()
+    ap.add_argument("--cpu1-cols", type=int, default=64, help="columns in the one-core CPU-baseline sample")
+    return ap.parse_args(argv)
+
+
+def max_over_ranks(x, world, dist=None, device=None):
+    """The largest of the ranks' values of x (every rank gets it; x itself when world == 1)."""
+    if world == 1:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, points_per_rank_step, steps, max_ms):
+    """Whole-job throughput: the points all ranks processed over the slowest rank's time."""
+    return world * points_per_rank_step * steps / (max_ms / 1e3)
 
 
 # ---- clocks during the timed region ---------------------------------------------------------
@@ -278,12 +293,9 @@ class Grid:
         step_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(steps)]
         total_ms = evs[0].elapsed_time(evs[-1])
         solve_ms, pil_ms, nsolve = self.eng.kernel_times()
-        if world > 1:
-            t = torch.tensor([total_ms], device=self.dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total_ms = float(t.item())
+        total_ms = max_over_ranks(total_ms, world, dist, self.dev)
         pts_step = self.ncol * self.nz * self.nw
-        return {"value": world * pts_step * steps / (total_ms / 1e3), "total_ms": total_ms, "step_ms": step_ms,
+        return {"value": whole_job_rate(world, pts_step, steps, total_ms), "total_ms": total_ms, "step_ms": step_ms,
                 "launches": launches, "solve_ms": solve_ms, "pil_ms": pil_ms, "nsolve": nsolve, "clocks": clk,
                 "pts_step": pts_step}
 
@@ -346,7 +358,9 @@ def flux_error(g, form_a, form_b, eps=1e-7, seed=7):
     pert = g.rho * (1.0 + eps * torch.randn(g.rho.shape, generator=gen, device=g.rho.device, dtype=g.rho.dtype))
     rp = planes(form_b, pert)
     del pert
+    g.eng.mixed_repairs()  # counts from here: the items form_a re-solves in FP64
     ra = planes(form_a)
+    repaired = g.eng.mixed_repairs()
     ok = torch.isfinite(rb) & (rb != 0) & torch.isfinite(rp)
     rel = ((ra - rb).abs() / rb.abs())[ok]
     sens = ((rp - rb).abs() / rb.abs())[ok]
@@ -356,6 +370,7 @@ def flux_error(g, form_a, form_b, eps=1e-7, seed=7):
     sensitive = sens > 10 * eps  # items whose FP64 flux responds to the perturbation
     backward = rel[sensitive] / sens[sensitive] * eps
     return {"reference_form": form_b, "items": int(rel.numel()),
+            "repaired_items": repaired, "repaired_frac": repaired / (g.ncol * g.nw),
             "all": {"max": rel.max().item(), "p99": q(rel, 0.99), "p9999": q(rel, 0.9999),
                     "frac_above_1e-4": (rel > 1e-4).double().mean().item()},
             "conditioned": {"definition": f"FP64 flux changes by <= {100 * eps:g} under a {eps:g} relative "
@@ -488,9 +503,9 @@ def measure_batch(a, eng, dev):
 def measure_precision_c3(a, eng, dev):
     """Config 'precision form': 512x512 columns, nz=1024, nw=512 log-spaced 100 A - 10 um, the AGN
     construction with rho0 drawn log-uniform in [1e-11, 1e-7].  Mixed and plain throughput over
-    the whole grid (2048-column chunks, lambda-fastest outputs), and the mixed emergent-flux error
-    against the difference-form and the reference-form FP64 paths on a 32x32-column draw of the
-    same construction (same rho0)."""
+    the whole grid (2048-column chunks, lambda-fastest outputs), the mixed emergent-flux error
+    against the difference-form FP64 path over the whole grid, and against the reference-form
+    FP64 path and the mean-intensity error on a 32x32-column draw of the same construction."""
     import copy
     import torch
     b = copy.copy(a)
@@ -502,6 +517,9 @@ def measure_precision_c3(a, eng, dev):
     mm = g.measure("mixed", steps, 1, 1)
     mp = g.measure("plain", steps, 1, 1)
     rho0 = g.rho0
+    g.sets = None  # the error passes store the emergent planes only
+    torch.cuda.empty_cache()
+    err = flux_error(g, "mixed", "stable")
     del g
     torch.cuda.empty_cache()
     s = copy.copy(b)
@@ -512,8 +530,8 @@ def measure_precision_c3(a, eng, dev):
            "points": 512 * 512 * 1024 * 512, "steps": steps,
            "mixed_value": mm["value"], "plain_value": mp["value"], "ratio": mm["value"] / mp["value"],
            "mixed_ms_per_step": mm["total_ms"] / steps, "plain_ms_per_step": mp["total_ms"] / steps,
+           "emergent_flux_rel_err": dict(err, sample="whole grid (2.6e8 emergent fluxes)"),
            "error_sample": "32x32 columns of the same construction, all z and lambda",
-           "emergent_flux_rel_err": flux_error(gs, "mixed", "stable"),
            "emergent_flux_rel_err_vs_plain": flux_error_vs_plain(gs),
            "mean_intensity_rel_err": intensity_error(gs)}
     del gs
@@ -521,8 +539,11 @@ def measure_precision_c3(a, eng, dev):
     return res
 
 
-def measure_serving(a, dev, form, specs, arrays):
-    """Runs the job stream through a fresh server; latency = done - submit (server clock)."""
+def run_stream(dev, form, specs, arrays, pinned):
+    """Runs one job stream through a fresh server: each job is submitted at its arrival time,
+    and every finished job is fetched at once (emergent-flux planes into pinned host memory).
+    Per job: device latency (submit -> results complete on the device, server clock), fetch
+    latency (submit -> planes in host memory) and admission wait (submit -> admitted)."""
     import torch
     from ocotillo_b200 import Server, workloads
     srv = Server(dev.index or 0, max_jobs=4, max_nz=1024, reserve_bytes=24e9)
@@ -531,26 +552,133 @@ def measure_serving(a, dev, form, specs, arrays):
     srv.wait(jid)
     srv.fetch(jid)
     torch.cuda.synchronize(dev)
-    ids = []
-    t0 = time.perf_counter()
-    for spec, (rho, T, dz) in zip(specs, arrays):
-        delay = t0 + spec["arrival_s"] - time.perf_counter()
-        if delay > 0:
-            time.sleep(delay)
-        ids.append(srv.submit(rho, T, workloads.log_wavelengths(spec["nw"]), dz, form=form))
-    lat, queue, first, last, pts = [], [], None, None, 0
-    for spec, jid in zip(specs, ids):
-        srv.wait(jid, 3600.0)
-        st = srv.status(jid)
-        lat.append(1e3 * (st["done_s"] - st["submit_s"]))
-        queue.append(1e3 * (st["admit_s"] - st["submit_s"]))
-        first = st["submit_s"] if first is None else min(first, st["submit_s"])
-        last = st["done_s"] if last is None else max(last, st["done_s"])
-        pts += spec["nx"] * spec["ny"] * spec["nz"] * spec["nw"]
-        srv.fetch(jid)
+    ids, jobs = {}, []
+    pending = list(range(len(specs)))
+    outstanding = set()
+    done = {}
+    t0 = time.monotonic()
+    while pending or outstanding:
+        now = time.monotonic()
+        while pending and t0 + specs[pending[0]]["arrival_s"] <= now:
+            k = pending.pop(0)
+            rho, T, dz = arrays[k]
+            ids[k] = srv.submit(rho, T, workloads.log_wavelengths(specs[k]["nw"]), dz, form=form)
+            outstanding.add(k)
+        for k in list(outstanding):
+            st = srv.status(ids[k])
+            if st["state"] == "done":
+                sp = specs[k]
+                n = sp["nw"] * sp["nx"] * sp["ny"]
+                shp = (sp["nw"], sp["nx"], sp["ny"])
+                srv.fetch(ids[k], out={"Vtop": pinned[0][:n].reshape(shp), "Vbot": pinned[1][:n].reshape(shp)})
+                done[k] = (st, time.monotonic())
+                outstanding.discard(k)
+            elif st["state"] == "failed":
+                raise RuntimeError(f"serving job {k} failed: {st['error']}")
+        if pending and not outstanding:
+            time.sleep(max(0.0, min(0.002, t0 + specs[pending[0]]["arrival_s"] - time.monotonic())))
+        else:
+            time.sleep(0.0005)
     srv.close()
-    return {"p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99), "mean_ms": sum(lat) / len(lat),
-            "max_queue_ms": max(queue), "throughput_points_per_s": pts / (last - first), "jobs": len(lat)}
+    lat, fet, adm, cls = [], [], [], {}
+    first, last, pts = None, None, 0
+    for k, (st, tf) in done.items():
+        sp = specs[k]
+        lat.append(1e3 * (st["done_s"] - st["submit_s"]))
+        fet.append(1e3 * (tf - st["submit_s"]))
+        adm.append(1e3 * (st["admit_s"] - st["submit_s"]))
+        cls.setdefault(sp["nx"], []).append((lat[-1], fet[-1]))
+        first = st["submit_s"] if first is None else min(first, st["submit_s"])
+        last = tf if last is None else max(last, tf)
+        pts += sp["nx"] * sp["ny"] * sp["nz"] * sp["nw"]
+    return {"jobs": len(lat), "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99),
+            "fetch_p50_ms": pct(fet, 0.5), "fetch_p99_ms": pct(fet, 0.99),
+            "admission_wait_p99_ms": pct(adm, 0.99), "admission_wait_max_ms": max(adm),
+            "throughput_points_per_s": pts / (last - first), "makespan_s": last - first,
+            "per_class": {f"{n}x{n}": {"jobs": len(v), "p50_ms": pct([x[0] for x in v], 0.5),
+                                       "p99_ms": pct([x[0] for x in v], 0.99),
+                                       "fetch_p99_ms": pct([x[1] for x in v], 0.99)} for n, v in sorted(cls.items())}}
+
+
+def measure_serving_sweep(a, dev):
+    """Config 'serving form': the Poisson job stream (seed 5) at rising arrival rates.  The
+    saturation rate comes from the same jobs all submitted at once (jobs / makespan); the mixed
+    form then runs at 0.3, 0.5, 0.7 and 0.9 of its saturation rate and the plain FP64 form at half
+    of its own.  Job inputs are generated on the device once and reused by every run (the same
+    seed gives the same jobs at every rate; only the arrival times scale)."""
+    import torch
+    from ocotillo_b200 import workloads
+    n = a.serve_jobs
+    base = workloads.serving_stream(n, 1.0, seed=5)
+    arrays = [workloads.job_arrays_device(sp, dev) for sp in base]
+    torch.cuda.synchronize(dev)
+    maxn = max(sp["nw"] * sp["nx"] * sp["ny"] for sp in base)
+    pinned = [torch.empty(maxn, dtype=torch.float64, pin_memory=True).numpy() for _ in range(2)]
+    points = int(sum(sp["nx"] * sp["ny"] * sp["nz"] * sp["nw"] for sp in base))
+    res = {"jobs_per_run": n, "points_per_run": points, "max_jobs_resident": 4,
+           "stream": "Poisson (seed 5); nx=ny in {64,128,256,512}, nz U[128,1024], nw U[64,512], rho0 log-uniform "
+                     "[1e-11,1e-7]; outputs: emergent-flux planes, fetched into pinned host memory as each job ends",
+           "latency": "p50/p99_ms: submit to results complete on the device; fetch_*: submit to planes in host memory"}
+    fracs = {"mixed": (0.3, 0.5, 0.7, 0.9), "plain": (0.5,)}
+    for form in ("mixed", "plain"):
+        sat_specs = [dict(sp, arrival_s=0.0) for sp in base]
+        sat = run_stream(dev, form, sat_specs, arrays, pinned)
+        sat_rate = n / sat["makespan_s"]
+        runs = {"saturation": dict(sat, rate_jobs_per_s=sat_rate)}
+        for f in fracs[form]:
+            specs = [dict(sp, arrival_s=sp["arrival_s"] / (f * sat_rate)) for sp in base]
+            runs[f"{f:g}x_saturation"] = dict(run_stream(dev, form, specs, arrays, pinned), rate_jobs_per_s=f * sat_rate)
+        res[form] = runs
+    del arrays
+    torch.cuda.empty_cache()
+    mx = res["mixed"]
+    res["headline"] = {"serving_saturation_jobs_per_s": mx["saturation"]["rate_jobs_per_s"],
+                       "serving_rate_jobs_per_s": mx["0.7x_saturation"]["rate_jobs_per_s"],
+                       "serving_p50_ms": mx["0.7x_saturation"]["p50_ms"], "serving_p99_ms": mx["0.7x_saturation"]["p99_ms"],
+                       "serving_fetch_p99_ms": mx["0.7x_saturation"]["fetch_p99_ms"],
+                       "serving_plain_p99_ms": res["plain"]["0.5x_saturation"]["p99_ms"]}
+    return res
+
+
+def _rel_inf(a, b):
+    with np.errstate(all="ignore"):
+        return np.nan_to_num(np.abs(a - b) / np.abs(b), nan=np.inf)
+
+
+def parity_vs_glibc(eng):
+    """The plain form (GPU) against the oracle built on glibc's exp/log/pow (what the gfortran
+    reference calls), on 16 AGN columns x 64 wavelengths of two constructions: the benchmark
+    grid's (density floor 1e-24) and the NongreyAGN deck's floor (1e-15).  The conditioning mask
+    keeps the items whose U (every z) and emergent fluxes move by < 1e-14 relative when rho is
+    perturbed by one ulp (glibc oracle); reported: the fraction of items in the mask, the largest
+    relative difference there (U, kappa, Vtop, Vbot), whether the finite class and sign agree
+    everywhere, and the fraction of bit-identical items."""
+    from oracle import pyoracle
+    from ocotillo_b200 import workloads
+    res = {"mask": "U and emergent fluxes change < 1e-14 under a one-ulp random perturbation of rho"}
+    for name, floor in (("floor_1e-24", 1e-24), ("floor_1e-15", 1e-15)):
+        rho, T, dz = workloads.agn_block(4, 4, 512, seed=2, rho_floor=floor)
+        wa = workloads.log_wavelengths(256)[::4]
+        eng.set_wavelengths(wa)
+        gpu = eng.solve_block(rho, T, dz, form="plain", allow_zero_pivot=True)
+        ref = pyoracle.solve_block(rho, T, wa, dz, form=pyoracle.FORM_REFERENCE, backend="glibc")
+        rp = rho * (1.0 + 2.0 ** -52 * np.random.default_rng(7).standard_normal(rho.shape))
+        refp = pyoracle.solve_block(rp, T, wa, dz, form=pyoracle.FORM_REFERENCE, backend="glibc")
+        s_ = np.maximum(_rel_inf(refp["U"], ref["U"]).max(-1),
+                        np.maximum(_rel_inf(refp["V"][..., -1], ref["V"][..., -1]),
+                                   _rel_inf(refp["V"][..., 0], ref["V"][..., 0])))
+        mask = s_ < 1e-14
+        d = np.maximum(np.maximum(_rel_inf(gpu["U"], ref["U"]).max(-1), _rel_inf(gpu["kappa"], ref["kappa"]).max(-1)),
+                       np.maximum(_rel_inf(gpu["Vtop"], ref["V"][..., -1]), _rel_inf(gpu["Vbot"], ref["V"][..., 0])))
+        cls = True
+        for x, y in ((gpu["U"], ref["U"]), (gpu["kappa"], ref["kappa"]), (gpu["Vtop"], ref["V"][..., -1]),
+                     (gpu["Vbot"], ref["V"][..., 0])):
+            fx, fy = np.isfinite(x), np.isfinite(y)
+            cls = cls and bool(np.array_equal(fx, fy) and np.array_equal(np.sign(x[fx]), np.sign(y[fy])))
+        res[name] = {"items": int(d.size), "in_mask": float(mask.mean()),
+                     "max_rel_in_mask": float(d[mask].max()) if mask.any() else None, "class_equal": cls,
+                     "bitwise": float((d == 0).mean())}
+    return res
 
 
 def main():
@@ -603,7 +731,7 @@ def main():
         torch.cuda.empty_cache()
 
     # ---- e2e: host arrays through oco_solve_block (pinned), one batch of columns per step
-    e2e = None
+    e2e, e2e_mixed = None, None
     if not a.no_e2e:
         E = min(a.e2e_cols, ncol)
         pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
@@ -615,99 +743,141 @@ def main():
                 "Vtop": pin((nw, E, 1)), "Vbot": pin((nw, E, 1))}
         nb = ncol // E
 
-        def e2e_step(i):
-            c0 = (i % nb) * E
-            eng.solve_block(rho_p[c0:c0 + E].reshape(E, 1, nz), T_p[c0:c0 + E].reshape(E, 1, nz), g.dz,
-                            form=a.form, out=outs, allow_zero_pivot=True)
+        def e2e_measure(form):
+            def e2e_step(i):
+                c0 = (i % nb) * E
+                eng.solve_block(rho_p[c0:c0 + E].reshape(E, 1, nz), T_p[c0:c0 + E].reshape(E, 1, nz), g.dz,
+                                form=form, out=outs, allow_zero_pivot=True)
 
-        for i in range(a.warmup):
-            e2e_step(i)
-        if world > 1:
-            dist.barrier()
-        lat = []
-        t0 = time.perf_counter()
-        for i in range(a.steps):
-            s0 = time.perf_counter()
-            e2e_step(i)
-            lat.append(time.perf_counter() - s0)
-        el = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([el], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
-        e2e = {"value": world * E * nz * nw * a.steps / el, "unit": "points/s",
-               "h2d_bytes_per_step": 2 * E * nz * 8, "d2h_bytes_per_step": E * nw * (mz + 2 * nz + 2) * 8,
-               "columns_per_step": E, "form": a.form, "outputs": "U, kappa, V, Vtop, Vbot (all, reference layout)",
-               "p50_ms": 1e3 * pct(lat, 0.5), "p99_ms": 1e3 * pct(lat, 0.99)}
+            for i in range(a.warmup):
+                e2e_step(i)
+            if world > 1:
+                dist.barrier()
+            lat = []
+            t0 = time.perf_counter()
+            for i in range(a.steps):
+                s0 = time.perf_counter()
+                e2e_step(i)
+                lat.append(time.perf_counter() - s0)
+            el = max_over_ranks(time.perf_counter() - t0, world, dist, dev)
+            return {"value": whole_job_rate(world, E * nz * nw, a.steps, 1e3 * el), "unit": "points/s",
+                    "h2d_bytes_per_step": 2 * E * nz * 8, "d2h_bytes_per_step": E * nw * (mz + 2 * nz + 2) * 8,
+                    "columns_per_step": E, "form": form,
+                    "outputs": "U, kappa, V, Vtop, Vbot (all, FP64, reference layout)",
+                    "p50_ms": 1e3 * pct(lat, 0.5), "p99_ms": 1e3 * pct(lat, 0.99)}
+
+        e2e = e2e_measure(a.form)
+        if world == 1 and not a.no_extra:
+            e2e_mixed = e2e_measure("mixed" if a.form != "mixed" else "plain")
         del outs
         # the same call returning only the emergent-flux planes (the spectra), whole grid per step
         if world == 1 and not a.no_extra:
             fl = {"Vtop": pin((nw, ncol, 1)), "Vbot": pin((nw, ncol, 1))}
             rho_all, T_all = rho_p.reshape(ncol, 1, nz), T_p.reshape(ncol, 1, nz)
-            for i in range(max(1, a.warmup)):
-                eng.solve_block(rho_all, T_all, g.dz, form=a.form, out=fl, want=("Vtop", "Vbot"),
-                                allow_zero_pivot=True)
-            lat = []
-            for i in range(a.steps):
-                s0 = time.perf_counter()
-                eng.solve_block(rho_all, T_all, g.dz, form=a.form, out=fl, want=("Vtop", "Vbot"),
-                                allow_zero_pivot=True)
-                lat.append(time.perf_counter() - s0)
-            extra["e2e_emergent_flux_only"] = {
-                "value": ncol * nz * nw * a.steps / sum(lat), "unit": "points/s", "form": a.form,
-                "h2d_bytes_per_step": 2 * ncol * nz * 8, "d2h_bytes_per_step": 2 * ncol * nw * 8,
-                "outputs": "Vtop, Vbot only (oco_solve_block with U, kappa, V NULL), whole grid per call",
-                "p50_ms": 1e3 * pct(lat, 0.5), "p99_ms": 1e3 * pct(lat, 0.99)}
+            for form in (a.form, "mixed"):
+                for i in range(max(1, a.warmup)):
+                    eng.solve_block(rho_all, T_all, g.dz, form=form, out=fl, want=("Vtop", "Vbot"),
+                                    allow_zero_pivot=True)
+                lat = []
+                for i in range(a.steps):
+                    s0 = time.perf_counter()
+                    eng.solve_block(rho_all, T_all, g.dz, form=form, out=fl, want=("Vtop", "Vbot"),
+                                    allow_zero_pivot=True)
+                    lat.append(time.perf_counter() - s0)
+                extra[f"e2e_emergent_flux_only_{form}"] = {
+                    "value": ncol * nz * nw * a.steps / sum(lat), "unit": "points/s", "form": form,
+                    "h2d_bytes_per_step": 2 * ncol * nz * 8, "d2h_bytes_per_step": 2 * ncol * nw * 8,
+                    "outputs": "Vtop, Vbot only (oco_solve_block with U, kappa, V NULL), whole grid per call",
+                    "p50_ms": 1e3 * pct(lat, 0.5), "p99_ms": 1e3 * pct(lat, 0.99)}
             del fl
         del rho_p, T_p
 
     if world == 1 and not a.no_extra:
-        del g.sets
+        g.sets = None
         torch.cuda.empty_cache()
         extra["batch"] = measure_batch(a, eng, dev)
         torch.cuda.empty_cache()
     if world == 1 and not a.no_extra and not a.no_serve:
-        specs = workloads.serving_stream(a.serve_jobs, a.serve_rate, seed=5)
-        arrays = [workloads.job_arrays_device(sp, dev) for sp in specs]
-        torch.cuda.synchronize(dev)
-        extra["serving"] = {"rate_jobs_per_s": a.serve_rate, "jobs": a.serve_jobs, "max_jobs_resident": 4,
-                            "latency": "submit to results complete on the device (server clock)",
-                            "stream": "Poisson (seed 5); nx=ny in {64,128,256,512}, nz U[128,1024], nw U[64,512], "
-                                      "rho0 log-uniform [1e-11,1e-7]; outputs: emergent-flux planes",
-                            "points": int(sum(sp["nx"] * sp["ny"] * sp["nz"] * sp["nw"] for sp in specs))}
-        for form in ("mixed", "plain"):
-            extra["serving"][form] = measure_serving(a, dev, form, specs, arrays)
-        del arrays
+        extra["serving"] = measure_serving_sweep(a, dev)
         torch.cuda.empty_cache()
     if world == 1 and not a.no_extra and not a.no_c3:
         extra["precision_c3"] = measure_precision_c3(a, eng, dev)
+        torch.cuda.empty_cache()
 
-    cpu = None
+    cpu, cpu1 = None, None
     if rank == 0 and world == 1 and not a.no_cpu:
+        # the CPU leg also checks the plain form against the glibc build of the oracle
+        extra["parity_vs_glibc"] = parity_vs_glibc(eng)
         procs = os.cpu_count() or 1
         v, dt, pts = cpu_baseline(g.rho_h, g.T_h, g.wa, g.dz, min(a.cpu_cols, ncol), procs)
         cpu = {"value": v, "unit": "points/s", "cores": procs, "kind": "port",
                "sample": f"first {min(a.cpu_cols, ncol)} columns of the same grid, all z and lambda "
                          f"({pts:.3g} points, {dt:.1f} s wall on {procs} processes), glibc math"}
+        v1, dt1, pts1 = cpu_baseline(g.rho_h, g.T_h, g.wa, g.dz, min(a.cpu1_cols, ncol), 1)
+        cpu1 = {"value": v1, "unit": "points/s", "cores": 1, "kind": "port",
+                "sample": f"first {min(a.cpu1_cols, ncol)} columns of the same grid, all z and lambda "
+                          f"({pts1:.3g} points, {dt1:.1f} s on one process), glibc math: the serial "
+                          "reference's setting (its published rate is 6.94e6 points/s on one core)"}
 
     if rank == 0:
-        line = {"metric": METRIC, "value": m["value"], "unit": "points/s", "n_gpus": world,
-                "steps": a.steps, "warmup": a.warmup, "ms_per_step": m["total_ms"] / a.steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": m["value"] / PUBLISHED_POINTS_PER_S,
-                "vs_baseline_source": "reference's published xy-loop rate, 6.94e6 mesh*lambda points/s (one CPU "
-                                      "core, multiInTest sample; README.md:41-42)",
-                "dtype": "f64" if a.form != "mixed" else "f32 (FP64 Saha)", "data": "synthetic",
-                "config": config_dict(a, a.form),
-                "latency_ms": {"p50": pct(m["step_ms"], 0.5), "p99": pct(m["step_ms"], 0.99)},
-                "zero_pivot_items": g.zero_pivot, "clocks": m["clocks"], "gpu_launches": int(m["launches"]),
-                "roofline": roof, "e2e": e2e, "cpu_baseline": cpu}
-        line["config"]["layout"] = a.layout
-        line["config"]["chunk_columns"] = g.CH
-        line.update(extra)
+        line = {"details": extra} if extra else {}
+        line.update(contract_line(a, world, m, g, roof, e2e, cpu))
+        if cpu1:
+            line["cpu_baseline_1core"] = cpu1
+        line.update(headline(extra, e2e_mixed, cpu1))
         print(json.dumps(line), flush=True)
     eng.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def contract_line(a, world, m, g, roof, e2e, cpu):
+    """The keys of the one-line result every run prints (value: the plain FP64 form)."""
+    line = {"metric": METRIC, "value": m["value"], "unit": "points/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": m["total_ms"] / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": m["value"] / PUBLISHED_POINTS_PER_S,
+            "vs_baseline_source": "reference's published xy-loop rate, 6.94e6 mesh*lambda points/s (one CPU "
+                                  "core, multiInTest sample; README.md:41-42)",
+            "dtype": "f64" if a.form != "mixed" else "f32 (FP64 Saha)", "data": "synthetic",
+            "config": config_dict(a, a.form),
+            "latency_ms": {"p50": pct(m["step_ms"], 0.5), "p99": pct(m["step_ms"], 0.99)},
+            "zero_pivot_items": g.zero_pivot, "clocks": m["clocks"], "gpu_launches": int(m["launches"]),
+            "roofline": roof, "e2e": e2e, "cpu_baseline": cpu}
+    line["config"]["layout"] = a.layout
+    line["config"]["chunk_columns"] = g.CH
+    line["config"]["parallelism"] = f"columns sharded over {world} rank(s), no exchange"
+    return line
+
+
+def headline(extra, e2e_mixed, cpu1):
+    """Compact top-level keys, printed last: the mixed form against the plain FP64 form on each
+    config, the mixed error bar, serving p99 at a named rate, the one-core CPU rate."""
+    h = {}
+    mx = extra.get("mixed")
+    if mx:
+        er = mx["emergent_flux_rel_err"]
+        h.update({"mixed_value": mx["value"], "mixed_ratio": mx["ratio_vs_plain_fp64"],
+                  "mixed_flux_err_max": er["all"]["max"], "mixed_flux_frac_above_1e-4": er["all"]["frac_above_1e-4"],
+                  "mixed_repaired_frac": er["repaired_frac"]})
+    if e2e_mixed:
+        h["mixed_e2e"] = e2e_mixed["value"]
+    c3 = extra.get("precision_c3")
+    if c3:
+        er = c3["emergent_flux_rel_err"]
+        h.update({"c3_mixed_value": c3["mixed_value"], "c3_mixed_ratio": c3["ratio"], "c3_flux_err_max": er["all"]["max"],
+                  "c3_flux_frac_above_1e-4": er["all"]["frac_above_1e-4"], "c3_repaired_frac": er["repaired_frac"]})
+    bt = extra.get("batch")
+    if bt:
+        h.update({"c4_mixed_value": bt["value"], "c4_mixed_ratio": bt["ratio_mixed_vs_plain"]})
+    sv = extra.get("serving")
+    if sv and sv.get("headline"):
+        h.update(sv["headline"])
+    pg = extra.get("parity_vs_glibc")
+    if pg:
+        h["glibc_parity"] = {k: pg["floor_1e-15"][k] for k in ("in_mask", "max_rel_in_mask", "class_equal")}
+    if cpu1:
+        h["cpu_1core_value"] = cpu1["value"]
+    return h
 
 
 if __name__ == "__main__":

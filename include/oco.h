@@ -127,6 +127,24 @@ int oco_solve_block_device(oco_ctx *ctx, const oco_params *p, const double *rho,
  * last call met a zero pivot. */
 int oco_synchronize(oco_ctx *ctx);
 
+/* Mixed form: the FP32 arithmetic resolves an emergent flux to ~1e-5 only where the flux is
+ * well conditioned.  The flux is a weighted sum of the boundary differences of U, computed as
+ * D_k = u_k - q_k U_{k+1} from non-negative terms, and its condition number is
+ * sum |w_k| (u_k + q_k U_{k+1}) / |sum w_k D_k|.  The solve kernels compute it for every item
+ * (top and bottom) and re-solve an item whose condition number exceeds cond_max in the stable
+ * FP64 form, in place, before the item's results are final.  Default 100 (the kernel's error
+ * grows as ~1e-5 + 2e-7 x condition number); cond_max >= 3e38 turns the re-solve off; values
+ * below 1 are refused.  Block solves use the value current at the call; a batch uses the
+ * value current when its graph is captured (oco_batch_bind, _tune, _set_tiling).  No reference
+ * counterpart: the reference computes in FP64 only. */
+int oco_set_mixed_repair(oco_ctx *ctx, double cond_max);
+
+/* Waits for the context's work and returns in *items the number of (column, wavelength) items
+ * the mixed form re-solved in FP64 since the previous call (or since creation) in the
+ * context's block solves and batches; resets the count.  Batches replayed on other streams
+ * must have been waited for (oco_batch_wait). */
+int oco_mixed_repairs(oco_ctx *ctx, int64_t *items);
+
 /* Number of kernel launches this context has issued since creation (for accounting). */
 int64_t oco_kernel_launches(const oco_ctx *ctx);
 

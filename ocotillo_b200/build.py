@@ -36,7 +36,7 @@ UNITS = [
 ]
 HOST_UNITS = [("oco_deck.cpp", [])]
 
-HEADERS = ["ocomath.h", "ocomath_tables.h", "oco_consts.h", "oco_internal.h", "oco_ctx.h", "mixed_core.h",
+HEADERS = ["ocomath.h", "ocomath_tables.h", "oco_consts.h", "oco_internal.h", "oco_ctx.h", "mixed_core.h", "fp64_core.h",
            "batch_layout.h", "fortran_records.h"]
 
 

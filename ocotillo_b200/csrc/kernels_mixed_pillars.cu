@@ -5,6 +5,7 @@
  *                          in FP64, written as the FP32 log2 record of mixed_core.h (MixedZ,
  *                          256 B; large logarithms as integer + fraction).
  *   k_pillars_mixed_batch  the same for the columns of a ragged batch.
+ * Both mark the columns that the solve kernels must re-solve in FP64 (mx::pillar).
  *
  * Compiled with -fmad=false like the FP64 kernels: the Saha quadratic
  * 0.5*(sqrt(C^2 + 4C) - C) (gas_state.f90:63) cancels as the gas approaches full ionization
@@ -20,12 +21,15 @@
 namespace oco {
 using namespace oco::mx;
 
+/* colflag[col] is set to 1 when a cell of the column has a negative neutral fraction (see
+ * mx::pillar); the caller clears it first. */
 __global__ void __launch_bounds__(256) k_pillars_mixed(const double *__restrict__ rho, const double *__restrict__ T,
-                                                       int64_t n, double fully_ionized_T, float *__restrict__ rec) {
+                                                       int64_t n, int nz, double fully_ionized_T, float *__restrict__ rec,
+                                                       unsigned *__restrict__ colflag) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   float r[MZN];
-  pillar(rho[i], T[i], fully_ionized_T, r);
+  if (pillar(rho[i], T[i], fully_ionized_T, r)) colflag[i / nz] = 1u;
   float4 *o = reinterpret_cast<float4 *>(rec + i * MZN);
 #pragma unroll
   for (int k = 0; k < MZN / 4; k++) o[k] = make_float4(r[4 * k], r[4 * k + 1], r[4 * k + 2], r[4 * k + 3]);
@@ -34,10 +38,10 @@ __global__ void __launch_bounds__(256) k_pillars_mixed(const double *__restrict_
 static_assert(MZN == MIXED_ZN, "mixed record size");
 
 cudaError_t launch_pillars_mixed(const double *rho, const double *T, int64_t ncol, int nz, double fully_ionized_T,
-                                 float *rec, cudaStream_t s) {
+                                 float *rec, unsigned *colflag, cudaStream_t s) {
   const int64_t n = ncol * nz;
   if (n == 0) return cudaSuccess;
-  k_pillars_mixed<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(rho, T, n, fully_ionized_T, rec);
+  k_pillars_mixed<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(rho, T, n, nz, fully_ionized_T, rec, colflag);
   return cudaGetLastError();
 }
 
@@ -48,7 +52,7 @@ __global__ void __launch_bounds__(256) k_pillars_mixed_batch(const double *__res
                                                              const MBatchCol *__restrict__ cols,
                                                              const int64_t *__restrict__ rec_pre, int64_t ncol,
                                                              int64_t n, double fully_ionized_T,
-                                                             float *__restrict__ rec) {
+                                                             float *__restrict__ rec, unsigned *__restrict__ colflag) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   int64_t lo = 0, hi = ncol;
@@ -61,7 +65,7 @@ __global__ void __launch_bounds__(256) k_pillars_mixed_batch(const double *__res
   }
   const int64_t src = cols[lo].in_off + (i - rec_pre[lo]);
   float r[MZN];
-  pillar(rho[src], T[src], fully_ionized_T, r);
+  if (pillar(rho[src], T[src], fully_ionized_T, r)) colflag[lo] = 1u;
   float4 *o = reinterpret_cast<float4 *>(rec + i * MZN);
 #pragma unroll
   for (int k = 0; k < MZN / 4; k++) o[k] = make_float4(r[4 * k], r[4 * k + 1], r[4 * k + 2], r[4 * k + 3]);
@@ -69,10 +73,10 @@ __global__ void __launch_bounds__(256) k_pillars_mixed_batch(const double *__res
 
 cudaError_t launch_pillars_mixed_batch(const double *rho, const double *T, const MBatchCol *cols,
                                        const int64_t *rec_pre, int64_t ncol, int64_t nrec, double fully_ionized_T,
-                                       float *rec, cudaStream_t s) {
+                                       float *rec, unsigned *colflag, cudaStream_t s) {
   if (nrec == 0) return cudaSuccess;
   k_pillars_mixed_batch<<<(unsigned)((nrec + 255) / 256), 256, 0, s>>>(rho, T, cols, rec_pre, ncol, nrec,
-                                                                       fully_ionized_T, rec);
+                                                                       fully_ionized_T, rec, colflag);
   return cudaGetLastError();
 }
 

@@ -169,7 +169,13 @@ MX_HD void put_l2(double v, float *o) {
 }
 
 /* ---- per-(column, z) record (gas_state.f90:30-110, c_o :143-163) ------------------------ */
-MX_HD void pillar(double r, double t, double fully_ionized_T, float *o) {
+/* Returns true when the cell's neutral hydrogen density is negative.  The reference's Saha root
+ * 0.5*(sqrt(C^2 + 4C) - C) (gas_state.f90:63) cancels for large C and can round above 1 below
+ * fully_ionized_T; nHI = n - nHII and ionf are then negative, and the reference's opacity terms
+ * proportional to ionf (continuous_opacity.f90:237-244, :318-322, :337-339, :265) turn negative.
+ * Logarithms cannot carry that (the record holds such terms as vanishing): a column with such a
+ * cell is solved in FP64 instead. */
+MX_HD bool pillar(double r, double t, double fully_ionized_T, float *o) {
   using namespace oco::k;
   const double rho1 = 1.0 / r, T1 = 1.0 / t;
   double c_ion = (mp * rho1) * (saha_const * oco_pow(t, 1.5) * oco_exp(-((T1 * hydrogen_ionization_eV) * k1_eV)));
@@ -222,6 +228,7 @@ MX_HD void pillar(double r, double t, double fully_ionized_T, float *o) {
   o[MZ_T1] = (float)(T1);
   split2(damping_factor_const * T1, o[MZ_DFT1], o[MZ_DFT1L]);
   for (int k2 = MZ_END; k2 < MZN; k2++) o[k2] = 0.0f;
+  return nHI < 0.0;
 }
 
 /* ---- per-wavelength record from the FP64 table entries --------------------------------- */

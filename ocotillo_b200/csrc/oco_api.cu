@@ -67,6 +67,9 @@ extern "C" int oco_create(oco_ctx **out, int device) {
     e = cudaEventCreateWithFlags(&c->stage[i].done, cudaEventDisableTiming);
   if (e == cudaSuccess) e = c->work.ensure(64);
   if (e == cudaSuccess) e = c->status.ensure(64);
+  if (e == cudaSuccess) e = c->stats.ensure(64);
+  if (e == cudaSuccess) e = cudaMemset(c->stats.p, 0, 64);
+  c->repair_cond = MIXED_REPAIR_COND;
   if (e != cudaSuccess) {
     int code = oco_set_err(nullptr, OCO_ECUDA, "oco_create: %s", cudaGetErrorString(e));
     oco_destroy(c);
@@ -97,6 +100,9 @@ extern "C" void oco_destroy(oco_ctx *c) {
   c->tmpV.release();
   c->work.release();
   c->status.release();
+  c->scratch64.release();
+  c->stats.release();
+  c->colflag.release();
   for (auto &s : c->stage) {
     s.rho.release();
     s.T.release();
@@ -291,7 +297,8 @@ static int check_params(oco_ctx *c, const oco_params *p) {
 static const int kSolveThreads = 128;
 
 /* Grid of the persistent solve kernel and its scratch: per resident thread and z, FP64
- * gamma, u, 1/kappa, q (32 B) or, for the mixed form, one float4 (16 B). */
+ * gamma, u, 1/kappa, q (32 B) or, for the mixed form, one float4 (16 B) plus the 32 B of the
+ * FP64 re-solve of flagged items. */
 static int prepare_solve(oco_ctx *c, int form, int grey, int64_t nitems, int nz, int *blocks) {
   const bool mixed = form == OCO_FORM_MIXED;
   int bps = mixed ? solve_mixed_max_blocks_per_sm(kSolveThreads, c->nw)
@@ -302,6 +309,7 @@ static int prepare_solve(oco_ctx *c, int form, int grey, int64_t nitems, int nz,
   *blocks = (int)std::max<int64_t>(1, std::min(maxb, need));
   size_t slots = (size_t)(*blocks) * kSolveThreads;
   CU(c->scratch.ensure(slots * (size_t)nz * (mixed ? 16 : 4 * sizeof(double))));
+  if (mixed) CU(c->scratch64.ensure(slots * (size_t)nz * 4 * sizeof(double))); /* FP64 re-solves */
   return OCO_OK;
 }
 
@@ -345,7 +353,9 @@ static int run_chunk_mixed(oco_ctx *c, const oco_params *p, const double *rho, c
     CU(cudaEventRecord(e0, s));
   }
   float *rec = c->pil.as<float>();
-  CU(launch_pillars_mixed(rho, T, nb, p->nz, p->fully_ionized_T, rec, s));
+  CU(c->colflag.ensure((size_t)nb * sizeof(unsigned)));
+  CU(cudaMemsetAsync(c->colflag.p, 0, (size_t)nb * sizeof(unsigned), s));
+  CU(launch_pillars_mixed(rho, T, nb, p->nz, p->fully_ionized_T, rec, c->colflag.as<unsigned>(), s));
   if (c->prof) {
     CU(cudaEventRecord(e1, s));
     c->ev_pil.emplace_back(e0, e1);
@@ -371,6 +381,14 @@ static int run_chunk_mixed(oco_ctx *c, const oco_params *p, const double *rho, c
   a.slot_stride = (int64_t)slots;
   a.work = c->work.as<unsigned long long>();
   a.status = c->status.as<unsigned long long>();
+  a.rho = rho;
+  a.T = T;
+  a.lam64 = c->lam.as<double>();
+  a.fully_ionized_T = p->fully_ionized_T;
+  a.s64 = c->scratch64.as<double>();
+  a.repair_cond = c->repair_cond;
+  a.repairs = c->stats.as<unsigned long long>();
+  a.colflag = c->colflag.as<unsigned>();
   CU(cudaMemsetAsync(a.work, 0, sizeof(unsigned long long), s));
   if (c->prof) CU(cudaEventRecord(e2, s));
   CU(launch_solve_mixed(a, blocks, kSolveThreads, s));
@@ -656,6 +674,25 @@ extern "C" int oco_synchronize(oco_ctx *c) {
   }
   CU(cudaStreamSynchronize(c->stream));
   CU(cudaStreamSynchronize(c->copy));
+  return OCO_OK;
+}
+
+extern "C" int oco_set_mixed_repair(oco_ctx *c, double cond_max) {
+  if (!c) return oco_set_err(nullptr, OCO_EINVAL, "NULL context");
+  if (!(cond_max >= 1.0)) return oco_set_err(c, OCO_EINVAL, "cond_max must be at least 1 (got %g)", cond_max);
+  c->repair_cond = cond_max >= 3.0e38 ? INFINITY : (float)cond_max;
+  return OCO_OK;
+}
+
+extern "C" int oco_mixed_repairs(oco_ctx *c, int64_t *items) {
+  if (!c || !items) return oco_set_err(c, OCO_EINVAL, "NULL argument");
+  CU(cudaSetDevice(c->device));
+  if (c->status_pending) CU(cudaStreamSynchronize(c->status_stream));
+  CU(cudaStreamSynchronize(c->stream));
+  unsigned long long n = 0;
+  CU(cudaMemcpy(&n, c->stats.p, sizeof n, cudaMemcpyDeviceToHost));
+  CU(cudaMemset(c->stats.p, 0, sizeof n));
+  *items = (int64_t)n;
   return OCO_OK;
 }
 

@@ -52,6 +52,7 @@ struct oco_batch {
      Vtop and Vbot), {-1, -1} if none: binding an array of an overlapping family fails */
   int64_t overlap[3][2] = {{-1, -1}, {-1, -1}, {-1, -1}};
   DevBuf cols, rec_pre, tasks, order, item_pre, lam, rec, scratch, work, status;
+  DevBuf lam64, scratch64, colflag; /* mixed form: FP64 tables, scratch and column marks of the re-solve */
   int64_t slots = 0; /* scratch slots (threads of the largest persistent grid) */
   int tiling = OCO_TILING_WARP_COLUMN, bps = 1, max_bps[2] = {1, 1}; /* max_bps 0: tiling not available */
   /* bound arrays */
@@ -89,6 +90,14 @@ static MixedBatchArgs batch_args(const oco_batch *b) {
   a.max_nz = b->max_nz;
   a.work = b->work.as<unsigned long long>();
   a.status = b->status.as<unsigned long long>();
+  a.rho = b->rho;
+  a.T = b->T;
+  a.lam64 = b->lam64.as<double>();
+  a.fully_ionized_T = b->fully_ionized_T;
+  a.s64 = b->scratch64.as<double>();
+  a.repair_cond = b->c->repair_cond;
+  a.repairs = b->c->stats.as<unsigned long long>();
+  a.colflag = b->colflag.as<unsigned>();
   return a;
 }
 
@@ -126,8 +135,9 @@ static int enqueue_run(oco_batch *b, cudaStream_t s) {
   CU(cudaMemsetAsync(b->status.as<unsigned long long>() + 1, 0xff, sizeof(unsigned long long), s)); /* atomicMin */
   const int blocks = b->bps * c->num_sms;
   if (b->form == OCO_FORM_MIXED) {
+    CU(cudaMemsetAsync(b->colflag.p, 0, (size_t)b->ncol * sizeof(unsigned), s));
     CU(launch_pillars_mixed_batch(b->rho, b->T, b->cols.as<MBatchCol>(), b->rec_pre.as<int64_t>(), b->ncol, b->nrec,
-                                  b->fully_ionized_T, b->rec.as<float>(), s));
+                                  b->fully_ionized_T, b->rec.as<float>(), b->colflag.as<unsigned>(), s));
     const MixedBatchArgs a = batch_args(b);
     CU(launch_batch_mixed(a, b->tiling == OCO_TILING_PACKED ? BATCH_TILING_PACKED : BATCH_TILING_WARP_COLUMN, blocks,
                           kBatchThreads, s));
@@ -229,10 +239,11 @@ static int batch_create(oco_ctx *c, const oco_batch_column *cols, int64_t ncol, 
       if (fp64) {
         loff = (int64_t)lam64.size();
         lam64.insert(lam64.end(), tab.begin(), tab.end());
-      } else {
+      } else { /* mixed tables; the FP64 ones follow in step (offset lam_off / MIXED_LN * NL) */
         loff = (int64_t)lam.size();
         lam.resize(lam.size() + (size_t)MIXED_LN * q.nw);
         fill_mixed_lambda_table(tab.data(), q.nw, lam.data() + loff);
+        lam64.insert(lam64.end(), tab.begin(), tab.end());
       }
       grids.emplace(key, loff);
     } else {
@@ -318,6 +329,9 @@ static int batch_create(oco_ctx *c, const oco_batch_column *cols, int64_t ncol, 
     CU(b->lam.ensure(lam.size() * sizeof(float)));
     CU(b->rec.ensure((size_t)b->nrec * MIXED_ZN * sizeof(float)));
     CU(b->scratch.ensure((size_t)b->slots * b->max_nz * sizeof(float4)));
+    CU(b->lam64.ensure(lam64.size() * sizeof(double)));
+    CU(b->scratch64.ensure((size_t)4 * b->slots * b->max_nz * sizeof(double)));
+    CU(b->colflag.ensure((size_t)ncol * sizeof(unsigned)));
   }
   CU(b->work.ensure(64));
   CU(b->status.ensure(64));
@@ -328,8 +342,10 @@ static int batch_create(oco_ctx *c, const oco_batch_column *cols, int64_t ncol, 
   CU(cudaMemcpy(b->item_pre.p, ipre.data(), ipre.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
   if (fp64)
     CU(cudaMemcpy(b->lam.p, lam64.data(), lam64.size() * sizeof(double), cudaMemcpyHostToDevice));
-  else
+  else {
     CU(cudaMemcpy(b->lam.p, lam.data(), lam.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(b->lam64.p, lam64.data(), lam64.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
   CU(cudaMemset(b->status.p, 0, 64));
 
   b->info.ncol = ncol;
@@ -506,7 +522,7 @@ extern "C" void oco_batch_destroy(oco_batch *b) {
   if (b->pending) cudaStreamSynchronize(b->last); /* a null stream is the default stream */
   if (b->cap) cudaStreamSynchronize(b->cap);
   drop_graph(b);
-  for (DevBuf *d : {&b->cols, &b->rec_pre, &b->tasks, &b->order, &b->item_pre, &b->lam, &b->rec, &b->scratch,
+  for (DevBuf *d : {&b->lam64, &b->scratch64, &b->colflag, &b->cols, &b->rec_pre, &b->tasks, &b->order, &b->item_pre, &b->lam, &b->rec, &b->scratch,
                     &b->work, &b->status})
     d->release();
   if (b->after_last) cudaEventDestroy(b->after_last);

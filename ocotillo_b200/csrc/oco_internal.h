@@ -123,6 +123,15 @@ struct MixedArgs {
   int64_t slot_stride; /* resident threads the scratch is sized for */
   unsigned long long *work;
   unsigned long long *status;
+  /* FP64 re-solve (stable form) of the items whose emergent flux the FP32 arithmetic cannot
+   * resolve: a warp that flags items re-solves them at once, in place */
+  const double *rho, *T; /* the chunk's inputs [ncol][nz] */
+  const double *lam64;   /* [NL][nw] FP64 wavelength table */
+  double fully_ionized_T;
+  double *s64;           /* FP64 scratch [warp slot][4][nz][32]: gamma, u, 1/kappa, q */
+  float repair_cond;     /* re-solve when the boundary-flux condition number exceeds this */
+  unsigned long long *repairs; /* [0] items re-solved in FP64 (accumulates) */
+  const unsigned *colflag;     /* [ncol] columns re-solved in FP64 entirely (record kernel) */
 };
 
 /* One column of a ragged batch as the batch kernels see it (built from oco_batch_column). */
@@ -156,6 +165,14 @@ struct MixedBatchArgs {
   int max_nz;
   unsigned long long *work;
   unsigned long long *status;
+  /* FP64 re-solve of ill-conditioned items (as in MixedArgs) */
+  const double *rho, *T;   /* the bound inputs (column profiles at in_off) */
+  const double *lam64;     /* packed [NL][nw] FP64 tables: a column's starts at lam_off / MIXED_LN * NL */
+  double fully_ionized_T;
+  double *s64;             /* FP64 scratch [warp slot][4][max_nz][32] */
+  float repair_cond;
+  unsigned long long *repairs;
+  const unsigned *colflag; /* [ncol] columns re-solved in FP64 entirely */
 };
 
 /* Arguments of the ragged-batch kernels (plain and stable FP64 forms; warp-column tiling). */
@@ -184,7 +201,7 @@ constexpr int BATCH_TILING_PACKED = 1;      /* a warp solves 32 consecutive item
 
 cudaError_t launch_pillars_mixed_batch(const double *rho, const double *T, const MBatchCol *cols,
                                        const int64_t *rec_pre, int64_t ncol, int64_t nrec, double fully_ionized_T,
-                                       float *rec, cudaStream_t s);
+                                       float *rec, unsigned *colflag, cudaStream_t s);
 cudaError_t launch_batch_mixed(const MixedBatchArgs &a, int tiling, int blocks, int threads, cudaStream_t s);
 int batch_mixed_max_blocks_per_sm(int tiling, int threads);
 
@@ -226,9 +243,14 @@ cudaError_t launch_bounded_wait_check(long long limit, unsigned long long *statu
 
 /* Mixed-precision kernels (kernels_mixed.cu). */
 constexpr int MIXED_ZN = 64; /* floats per mixed record */
+/* Default condition number of the mixed form's emergent flux above which an item is re-solved
+ * in FP64 (stable form): the flux is a weighted sum of boundary differences D_k = u_k - q_k
+ * U_{k+1}, and its condition number is sum |w_k| (u_k + q_k U_{k+1}) / |sum w_k D_k|. */
+constexpr float MIXED_REPAIR_COND = 100.0f;
 constexpr int MIXED_LN = 29; /* fields of the mixed wavelength table */
+/* colflag[ncol] (cleared by the caller) marks columns to re-solve in FP64 (mx::pillar). */
 cudaError_t launch_pillars_mixed(const double *rho, const double *T, int64_t ncol, int nz, double fully_ionized_T,
-                                 float *rec, cudaStream_t s);
+                                 float *rec, unsigned *colflag, cudaStream_t s);
 cudaError_t launch_solve_mixed(const MixedArgs &a, int blocks, int threads, cudaStream_t s);
 int solve_mixed_max_blocks_per_sm(int threads, int nw); /* occupancy of the kernel used for nw */
 /* Fills tab32[MIXED_LN*nw] from the FP64 table tab[NL*nw]. */

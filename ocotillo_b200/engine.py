@@ -114,6 +114,8 @@ def load_library(path=None):
         "oco_solve_block": (I, [V, P, _DP, _DP, _DP, _DP, _DP, _DP, _DP]),
         "oco_solve_block_device": (I, [V, P, V, V, V, V, V, V, V, V]),
         "oco_synchronize": (I, [V]),
+        "oco_set_mixed_repair": (I, [V, D]),
+        "oco_mixed_repairs": (I, [V, ctypes.POINTER(ctypes.c_int64)]),
         "oco_kernel_launches": (ctypes.c_int64, [V]),
         "oco_check_bounded_wait": (I, [V, ctypes.c_int64]),
         "oco_integrated_flux_device": (I, [V, P, V, V, V]),
@@ -365,6 +367,17 @@ class Engine:
 
     def synchronize(self):
         self._check(self.lib.oco_synchronize(self.ctx))
+
+    def set_mixed_repair(self, cond_max=100.0):
+        """Condition number of a mixed-form emergent flux above which the item is re-solved in the
+        stable FP64 form (float('inf') turns the re-solve off)."""
+        self._check(self.lib.oco_set_mixed_repair(self.ctx, min(float(cond_max), 3.4e38)))
+
+    def mixed_repairs(self):
+        """Items the mixed form re-solved in FP64 since the previous call (waits for the work)."""
+        n = ctypes.c_int64(0)
+        self._check(self.lib.oco_mixed_repairs(self.ctx, ctypes.byref(n)))
+        return n.value
 
     def intensities_device(self, U, V, shape, nw, out, layout=LAYOUT_REFERENCE, stream=None):
         """Ip = U + V, Im = U - V (calc_intensity) on torch CUDA tensors of a solved block of
@@ -660,16 +673,24 @@ class Server:
     def wait(self, jid, timeout=3600.0):
         self._check(self.lib.oco_server_wait(self.h, int(jid), float(timeout)))
 
-    def fetch(self, jid, fields=None):
+    def fetch(self, jid, fields=None, out=None):
         """Results of a done job as numpy arrays: Vtop, Vbot (nw, nx, ny) and, if the job kept
-        them (or fields=True), U (nw, nx, ny, nz+6), kappa and V (nw, nx, ny, nz).  Releases the job."""
+        them (or fields=True), U (nw, nx, ny, nz+6), kappa and V (nw, nx, ny, nz).  `out` may
+        supply the destination arrays by name (e.g. views of pinned memory; C-contiguous
+        float64 with exactly those element counts).  Releases the job."""
         _, _, (nx, ny, nz, nw), kept = self._jobs[jid]
         fields = kept if fields is None else fields
-        out = {"Vtop": np.empty((nw, nx, ny)), "Vbot": np.empty((nw, nx, ny))}
+        shapes = {"Vtop": (nw, nx, ny), "Vbot": (nw, nx, ny)}
         if fields:
-            out["U"] = np.empty((nw, nx, ny, nz + 6))
-            out["kappa"] = np.empty((nw, nx, ny, nz))
-            out["V"] = np.empty((nw, nx, ny, nz))
+            shapes.update({"U": (nw, nx, ny, nz + 6), "kappa": (nw, nx, ny, nz), "V": (nw, nx, ny, nz)})
+        given = out or {}
+        out = {}
+        for k, shp in shapes.items():
+            if k in given:
+                _need_host(k, given[k], int(np.prod(shp)))
+                out[k] = given[k]
+            else:
+                out[k] = np.empty(shp)
         self._check(self.lib.oco_server_fetch(self.h, int(jid), _ptr(out["Vtop"]), _ptr(out["Vbot"]),
                                               _ptr(out.get("U")), _ptr(out.get("kappa")), _ptr(out.get("V"))))
         del self._jobs[jid]
