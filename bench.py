@@ -223,13 +223,15 @@ class Grid:
         self.a, self.eng, self.dev = a, eng, dev
         nx, ny, nz, nw = a.nx, a.ny, a.nz, a.nw
         self.ncol, self.nz, self.nw, self.mz = nx * ny, nz, nw, nz + 6
-        if workload == "precision":  # rho0 log-uniform in [1e-11, 1e-7] (seed 3), else as the AGN grid
-            self.rho_h, self.T_h, self.dz, self.rho0 = workloads.precision_block(nx, ny, nz, seed=3 + rank)
+        if workload == "precision":  # rho0 log-uniform in [1e-11, 1e-7] (seed 3), generated on the device
+            r, t, self.dz, self.rho0 = workloads.precision_block_device(eng, nx, ny, nz, seed=3 + rank)
+            self.rho, self.T = r.reshape(self.ncol, nz), t.reshape(self.ncol, nz)
+            self.rho_h = self.T_h = None
         else:
             self.rho_h, self.T_h, self.dz = workloads.agn_block(nx, ny, nz, seed=2 + rank)
+            self.rho = torch.from_numpy(self.rho_h).to(dev).reshape(self.ncol, nz)
+            self.T = torch.from_numpy(self.T_h).to(dev).reshape(self.ncol, nz)
         self.wa = workloads.log_wavelengths(nw)
-        self.rho = torch.from_numpy(self.rho_h).to(dev).reshape(self.ncol, nz)
-        self.T = torch.from_numpy(self.T_h).to(dev).reshape(self.ncol, nz)
         self.layout = LAYOUT_REFERENCE if a.layout == "reference" else LAYOUT_LAMBDA_FASTEST
         self.CH = min(a.chunk_cols, self.ncol)
         if self.ncol % self.CH:
@@ -539,7 +541,7 @@ def measure_precision_c3(a, eng, dev):
     return res
 
 
-def run_stream(dev, form, specs, arrays, pinned):
+def run_stream(eng, dev, form, specs, arrays, pinned):
     """Runs one job stream through a fresh server: each job is submitted at its arrival time,
     and every finished job is fetched at once (emergent-flux planes into pinned host memory).
     Per job: device latency (submit -> results complete on the device, server clock), fetch
@@ -547,7 +549,7 @@ def run_stream(dev, form, specs, arrays, pinned):
     import torch
     from ocotillo_b200 import Server, workloads
     srv = Server(dev.index or 0, max_jobs=4, max_nz=1024, reserve_bytes=24e9)
-    wr, wt, _ = workloads.job_arrays_device({"nx": 8, "ny": 8, "nz": 128, "nw": 64, "rho0": 1e-9, "seed": 1}, dev)
+    wr, wt, _ = workloads.job_arrays_device({"nx": 8, "ny": 8, "nz": 128, "nw": 64, "rho0": 1e-9, "seed": 1}, eng)
     jid = srv.submit(wr, wt, workloads.log_wavelengths(64), 1e16 / 127, form=form)  # warm-up
     srv.wait(jid)
     srv.fetch(jid)
@@ -600,7 +602,7 @@ def run_stream(dev, form, specs, arrays, pinned):
                                        "fetch_p99_ms": pct([x[1] for x in v], 0.99)} for n, v in sorted(cls.items())}}
 
 
-def measure_serving_sweep(a, dev):
+def measure_serving_sweep(a, eng, dev):
     """Config 'serving form': the Poisson job stream (seed 5) at rising arrival rates.  The
     saturation rate comes from the same jobs all submitted at once (jobs / makespan); the mixed
     form then runs at 0.3, 0.5, 0.7 and 0.9 of its saturation rate and the plain FP64 form at half
@@ -610,7 +612,7 @@ def measure_serving_sweep(a, dev):
     from ocotillo_b200 import workloads
     n = a.serve_jobs
     base = workloads.serving_stream(n, 1.0, seed=5)
-    arrays = [workloads.job_arrays_device(sp, dev) for sp in base]
+    arrays = [workloads.job_arrays_device(sp, eng) for sp in base]
     torch.cuda.synchronize(dev)
     maxn = max(sp["nw"] * sp["nx"] * sp["ny"] for sp in base)
     pinned = [torch.empty(maxn, dtype=torch.float64, pin_memory=True).numpy() for _ in range(2)]
@@ -622,12 +624,13 @@ def measure_serving_sweep(a, dev):
     fracs = {"mixed": (0.3, 0.5, 0.7, 0.9), "plain": (0.5,)}
     for form in ("mixed", "plain"):
         sat_specs = [dict(sp, arrival_s=0.0) for sp in base]
-        sat = run_stream(dev, form, sat_specs, arrays, pinned)
+        sat = run_stream(eng, dev, form, sat_specs, arrays, pinned)
         sat_rate = n / sat["makespan_s"]
         runs = {"saturation": dict(sat, rate_jobs_per_s=sat_rate)}
         for f in fracs[form]:
             specs = [dict(sp, arrival_s=sp["arrival_s"] / (f * sat_rate)) for sp in base]
-            runs[f"{f:g}x_saturation"] = dict(run_stream(dev, form, specs, arrays, pinned), rate_jobs_per_s=f * sat_rate)
+            runs[f"{f:g}x_saturation"] = dict(run_stream(eng, dev, form, specs, arrays, pinned),
+                                              rate_jobs_per_s=f * sat_rate)
         res[form] = runs
     del arrays
     torch.cuda.empty_cache()
@@ -798,7 +801,7 @@ def main():
         extra["batch"] = measure_batch(a, eng, dev)
         torch.cuda.empty_cache()
     if world == 1 and not a.no_extra and not a.no_serve:
-        extra["serving"] = measure_serving_sweep(a, dev)
+        extra["serving"] = measure_serving_sweep(a, eng, dev)
         torch.cuda.empty_cache()
     if world == 1 and not a.no_extra and not a.no_c3:
         extra["precision_c3"] = measure_precision_c3(a, eng, dev)

@@ -178,6 +178,29 @@ int oco_optical_depth_device(oco_ctx *ctx, const oco_params *p, const double *ka
  * Enqueued on `stream`. */
 int oco_integrated_flux_device(oco_ctx *ctx, const oco_params *p, const double *V, double *F, void *stream);
 
+/* ---- Synthetic disk inputs ---------------------------------------------------------------
+ * The reference's synthetic disk (source/disk.f90:42-129: calc_grid, calc_density with its
+ * floor, calc_temperature with switchTemp = (1 + 2^-52)*isoTemp, the Gaussian and the floor),
+ * every column the same profile, times a seeded lognormal perturbation of the density per cell
+ * (10^(sigma_dex*N), N standard normal from Philox4x32-10 keyed by seed and counted by cell;
+ * sigma_dex = 0: none).  The reference evaluates exp with the C library; here both builds use
+ * the library's correctly rounded exp so that host and device give the same bits. */
+typedef struct oco_disk_params {
+  int32_t nx, ny, nz;
+  int32_t reserved;  /* must be 0 */
+  double z0, z1;     /* &input z0, z1 (cm): the grid of calc_grid */
+  double rho0, H, rho_floor;                   /* &density_input */
+  double midTemp, sigma, floorTemp, isoTemp;   /* &temperature_input */
+  double sigma_dex;  /* lognormal density perturbation (dex) */
+  uint64_t seed;
+} oco_disk_params;
+
+/* Fills host arrays rho, T (nz, ny, nx) and *dz (may be NULL).  No GPU needed. */
+int oco_disk_inputs(const oco_disk_params *p, double *rho, double *T, double *dz);
+
+/* Same on device arrays, enqueued on `stream`; bit-identical to oco_disk_inputs. */
+int oco_disk_inputs_device(oco_ctx *ctx, const oco_disk_params *p, double *rho, double *T, void *stream);
+
 /* Diagnostic of the failure path: runs the kernels' bounded wait (the mbarrier poll the
  * solve kernels use for their shared-memory copies) on a barrier phase that nothing
  * completes, polling spin_limit times.  Returns OCO_ETIMEDOUT when the wait ran out, as a

@@ -9,9 +9,9 @@ raises.
 from .engine import (Engine, Batch, Server, OcoError, FORM_PLAIN, FORM_STABLE, FORM_MIXED, LAYOUT_REFERENCE,
                      LAYOUT_LAMBDA_FASTEST, TILING_WARP_COLUMN, TILING_PACKED, calc_wavelength,
                      dense_batch_offsets, batch_offsets, load_library, format_e, deck_block_inputs, run_deck,
-                     read_fortran_records)
+                     read_fortran_records, disk_inputs, disk_params)
 
 __all__ = ["Engine", "Batch", "Server", "OcoError", "FORM_PLAIN", "FORM_STABLE", "FORM_MIXED", "LAYOUT_REFERENCE",
            "LAYOUT_LAMBDA_FASTEST", "TILING_WARP_COLUMN", "TILING_PACKED", "calc_wavelength",
            "dense_batch_offsets", "batch_offsets", "load_library", "format_e", "deck_block_inputs", "run_deck",
-           "read_fortran_records"]
+           "read_fortran_records", "disk_inputs", "disk_params"]

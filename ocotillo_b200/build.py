@@ -32,11 +32,12 @@ UNITS = [
     ("oco_noalloc.cu", []),
     ("oco_batch.cu", []),
     ("kernels_epilogue.cu", ["-fmad=false"]),
+    ("kernels_inputs.cu", ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
     ("oco_server.cu", []),
 ]
 HOST_UNITS = [("oco_deck.cpp", [])]
 
-HEADERS = ["ocomath.h", "ocomath_tables.h", "oco_consts.h", "oco_internal.h", "oco_ctx.h", "mixed_core.h", "fp64_core.h",
+HEADERS = ["ocomath.h", "ocomath_tables.h", "oco_consts.h", "oco_internal.h", "oco_ctx.h", "mixed_core.h", "fp64_core.h", "disk_core.h",
            "batch_layout.h", "fortran_records.h"]
 
 

@@ -90,6 +90,16 @@ class OcoDeckInfo(ctypes.Structure):
                 ("lread_athena", ctypes.c_int32), ("reserved", ctypes.c_int32), ("dz", ctypes.c_double),
                 ("sigma_grey", ctypes.c_double), ("fully_ionized_T", ctypes.c_double)]
 
+class OcoDiskParams(ctypes.Structure):
+    """oco_disk_params: the reference's synthetic disk (disk.f90:42-129) plus a seeded lognormal
+    density perturbation."""
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("z0", ctypes.c_double), ("z1", ctypes.c_double), ("rho0", ctypes.c_double), ("H", ctypes.c_double),
+                ("rho_floor", ctypes.c_double), ("midTemp", ctypes.c_double), ("sigma", ctypes.c_double),
+                ("floorTemp", ctypes.c_double), ("isoTemp", ctypes.c_double), ("sigma_dex", ctypes.c_double),
+                ("seed", ctypes.c_uint64)]
+
+
 _LIB = None
 _DP = ctypes.POINTER(ctypes.c_double)
 
@@ -115,6 +125,8 @@ def load_library(path=None):
         "oco_solve_block_device": (I, [V, P, V, V, V, V, V, V, V, V]),
         "oco_synchronize": (I, [V]),
         "oco_set_mixed_repair": (I, [V, D]),
+        "oco_disk_inputs": (I, [ctypes.POINTER(OcoDiskParams), _DP, _DP, _DP]),
+        "oco_disk_inputs_device": (I, [V, ctypes.POINTER(OcoDiskParams), V, V, V]),
         "oco_mixed_repairs": (I, [V, ctypes.POINTER(ctypes.c_int64)]),
         "oco_kernel_launches": (ctypes.c_int64, [V]),
         "oco_check_bounded_wait": (I, [V, ctypes.c_int64]),
@@ -373,6 +385,21 @@ class Engine:
         stable FP64 form (float('inf') turns the re-solve off)."""
         self._check(self.lib.oco_set_mixed_repair(self.ctx, min(float(cond_max), 3.4e38)))
 
+    def disk_inputs_device(self, rho, T, disk, stream=None):
+        """Fills torch CUDA float64 tensors rho, T of shape (nx, ny, nz) with the synthetic disk of
+        `disk` (a dict of disk_params' keys), on the device; returns dz."""
+        import torch
+        prm = disk_params(tuple(rho.shape), **disk)
+        n = rho.numel()
+        _need_tensor("rho", rho, n, self.device)
+        _need_tensor("T", T, n, self.device)
+        if stream is None:
+            stream = torch.cuda.current_stream(rho.device)
+        self._check(self.lib.oco_disk_inputs_device(self.ctx, ctypes.byref(prm), ctypes.c_void_p(rho.data_ptr()),
+                                                     ctypes.c_void_p(T.data_ptr()),
+                                                     ctypes.c_void_p(stream.cuda_stream)))
+        return (prm.z1 - prm.z0) / (prm.nz - 1)
+
     def mixed_repairs(self):
         """Items the mixed form re-solved in FP64 since the previous call (waits for the work)."""
         n = ctypes.c_int64(0)
@@ -468,6 +495,36 @@ class Engine:
         arrays are packed densely (dense_batch_offsets) unless offsets gives the per-column
         element offsets {"in_off", "u_off", "kv_off", "flux_off"} of the caller's packing."""
         return Batch(self, nz, nw, dz, waves, wave_off, layout, fully_ionized_T, form, offsets)
+
+
+DISK_DEFAULTS = {"z0": -5e15, "z1": 5e15, "rho0": 1e-9, "H": 1.496e14, "rho_floor": 1e-24, "midTemp": 6.1e4,
+                 "sigma": 2.5e14, "floorTemp": 2000.0, "isoTemp": 1e8, "sigma_dex": 0.0, "seed": 0}
+
+
+def disk_params(shape, **kw):
+    """oco_disk_params for a block of shape (nx, ny, nz); keys as in DISK_DEFAULTS (the AGN grid's
+    disk: the Gaussian temperature applies since isoTemp exceeds midTemp)."""
+    nx, ny, nz = shape
+    d = dict(DISK_DEFAULTS, **kw)
+    unknown = set(kw) - set(DISK_DEFAULTS)
+    if unknown:
+        raise ValueError(f"disk parameters: unknown {sorted(unknown)}")
+    return OcoDiskParams(int(nx), int(ny), int(nz), 0, *(float(d[k]) for k in
+                                                          ("z0", "z1", "rho0", "H", "rho_floor", "midTemp", "sigma",
+                                                           "floorTemp", "isoTemp", "sigma_dex")), int(d["seed"]))
+
+
+def disk_inputs(shape, **kw):
+    """Host arrays rho, T (nx, ny, nz) and dz of the synthetic disk (bit-identical to
+    Engine.disk_inputs_device); no GPU needed."""
+    lib = load_library()
+    prm = disk_params(shape, **kw)
+    rho, T = np.empty(shape), np.empty(shape)
+    dz = ctypes.c_double()
+    rc = lib.oco_disk_inputs(ctypes.byref(prm), _ptr(rho), _ptr(T), ctypes.byref(dz))
+    if rc:
+        raise OcoError(rc, lib.oco_last_error(None).decode())
+    return rho, T, dz.value
 
 
 def dense_batch_offsets(nz, nw):

@@ -134,16 +134,29 @@ def serving_stream(n_jobs, rate, seed=5):
     return jobs
 
 
-def job_arrays_device(job, device, sigma_dex=0.3):
-    """rho, T (nx, ny, nz) float64 torch tensors on `device` for a serving_stream job: the
-    agn_block construction with the job's rho0, the perturbation drawn on the device."""
+def job_arrays_device(job, eng, sigma_dex=0.3):
+    """rho, T (nx, ny, nz) float64 torch tensors on the engine's device and dz for a
+    serving_stream job: the agn_block construction with the job's rho0, generated on the device
+    (Engine.disk_inputs_device: the reference's disk model and a Philox-seeded lognormal
+    perturbation), so no input crosses PCIe."""
     import torch
-    nz = job["nz"]
-    z, dz = grid(nz)
-    base = np.maximum(job["rho0"] * np.exp(-0.5 * z * z / (H * H)), RHO_FLOOR)
-    g = torch.Generator(device=device)
-    g.manual_seed(job["seed"])
-    pert = torch.randn((job["nx"], job["ny"], nz), generator=g, device=device, dtype=torch.float64)
-    rho = torch.pow(10.0, sigma_dex * pert) * torch.from_numpy(base).to(device)
-    T = torch.from_numpy(temperature(z)).to(device).expand(job["nx"], job["ny"], nz).contiguous()
+    shape = (job["nx"], job["ny"], job["nz"])
+    dev = torch.device("cuda", eng.device)
+    rho = torch.empty(shape, dtype=torch.float64, device=dev)
+    T = torch.empty(shape, dtype=torch.float64, device=dev)
+    dz = eng.disk_inputs_device(rho, T, {"rho0": job["rho0"], "sigma_dex": sigma_dex, "seed": job["seed"]})
     return rho, T, dz
+
+
+def precision_block_device(eng, nx, ny, nz, seed=3):
+    """Config 'precision form' generated on the engine's device: rho0 drawn log-uniform in
+    [1e-11, 1e-7] as precision_block draws it, the disk and its 0.3 dex lognormal perturbation
+    (Philox, keyed by seed + 1000) on the device.  Returns rho, T (torch, (nx, ny, nz)), dz, rho0."""
+    import torch
+    rng = np.random.default_rng(seed)
+    rho0 = 10.0 ** rng.uniform(-11.0, -7.0)
+    dev = torch.device("cuda", eng.device)
+    rho = torch.empty((nx, ny, nz), dtype=torch.float64, device=dev)
+    T = torch.empty((nx, ny, nz), dtype=torch.float64, device=dev)
+    dz = eng.disk_inputs_device(rho, T, {"rho0": rho0, "sigma_dex": 0.3, "seed": seed + 1000})
+    return rho, T, dz, rho0
