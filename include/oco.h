@@ -425,6 +425,16 @@ typedef struct oco_deck_info {
 int oco_deck_block_inputs(const char *deck_dir, const char *snapshot, int32_t iprocx, int32_t iprocy,
                           oco_deck_info *info, double *rho, double *T, double *wa, double *z);
 
+/* Same block inputs delivered into DEVICE arrays rho, T (nz, nyloc, nxloc) on the context's
+ * device (info, wa and z as above, host memory).  For an Athena deck the snapshot goes from disk
+ * to HBM: the host streams each z-block file's raw fields through pinned memory and the device
+ * reassembles the block and applies the reader's physics (read_athena.f90:101-277, calc_temperature
+ * disk.f90:64-109), bit-identical to oco_deck_block_inputs; a synthetic-disk deck is built on
+ * the host and copied.  Returns when the arrays are complete (uses `stream`). */
+int oco_deck_block_inputs_device(oco_ctx *ctx, const char *deck_dir, const char *snapshot, int32_t iprocx,
+                                 int32_t iprocy, oco_deck_info *info, double *rho, double *T, double *wa, double *z,
+                                 void *stream);
+
 /* Runs a deck: every processor block solved on CUDA device `device` in form `form`, writing
  * into out_dir (NULL or "": deck_dir/output) what the reference writes into output/:
  * diagnostics.txt (io.f90:31-46, gfortran Ew.d editing), zgrid.txt/.bin and wavegrid.txt/.bin

@@ -26,8 +26,12 @@
 #include <sys/stat.h>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "../../include/oco.h"
 #include "fortran_records.h"
+#include "oco_ctx.h"
+#include "oco_internal.h"
 
 namespace {
 
@@ -604,6 +608,151 @@ static int deck_block_inputs(const char *deck_dir, const char *snapshot, int32_t
   return OCO_OK;
 }
 
+/* The Athena reader with the data into HBM: per z-block file the host reads the header and
+ * coordinates (read_athena.f90:101-148, the same checks as read_athena_block) and the five raw
+ * fields into pinned memory (two buffers, so that reading file k+1 overlaps the copy of file k);
+ * the device reassembles the block (k_athena_zblock) and applies postprocess_athena_values and
+ * calc_temperature (k_athena_post) with the host reader's operations and the host's Gaussian
+ * profile, so rho and T equal read_athena_block's bit for bit. */
+int read_athena_block_device(oco_ctx *c, Deck &d, int iprocx, int iprocy, double *rho, double *T, double *z,
+                             double &dz, cudaStream_t s) {
+  const int nz = d.nz, nxl = d.nxloc, nyl = d.nyloc;
+  std::vector<double> zn((size_t)nz, 0.0);
+  double z0a = 0.0, dza = 0.0, gamma1 = 0.0;
+  struct Staging {
+    void *host[2] = {nullptr, nullptr};
+    size_t hn[2] = {0, 0};
+    DevBuf dev[2], tg;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    cudaStream_t s = nullptr;
+    ~Staging() {
+      if (s) cudaStreamSynchronize(s);
+      for (int b = 0; b < 2; b++) {
+        if (host[b]) cudaFreeHost(host[b]);
+        if (ev[b]) cudaEventDestroy(ev[b]);
+        dev[b].release();
+      }
+      tg.release();
+    }
+  } st;
+  st.s = s;
+  for (int b = 0; b < 2; b++)
+    if (cudaEventCreateWithFlags(&st.ev[b], cudaEventDisableTiming) != cudaSuccess)
+      return derr(OCO_ECUDA, "athena device reader: cudaEventCreate failed");
+  for (int iprocz = 0; iprocz < d.nprocz; iprocz++) {
+    const int iproc = iprocz * d.nprocx * d.nprocy + iprocy * d.nprocx + iprocx;
+    std::string head = d.dir + "/" + d.datadir + "/id" + std::to_string(iproc) + "/" + d.RunName;
+    const std::string fn = iproc == 0 ? head + "." + d.snapshot + ".bin"
+                                      : head + "-id" + std::to_string(iproc) + "." + d.snapshot + ".bin";
+    FILE *fp = fopen(fn.c_str(), "rb");
+    if (!fp) return derr(OCO_EIO, "File %s does not exist (iproc=%d)", fn.c_str(), iproc);
+    std::unique_ptr<FILE, int (*)(FILE *)> guard(fp, fclose);
+    int32_t coordsys, dims[3], dummies[4];
+    double reals[3];
+    if (!(read_i32(fp, &coordsys, 1) && read_i32(fp, dims, 3) && read_i32(fp, dummies, 4) &&
+          read_f64(fp, &gamma1, 1) && read_f64(fp, reals, 3)))
+      return derr(OCO_EIO, "%s: truncated header", fn.c_str());
+    if (dims[0] != nxl || dims[1] != nyl)
+      return derr(OCO_EDIM,
+                  "The Athena x/y dimensionality (%d, %d) does not match the chosen for the RT post-processing "
+                  "(%d, %d). Fix.",
+                  dims[0], dims[1], nxl, nyl);
+    const int nzl = dims[2];
+    std::vector<double> coords((size_t)nxl + nyl + (nzl > 0 ? nzl : 0));
+    if (nzl < 1 || !read_f64(fp, coords.data(), coords.size()))
+      return derr(OCO_EIO, "%s: truncated coordinates", fn.c_str());
+    const double *zloc = coords.data() + nxl + nyl;
+    if (iprocz == 0) {
+      z0a = zloc[0];
+      dza = nzl > 1 ? zloc[1] - zloc[0] : 0.0;
+    }
+    const long iz0 = dza != 0.0 ? std::lround((zloc[0] - z0a) / dza) : 0;
+    if (iz0 < 0 || iz0 + nzl > nz)
+      return derr(OCO_EDIM, "%s: z block %ld..%ld outside nz=%d", fn.c_str(), iz0, iz0 + nzl - 1, nz);
+    for (int k = 0; k < nzl; k++) zn[(size_t)(iz0 + k)] = zloc[k];
+    const size_t nc = (size_t)nxl * nyl * nzl, bytes = 5 * nc * sizeof(double);
+    const int b = iprocz & 1;
+    if (cudaEventSynchronize(st.ev[b]) != cudaSuccess) return derr(OCO_ECUDA, "athena device reader: event wait failed");
+    if (st.hn[b] < bytes) {
+      if (st.host[b]) cudaFreeHost(st.host[b]);
+      st.host[b] = nullptr;
+      st.hn[b] = 0;
+      if (cudaMallocHost(&st.host[b], bytes) != cudaSuccess) return derr(OCO_ENOMEM, "athena device reader: pinned staging");
+      st.hn[b] = bytes;
+    }
+    if (!read_f64(fp, (double *)st.host[b], 5 * nc)) return derr(OCO_EIO, "%s: truncated data", fn.c_str());
+    if (st.dev[b].n < bytes) {
+      cudaStreamSynchronize(s); /* the previous user of this buffer is done before it is replaced */
+      if (st.dev[b].ensure(bytes) != cudaSuccess) return derr(OCO_ENOMEM, "athena device reader: device staging");
+    }
+    if (cudaMemcpyAsync(st.dev[b].p, st.host[b], bytes, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaEventRecord(st.ev[b], s) != cudaSuccess)
+      return derr(OCO_ECUDA, "athena device reader: copy failed");
+    oco::AthenaZBlock zb{st.dev[b].as<double>(), nxl, nyl, nzl, nz, (int)iz0, d.lavoid, rho, T};
+    if (oco::launch_athena_zblock(zb, s) != cudaSuccess) return derr(OCO_ECUDA, "athena device reader: launch failed");
+    c->launches += 1;
+  }
+  if (d.a_rho_floor != d.a_rho_floor)
+    return derr(OCO_ENAN, "Must set `rho_floor` (cgs) value in namelist: `input.in/athena_input`.");
+  for (int i = 0; i < nz; i++) zn[(size_t)i] = zn[(size_t)i] * d.unit_length;
+  dz = (zn[(size_t)nz - 1] - zn[0]) / (double)(nz - 1);
+  for (int i = 0; i < nz; i++) z[kNg + i] = zn[(size_t)i];
+  for (int i = 1; i <= kNg; i++) {
+    z[kNg - i] = z[kNg] - (double)i * dz;
+    z[nz + kNg - 1 + i] = z[nz + kNg - 1] + (double)i * dz;
+  }
+  if (!d.have_tgauss) { /* calc_temperature's first call fixes the profile, as on the host */
+    for (int i = 0; i < nz; i++) {
+      const double zz = z[kNg + i];
+      d.Tgauss[(size_t)i] = d.midTemp * std::exp(-((0.5 * (zz * zz)) / (d.sigma * d.sigma)));
+    }
+    d.have_tgauss = true;
+  }
+  if (st.tg.ensure((size_t)nz * sizeof(double)) != cudaSuccess ||
+      cudaMemcpyAsync(st.tg.p, d.Tgauss.data(), (size_t)nz * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return derr(OCO_ECUDA, "athena device reader: temperature profile upload failed");
+  if (oco::launch_athena_post(rho, T, (int64_t)nxl * nyl * nz, nz, d.unit_density, d.a_rho_floor, gamma1, d.unit_temperature,
+                         st.tg.as<double>(), d.switchTemp, d.floorTemp, s) != cudaSuccess)
+    return derr(OCO_ECUDA, "athena device reader: launch failed");
+  c->launches += 1;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return derr(OCO_ECUDA, "athena device reader: device error");
+  return OCO_OK;
+}
+
+static int deck_block_inputs_device(oco_ctx *c, const char *deck_dir, const char *snapshot, int32_t iprocx,
+                                    int32_t iprocy, oco_deck_info *info, double *rho, double *T, double *wa, double *z,
+                                    cudaStream_t s) {
+  if (!c) return derr(OCO_EINVAL, "oco_deck_block_inputs_device: NULL context");
+  if (!info || !rho || !T) return derr(OCO_EINVAL, "oco_deck_block_inputs_device: info, rho and T are required");
+  Deck d;
+  int rc = load_deck(deck_dir, snapshot, d);
+  if (rc) return rc;
+  if (iprocx < 0 || iprocx >= d.nprocx || iprocy < 0 || iprocy >= d.nprocy)
+    return derr(OCO_EINVAL, "block (%d, %d) outside %d x %d processors", iprocx, iprocy, d.nprocx, d.nprocy);
+  if (cudaSetDevice(c->device) != cudaSuccess) return derr(OCO_ECUDA, "oco_deck_block_inputs_device: cudaSetDevice");
+  double dz = 0.0;
+  std::vector<double> zz((size_t)d.nz + 2 * kNg, 0.0);
+  const size_t n = (size_t)d.nxloc * d.nyloc * d.nz;
+  if (d.lread_athena) {
+    if (iprocx || iprocy) { /* the Gaussian temperature profile is fixed by the root block's grid (first call) */
+      std::vector<double> r0(n), t0(n);
+      if ((rc = block_inputs(d, 0, 0, r0.data(), t0.data(), zz.data(), dz))) return rc;
+    }
+    if ((rc = read_athena_block_device(c, d, iprocx, iprocy, rho, T, zz.data(), dz, s))) return rc;
+  } else { /* the synthetic disk is built on the host (the C library's exp, as the reference) */
+    std::vector<double> r(n), t(n);
+    disk_block(d, r.data(), t.data(), zz.data(), dz);
+    if (cudaMemcpyAsync(rho, r.data(), n * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(T, t.data(), n * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+      return derr(OCO_ECUDA, "oco_deck_block_inputs_device: copy failed");
+  }
+  if (z) memcpy(z, zz.data(), zz.size() * sizeof(double));
+  if (wa) memcpy(wa, d.wa.data(), d.wa.size() * sizeof(double));
+  fill_info(d, dz, info);
+  return OCO_OK;
+}
+
 static int run_deck(const char *deck_dir, const char *snapshot, const char *out_dir, int32_t form, int32_t device,
                     int32_t write_binary) {
   Deck d;
@@ -713,6 +862,19 @@ extern "C" int oco_deck_block_inputs(const char *deck_dir, const char *snapshot,
     return derr(OCO_ENOMEM, "oco_deck_block_inputs: out of host memory");
   } catch (const std::exception &e) {
     return derr(OCO_EINVAL, "oco_deck_block_inputs: %s", e.what());
+  }
+}
+
+extern "C" int oco_deck_block_inputs_device(oco_ctx *ctx, const char *deck_dir, const char *snapshot, int32_t iprocx,
+                                            int32_t iprocy, oco_deck_info *info, double *rho, double *T, double *wa,
+                                            double *z, void *stream) {
+  try {
+    return deck_block_inputs_device(ctx, deck_dir, snapshot, iprocx, iprocy, info, rho, T, wa, z,
+                                    (cudaStream_t)stream);
+  } catch (const std::bad_alloc &) {
+    return derr(OCO_ENOMEM, "oco_deck_block_inputs_device: out of host memory");
+  } catch (const std::exception &e) {
+    return derr(OCO_EINVAL, "oco_deck_block_inputs_device: %s", e.what());
   }
 }
 

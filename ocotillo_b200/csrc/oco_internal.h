@@ -227,6 +227,18 @@ cudaError_t launch_integrated_flux(const double *V, const double *w, int64_t nco
 cudaError_t launch_lambda_to_reference(const double *src, int64_t src_zs, double *dst, int64_t ld_col, int64_t c_off,
                                        int64_t nb, int rows, int nw, cudaStream_t s);
 
+/* One z-block file of an Athena snapshot in device memory (kernels_inputs.cu): raw = the five
+ * fields [5][nzl][nyl][nxl] as stored; the block arrays rho, T are (nxl, nyl, nz), z fastest. */
+struct AthenaZBlock {
+  const double *raw;
+  int nxl, nyl, nzl, nz, iz0, lavoid;
+  double *rho, *T;
+};
+cudaError_t launch_athena_zblock(const AthenaZBlock &b, cudaStream_t s);
+cudaError_t launch_athena_post(double *rho, double *T, int64_t n, int nz, double unit_density, double rho_floor,
+                               double gamma1, double unit_T, const double *Tgauss, double switchTemp, double floorTemp,
+                               cudaStream_t s);
+
 /* Fills tab[NL*nw] (layout [field][iw]) with the wavelength table of waves[nw] (Angstrom):
  * pre_calc_opacity_quantities' arithmetic plus the hot loop's lambda-only factors
  * (defined in oco_api.cu). */

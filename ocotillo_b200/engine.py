@@ -126,6 +126,8 @@ def load_library(path=None):
         "oco_synchronize": (I, [V]),
         "oco_set_mixed_repair": (I, [V, D]),
         "oco_disk_inputs": (I, [ctypes.POINTER(OcoDiskParams), _DP, _DP, _DP]),
+        "oco_deck_block_inputs_device": (I, [V, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32,
+                                             ctypes.POINTER(OcoDeckInfo), V, V, _DP, _DP, V]),
         "oco_disk_inputs_device": (I, [V, ctypes.POINTER(OcoDiskParams), V, V, V]),
         "oco_mixed_repairs": (I, [V, ctypes.POINTER(ctypes.c_int64)]),
         "oco_kernel_launches": (ctypes.c_int64, [V]),
@@ -399,6 +401,33 @@ class Engine:
                                                      ctypes.c_void_p(T.data_ptr()),
                                                      ctypes.c_void_p(stream.cuda_stream)))
         return (prm.z1 - prm.z0) / (prm.nz - 1)
+
+    def deck_block_inputs_device(self, deck_dir, snapshot="0000", iprocx=0, iprocy=0, stream=None):
+        """Inputs of processor block (iprocx, iprocy) of a reference deck delivered into device
+        memory (an Athena snapshot goes from disk to HBM): dict with info fields, rho and T as
+        torch CUDA tensors (nxloc, nyloc, nz), wa and z (numpy)."""
+        import torch
+        info = OcoDeckInfo()
+        rc = self.lib.oco_deck_block_inputs(deck_dir.encode(), snapshot.encode(), 0, 0, ctypes.byref(info), None, None,
+                                            None, None)
+        if rc:
+            raise OcoError(rc, self.lib.oco_deck_last_error().decode())
+        dev = torch.device("cuda", self.device)
+        rho = torch.empty((info.nxloc, info.nyloc, info.nz), dtype=torch.float64, device=dev)
+        T = torch.empty_like(rho)
+        wa = np.empty(info.nw)
+        z = np.empty(info.nz + 6)
+        if stream is None:
+            stream = torch.cuda.current_stream(dev)
+        rc = self.lib.oco_deck_block_inputs_device(self.ctx, deck_dir.encode(), snapshot.encode(), int(iprocx),
+                                                   int(iprocy), ctypes.byref(info), ctypes.c_void_p(rho.data_ptr()),
+                                                   ctypes.c_void_p(T.data_ptr()), _ptr(wa), _ptr(z),
+                                                   ctypes.c_void_p(stream.cuda_stream))
+        if rc:
+            raise OcoError(rc, self.lib.oco_deck_last_error().decode())
+        out = {k: getattr(info, k) for k, _ in OcoDeckInfo._fields_}
+        out.update(rho=rho, T=T, wa=wa, z=z)
+        return out
 
     def mixed_repairs(self):
         """Items the mixed form re-solved in FP64 since the previous call (waits for the work)."""
@@ -720,6 +749,15 @@ class Server:
         self._check(self.lib.oco_server_submit(self.h, ctypes.byref(job), ctypes.byref(jid)))
         self._jobs[jid.value] = (rho, T, (nx, ny, nz, w.size), bool(want_fields))
         return jid.value
+
+    def submit_deck(self, eng, deck_dir, snapshot="0000", iprocx=0, iprocy=0, form="mixed", want_fields=False):
+        """Queues processor block (iprocx, iprocy) of a reference deck as a job: its snapshot is
+        read into HBM (Engine.deck_block_inputs_device on `eng`, the server's device) and the job
+        takes the device arrays.  Returns (job id, the block's info dict)."""
+        d = eng.deck_block_inputs_device(deck_dir, snapshot, iprocx, iprocy)
+        jid = self.submit(d["rho"], d["T"], d["wa"], d["dz"], form=form, fully_ionized_T=d["fully_ionized_T"],
+                          want_fields=want_fields)
+        return jid, d
 
     def status(self, jid):
         st = OcoJobStatus()
