@@ -131,10 +131,12 @@ int oco_synchronize(oco_ctx *ctx);
  * well conditioned.  The flux is a weighted sum of the boundary differences of U, computed as
  * D_k = u_k - q_k U_{k+1} from non-negative terms, and its condition number is
  * sum |w_k| (u_k + q_k U_{k+1}) / |sum w_k D_k|.  The solve kernels compute it for every item
- * (top and bottom) and re-solve an item whose condition number exceeds cond_max in the stable
- * FP64 form, in place, before the item's results are final.  Default 100 (the kernel's error
- * grows as ~1e-5 + 2e-7 x condition number); cond_max >= 3e38 turns the re-solve off; values
- * below 1 are refused.  Block solves use the value current at the call; a batch uses the
+ * (top and bottom) and list the items whose condition number exceeds cond_max (and every item
+ * of a column holding a cell with a negative neutral fraction, where the reference's Saha root
+ * rounds above 1); a second kernel on the same stream re-solves the listed items in the stable
+ * FP64 form (bit-identical to OCO_FORM_STABLE) over the mixed results.  Default 100 (the FP32
+ * error grows as ~1e-5 + 2e-7 x condition number); cond_max >= 3e38 turns the re-solve off;
+ * values below 1 are refused.  Block solves use the value current at the call; a batch uses the
  * value current when its graph is captured (oco_batch_bind, _tune, _set_tiling).  No reference
  * counterpart: the reference computes in FP64 only. */
 int oco_set_mixed_repair(oco_ctx *ctx, double cond_max);

@@ -27,6 +27,7 @@ COMMON = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-con
 UNITS = [
     ("kernels_fp64.cu", ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
     ("kernels_mixed.cu", []),
+    ("kernels_repair.cu", ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
     ("kernels_mixed_pillars.cu", ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
     ("oco_api.cu", []),
     ("oco_noalloc.cu", []),

@@ -215,91 +215,17 @@ __device__ __forceinline__ Opac opacity_grey(const R P, double sg) {
 /* ---- the solve ----------------------------------------------------------------------- */
 /* Solves one (column, wavelength) item.  `active` false: the lane only keeps the warp's
  * shared pipeline in step (staged path, wavelength index beyond nw) and stores nothing. */
-template <int FORM, bool GREY, class IT, class PA>
-__device__ __forceinline__ void solve_item(const IT &it, bool active, PA &pa, double *__restrict__ gam,
-                                           double *__restrict__ uu, double *__restrict__ o1s,
-                                           double *__restrict__ qs) {
+/* The reverse sweep of one item (back-substitution, tridag :43-45; ghost zones :49-62; flux
+ * :96-109) from the forward sweep's last u and its scratch (gam, uu, o1s and, stable form, qs at
+ * stride it.ss()), storing U, V and the emergent fluxes through the item accessor. */
+template <int FORM, class IT>
+__device__ __forceinline__ void solve_reverse(const IT &it, double u, const double *__restrict__ gam,
+                                              const double *__restrict__ uu, const double *__restrict__ o1s,
+                                              const double *__restrict__ qs) {
   const int nz = it.nz();
   const int64_t ss = it.ss();
-  Lam L;
-  if (!GREY) load_lam(L, it.lam(), it.iw(), it.nw());
   double *Ub = it.U();
-  double *Kb = active ? it.K() : nullptr;
-  double *Vb = active ? it.V() : nullptr;
-  const double dz = it.dz(), dz2 = it.dz2();
-  bool bad = false;
-
-  /* forward sweep: row 0 (fill_boundary_coeffs :187-191) */
-  Opac cur = GREY ? opacity_grey(pa.at(0), it.sigma_grey()) : opacity_at<FORM == 1>(pa.at(0), L);
-  Opac nxt = GREY ? opacity_grey(pa.at(1), it.sigma_grey()) : opacity_at<FORM == 1>(pa.at(1), L);
-  double o1 = 1.0 / cur.op, o2 = cur.op * cur.op;
-  double zeta = ((cur.op * dz2) * (FORM == 1 ? cur.oma : (1.0 - cur.alb))) * 0.25;
-  double bet, h = 0.0;
-  if (FORM == 0) {
-    bet = -(((o1 + dz) + zeta) * o2);
-  } else {
-    h = (dz + zeta) * o2;
-    bet = -(cur.op + h);
-  }
-  if (bet == 0.0) bad = true;
-  double u = (-((cur.S * zeta) * o2)) / bet;
-  uu[0] = u;
-  o1s[0] = o1;
-  if (Kb) __stcs(&Kb[0], cur.op);
-  double c_prev = cur.op;
-  double kh_prev = 0.5 * (nxt.op + cur.op); /* kappa_p(1) = kappa_m(2), :147-154 */
-  cur = nxt;
-  for (int j = 1; j < nz; j++) {
-    const double op = cur.op;
-    o1 = 1.0 / op;
-    o2 = op * op;
-    double aa, bb, cc, dd, ee;
-    if (j < nz - 1) { /* fill_center_coeffs :159-165 */
-      nxt = GREY ? opacity_grey(pa.at(j + 1), it.sigma_grey()) : opacity_at<FORM == 1>(pa.at(j + 1), L);
-      aa = o2 / kh_prev;
-      double kh = 0.5 * (nxt.op + op);
-      cc = o2 / kh;
-      double z3 = (dz2 * (op * (op * op))) * (FORM == 1 ? cur.oma : (1.0 - cur.alb));
-      bb = -((aa + cc) + z3);
-      dd = -(cur.S * z3);
-      ee = z3;
-      kh_prev = kh;
-    } else { /* fill_boundary_coeffs :193-197 */
-      aa = op;
-      double zt = ((op * dz2) * (FORM == 1 ? cur.oma : (1.0 - cur.alb))) * 0.25;
-      bb = -(((o1 + dz) + zt) * o2);
-      cc = 0.0;
-      dd = -((cur.S * zt) * o2);
-      ee = (dz + zt) * o2;
-    }
-    double g;
-    if (FORM == 0) { /* tridag :34-35 */
-      g = c_prev / bet;
-      bet = bb - aa * g;
-    } else { /* difference form: bet = -(c + h), h = e + a*h_prev/(c_prev + h_prev) */
-      double den = c_prev + h;
-      g = -(c_prev / den);
-      qs[(j - 1) * ss] = h / den; /* q_{j-1} = h_{j-1}/(c_{j-1} + h_{j-1}) */
-      h = ee + (aa * h) / den;
-      bet = -(cc + h);
-      (void)bb;
-    }
-    if (bet == 0.0) bad = true;
-    u = (dd - aa * u) / bet; /* tridag :40 */
-    gam[j * ss] = g;
-    uu[j * ss] = u;
-    o1s[j * ss] = o1;
-    if (Kb) __stcs(&Kb[j * it.kz()], op);
-    c_prev = cc;
-    cur = nxt;
-  }
-  if (!active) return;
-  if (bad) {
-    atomicAdd(&it.status()[0], 1ull);
-    atomicMin(&it.status()[1], it.id());
-  }
-
-  /* reverse sweep: back-substitution (tridag :43-45), ghosts (:49-62), flux (:96-109) */
+  double *Vb = it.V();
   const double dz1 = it.dz1();
   const int64_t uz = it.uz();
   double vtop = 0.0, vbot = 0.0;
@@ -446,6 +372,91 @@ __device__ __forceinline__ void solve_item(const IT &it, bool active, PA &pa, do
   }
   if (double *p = it.vtop()) __stcs(p, vtop);
   if (double *p = it.vbot()) __stcs(p, vbot);
+}
+
+template <int FORM, bool GREY, class IT, class PA>
+__device__ __forceinline__ void solve_item(const IT &it, bool active, PA &pa, double *__restrict__ gam,
+                                           double *__restrict__ uu, double *__restrict__ o1s,
+                                           double *__restrict__ qs) {
+  const int nz = it.nz();
+  const int64_t ss = it.ss();
+  Lam L;
+  if (!GREY) load_lam(L, it.lam(), it.iw(), it.nw());
+  double *Kb = active ? it.K() : nullptr;
+  const double dz = it.dz(), dz2 = it.dz2();
+  bool bad = false;
+
+  /* forward sweep: row 0 (fill_boundary_coeffs :187-191) */
+  Opac cur = GREY ? opacity_grey(pa.at(0), it.sigma_grey()) : opacity_at<FORM == 1>(pa.at(0), L);
+  Opac nxt = GREY ? opacity_grey(pa.at(1), it.sigma_grey()) : opacity_at<FORM == 1>(pa.at(1), L);
+  double o1 = 1.0 / cur.op, o2 = cur.op * cur.op;
+  double zeta = ((cur.op * dz2) * (FORM == 1 ? cur.oma : (1.0 - cur.alb))) * 0.25;
+  double bet, h = 0.0;
+  if (FORM == 0) {
+    bet = -(((o1 + dz) + zeta) * o2);
+  } else {
+    h = (dz + zeta) * o2;
+    bet = -(cur.op + h);
+  }
+  if (bet == 0.0) bad = true;
+  double u = (-((cur.S * zeta) * o2)) / bet;
+  uu[0] = u;
+  o1s[0] = o1;
+  if (Kb) __stcs(&Kb[0], cur.op);
+  double c_prev = cur.op;
+  double kh_prev = 0.5 * (nxt.op + cur.op); /* kappa_p(1) = kappa_m(2), :147-154 */
+  cur = nxt;
+  for (int j = 1; j < nz; j++) {
+    const double op = cur.op;
+    o1 = 1.0 / op;
+    o2 = op * op;
+    double aa, bb, cc, dd, ee;
+    if (j < nz - 1) { /* fill_center_coeffs :159-165 */
+      nxt = GREY ? opacity_grey(pa.at(j + 1), it.sigma_grey()) : opacity_at<FORM == 1>(pa.at(j + 1), L);
+      aa = o2 / kh_prev;
+      double kh = 0.5 * (nxt.op + op);
+      cc = o2 / kh;
+      double z3 = (dz2 * (op * (op * op))) * (FORM == 1 ? cur.oma : (1.0 - cur.alb));
+      bb = -((aa + cc) + z3);
+      dd = -(cur.S * z3);
+      ee = z3;
+      kh_prev = kh;
+    } else { /* fill_boundary_coeffs :193-197 */
+      aa = op;
+      double zt = ((op * dz2) * (FORM == 1 ? cur.oma : (1.0 - cur.alb))) * 0.25;
+      bb = -(((o1 + dz) + zt) * o2);
+      cc = 0.0;
+      dd = -((cur.S * zt) * o2);
+      ee = (dz + zt) * o2;
+    }
+    double g;
+    if (FORM == 0) { /* tridag :34-35 */
+      g = c_prev / bet;
+      bet = bb - aa * g;
+    } else { /* difference form: bet = -(c + h), h = e + a*h_prev/(c_prev + h_prev) */
+      double den = c_prev + h;
+      g = -(c_prev / den);
+      qs[(j - 1) * ss] = h / den; /* q_{j-1} = h_{j-1}/(c_{j-1} + h_{j-1}) */
+      h = ee + (aa * h) / den;
+      bet = -(cc + h);
+      (void)bb;
+    }
+    if (bet == 0.0) bad = true;
+    u = (dd - aa * u) / bet; /* tridag :40 */
+    gam[j * ss] = g;
+    uu[j * ss] = u;
+    o1s[j * ss] = o1;
+    if (Kb) __stcs(&Kb[j * it.kz()], op);
+    c_prev = cc;
+    cur = nxt;
+  }
+  if (!active) return;
+  if (bad) {
+    atomicAdd(&it.status()[0], 1ull);
+    atomicMin(&it.status()[1], it.id());
+  }
+
+  solve_reverse<FORM>(it, u, gam, uu, o1s, qs);
 }
 
 }  // namespace oco

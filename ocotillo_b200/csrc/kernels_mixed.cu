@@ -15,7 +15,6 @@
  */
 #include <cuda_runtime.h>
 
-#include "fp64_core.h"
 #include "mixed_core.h"
 #include "oco_internal.h"
 
@@ -25,8 +24,6 @@ using namespace oco::mx;
 constexpr int MZC = 20;            /* z records per staged chunk (20 x 256 B) */
 constexpr int MWARPS = 4;          /* warps per 128-thread block */
 constexpr long long kMSpinLimit = 1ll << 26;
-static_assert(2 * MZC * MZN * sizeof(float) >= 32 * NF * sizeof(double),
-              "a warp's record buffers hold the 32 FP64 records of the re-solve");
 #ifndef OCO_MIXED_PREFETCH
 #define OCO_MIXED_PREFETCH 4 /* reverse-sweep steps whose scratch loads are issued together */
 #endif
@@ -170,7 +167,7 @@ __device__ __forceinline__ MItem block_item(const MixedArgs &a, int64_t cl, int 
  * errors of u, q and U is
  *   (37 C_a + 8 C_b + C_c) / |37 D_a - 8 D_b + D_c|,   C_k = u_k + q_k U_{k+1};
  * FP32 leaves relative errors of a few 1e-6 in u, q and U, so above `cond` the item is
- * flagged for the FP64 re-solve.  Columns with nz < 4 are never flagged (their flux is the
+ * flagged for the FP64 re-solve (kernels_repair.cu).  Columns with nz < 4 are never flagged (their flux is the
  * reference's stencil on U). */
 template <class PA>
 __device__ __forceinline__ bool msolve_item(const MItem &it, bool active, PA &pa, float4 *__restrict__ s4,
@@ -376,151 +373,20 @@ __device__ __forceinline__ bool msolve_item(const MItem &it, bool active, PA &pa
   return flag;
 }
 
-/* ---- FP64 re-solve of flagged items ------------------------------------------------------
- * A flagged item is solved again in the stable FP64 form (fp64_core.h: the block solve's
- * solve_item with FP64 pillar records computed from rho and T), overwriting its mixed
- * outputs.  FMA contraction is on in this translation unit, so a re-solved item agrees with
- * the FP64 stable form to rounding, not bit for bit. */
-
-/* Records of one column computed on the fly by the whole warp into shared memory: entering a
- * block of 32 z, lane l computes the record of z = block start + l.  The solve reads records
- * in increasing z, so one block of 32 records suffices (buf: 32 * NF doubles). */
-struct ComputedPillars {
-  double *buf;
-  const double *rho, *T;
-  double fit;
-  int nz, cur;
-  __device__ __forceinline__ SharedRec at(int z) {
-    const int c = z >> 5;
-    if (c != cur) {
-      __syncwarp();
-      const int zz = (c << 5) + (int)(threadIdx.x & 31);
-      if (zz < nz) pillar_record(rho[zz], T[zz], fit, 0, buf + (threadIdx.x & 31) * NF);
-      __syncwarp();
-      cur = c;
-    }
-    return SharedRec{buf + (z & 31) * NF};
-  }
-};
-
-/* Records computed per lane (lanes of one warp may belong to different columns). */
-struct LanePillars {
-  double rec[NF];
-  const double *rho, *T;
-  double fit;
-  __device__ __forceinline__ SharedRec at(int z) {
-    pillar_record(rho[z], T[z], fit, 0, rec);
-    return SharedRec{rec};
-  }
-};
-
-/* The block kernels' item in the FP64 item interface of solve_item (cf. BlockItem). */
-struct MRepairItem {
-  const MixedArgs &a;
-  int64_t cl;
-  int w;
-  __device__ __forceinline__ int64_t idx() const {
-    return (a.layout == 0) ? (int64_t)w * a.ld_col + a.c_off + cl : (a.c_off + cl) * a.nw + w;
-  }
-  __device__ __forceinline__ int64_t pidx() const { return (int64_t)w * a.ld_col + a.c_off + cl; }
-  __device__ __forceinline__ const double *lam() const { return a.lam64; }
-  __device__ __forceinline__ int nz() const { return a.nz; }
-  __device__ __forceinline__ int nw() const { return a.nw; }
-  __device__ __forceinline__ int iw() const { return w; }
-  __device__ __forceinline__ double dz() const { return a.dz; }
-  __device__ __forceinline__ double dz2() const { return a.dz * a.dz; }
-  __device__ __forceinline__ double dz1() const { return 1.0 / a.dz; }
-  __device__ __forceinline__ double sigma_grey() const { return 0.0; }
-  __device__ __forceinline__ double *U() const { return a.U ? a.U + idx() * a.U_is : nullptr; }
-  __device__ __forceinline__ double *K() const { return a.K ? a.K + idx() * a.K_is : nullptr; }
-  __device__ __forceinline__ double *V() const { return a.V ? a.V + idx() * a.V_is : nullptr; }
-  __device__ __forceinline__ int64_t uz() const { return a.U_zs; }
-  __device__ __forceinline__ int64_t kz() const { return a.K_zs; }
-  __device__ __forceinline__ int64_t vz() const { return a.V_zs; }
-  __device__ __forceinline__ double *vtop() const { return a.Vtop ? a.Vtop + pidx() : nullptr; }
-  __device__ __forceinline__ double *vbot() const { return a.Vbot ? a.Vbot + pidx() : nullptr; }
-  __device__ __forceinline__ int64_t ss() const { return 32; }
-  __device__ __forceinline__ unsigned long long *status() const { return a.status; }
-  __device__ __forceinline__ unsigned long long id() const { return (unsigned long long)((a.c_off + cl) * a.nw + w); }
-};
-
-/* The batch kernels' item (cf. BatchItem in kernels_fp64.cu). */
-struct MBatchRepairItem {
-  const MixedBatchArgs &b;
-  const MBatchCol &c;
-  int64_t col;
-  int w;
-  __device__ __forceinline__ int nz() const { return c.nz; }
-  __device__ __forceinline__ int nw() const { return c.nw; }
-  __device__ __forceinline__ int iw() const { return w; }
-  __device__ __forceinline__ const double *lam() const { return b.lam64 + c.lam_off / MIXED_LN * NL; }
-  __device__ __forceinline__ double dz() const { return c.dz; }
-  __device__ __forceinline__ double dz2() const { return c.dz2; }
-  __device__ __forceinline__ double dz1() const { return c.dz1; }
-  __device__ __forceinline__ double sigma_grey() const { return 0.0; }
-  __device__ __forceinline__ int64_t zoff(int64_t base, int rows) const {
-    return b.layout == 0 ? base + (int64_t)w * rows : base + w;
-  }
-  __device__ __forceinline__ double *U() const { return b.U ? b.U + zoff(c.u_off, c.nz + 6) : nullptr; }
-  __device__ __forceinline__ double *K() const { return b.K ? b.K + zoff(c.kv_off, c.nz) : nullptr; }
-  __device__ __forceinline__ double *V() const { return b.V ? b.V + zoff(c.kv_off, c.nz) : nullptr; }
-  __device__ __forceinline__ int64_t uz() const { return b.layout == 0 ? 1 : c.nw; }
-  __device__ __forceinline__ int64_t kz() const { return uz(); }
-  __device__ __forceinline__ int64_t vz() const { return uz(); }
-  __device__ __forceinline__ double *vtop() const { return b.Vtop ? b.Vtop + c.flux_off + w : nullptr; }
-  __device__ __forceinline__ double *vbot() const { return b.Vbot ? b.Vbot + c.flux_off + w : nullptr; }
-  __device__ __forceinline__ int64_t ss() const { return 32; }
-  __device__ __forceinline__ unsigned long long *status() const { return b.status; }
-  __device__ __forceinline__ unsigned long long id() const { return ((unsigned long long)col << 32) | (unsigned)w; }
-};
-
-/* FP64 scratch of the warp in slot `slot` for lane `lane`: gamma, u, 1/kappa, q ([z][32] each). */
-struct Scratch64 {
-  double *g, *u, *o, *q;
-  __device__ __forceinline__ Scratch64(double *s64, int64_t slot, int nz, int lane) {
-    g = s64 + slot * 4 * 32 * (int64_t)nz + lane;
-    u = g + 32 * (int64_t)nz;
-    o = u + 32 * (int64_t)nz;
-    q = o + 32 * (int64_t)nz;
-  }
-};
-
-/* The re-solves are separate (non-inlined) functions called on the rare flagged path, so that
- * their FP64 register demand does not enter the register allocation of the FP32 solve.  The
- * kernels' parameters are __grid_constant__, so these take them by reference without a copy.
- * Calls with flagged lanes are warp-uniform; `flag` selects the lanes that store. */
-__device__ __noinline__ void repair_block_staged(const MixedArgs &a, double *buf, int64_t slot, int64_t cl, int iw,
-                                                 bool flag) {
-  const Scratch64 r(a.s64, slot, a.nz, threadIdx.x & 31);
-  ComputedPillars cp{buf, a.rho + cl * a.nz, a.T + cl * a.nz, a.fully_ionized_T, a.nz, -1};
-  solve_item<1, false>(MRepairItem{a, cl, iw}, flag, cp, r.g, r.u, r.o, r.q);
-}
-__device__ __noinline__ void repair_block_lanes(const MixedArgs &a, int64_t slot, int64_t cl, int iw, bool flag) {
-  const Scratch64 r(a.s64, slot, a.nz, threadIdx.x & 31);
-  LanePillars lp;
-  lp.rho = a.rho + cl * a.nz;
-  lp.T = a.T + cl * a.nz;
-  lp.fit = a.fully_ionized_T;
-  solve_item<1, false>(MRepairItem{a, cl, iw}, flag, lp, r.g, r.u, r.o, r.q);
-}
-__device__ __noinline__ void repair_batch_staged(const MixedBatchArgs &b, double *buf, int64_t slot, int32_t col, int iw,
-                                                 bool flag) {
-  const MBatchCol &c = b.cols[col];
-  const Scratch64 r(b.s64, slot, b.max_nz, threadIdx.x & 31);
-  ComputedPillars cp{buf, b.rho + c.in_off, b.T + c.in_off, b.fully_ionized_T, c.nz, -1};
-  solve_item<1, false>(MBatchRepairItem{b, c, (int64_t)col, iw}, flag, cp, r.g, r.u, r.o, r.q);
-}
-__device__ __noinline__ void repair_batch_lanes(const MixedBatchArgs &b, int64_t slot, int32_t col, int iw, bool flag) {
-  const MBatchCol &c = b.cols[col];
-  const Scratch64 r(b.s64, slot, b.max_nz, threadIdx.x & 31);
-  LanePillars lp;
-  lp.rho = b.rho + c.in_off;
-  lp.T = b.T + c.in_off;
-  lp.fit = b.fully_ionized_T;
-  solve_item<1, false>(MBatchRepairItem{b, c, (int64_t)col, iw}, flag, lp, r.g, r.u, r.o, r.q);
+/* Appends the warp's flagged items (lanes with flag set) to the re-solve list: one atomic per
+ * warp, then each flagged lane writes its id at its rank among the flagged lanes. */
+__device__ __forceinline__ void push_flagged(bool flag, unsigned long long id, unsigned long long *list,
+                                             unsigned long long *count) {
+  const unsigned m = __ballot_sync(0xffffffffu, flag);
+  if (!m) return;
+  const int lane = threadIdx.x & 31;
+  unsigned long long base = 0;
+  if (lane == __ffs(m) - 1) base = atomicAdd(count, (unsigned long long)__popc(m));
+  base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+  if (flag) list[base + __popc(m & ((1u << lane) - 1u))] = id;
 }
 
-__global__ void __launch_bounds__(128, 5) k_solve_mixed_staged(const __grid_constant__ MixedArgs a) {
+__global__ void __launch_bounds__(128, 5) k_solve_mixed_staged(const MixedArgs a) {
   __shared__ __align__(128) float s_rec[MWARPS][2 * MZC * MZN];
   __shared__ __align__(8) unsigned long long s_bar[MWARPS][2];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -560,15 +426,11 @@ __global__ void __launch_bounds__(128, 5) k_solve_mixed_staged(const __grid_cons
       pa.wait(1);
       return;
     }
-    const unsigned m = __ballot_sync(0xffffffffu, flag);
-    if (m) { /* every record copy of this task has landed: the buffers hold the FP64 records */
-      repair_block_staged(a, reinterpret_cast<double *>(s_rec[wib]), slot, cl, iw, flag);
-      if (lane == 0) atomicAdd(a.repairs, (unsigned long long)__popc(m));
-    }
+    push_flagged(flag, (unsigned long long)(cl * a.nw + iw), a.rlist, a.rcount);
   }
 }
 
-__global__ void __launch_bounds__(128, 5) k_solve_mixed(const __grid_constant__ MixedArgs a) {
+__global__ void __launch_bounds__(128, 5) k_solve_mixed(const MixedArgs a) {
   const int lane = threadIdx.x & 31;
   const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nitems = a.ncol * a.nw;
@@ -587,13 +449,7 @@ __global__ void __launch_bounds__(128, 5) k_solve_mixed(const __grid_constant__ 
       MDirect pa{a.rec + cl * (int64_t)a.nz * MZN};
       flag = msolve_item(block_item(a, cl, iw), true, pa, s4, 32, a.repair_cond) || __ldg(a.colflag + cl) != 0u;
     }
-    const unsigned m = __ballot_sync(0xffffffffu, flag);
-    if (m) { /* lanes may hold different columns: each computes its own records */
-      const int64_t it = item < nitems ? item : nitems - 1;
-      const int64_t cl = it / a.nw;
-      repair_block_lanes(a, slot, cl, (int)(it - cl * a.nw), flag);
-      if (lane == 0) atomicAdd(a.repairs, (unsigned long long)__popc(m));
-    }
+    push_flagged(flag, (unsigned long long)item, a.rlist, a.rcount);
   }
 }
 
@@ -647,7 +503,7 @@ __device__ __forceinline__ MItem batch_item(const MixedBatchArgs &b, const MBatc
 
 /* Warp-column tiling: tasks (column, 32-wavelength tile) from the device queue, longest
  * columns first; the column's records stream through the warp's shared-memory buffers. */
-__global__ void __launch_bounds__(128, 5) k_batch_mixed_staged(const __grid_constant__ MixedBatchArgs b) {
+__global__ void __launch_bounds__(128, 5) k_batch_mixed_staged(const MixedBatchArgs b) {
   __shared__ __align__(128) float s_rec[MWARPS][2 * MZC * MZN];
   __shared__ __align__(8) unsigned long long s_bar[MWARPS][2];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -685,18 +541,14 @@ __global__ void __launch_bounds__(128, 5) k_batch_mixed_staged(const __grid_cons
       pa.wait(1);
       return;
     }
-    const unsigned m = __ballot_sync(0xffffffffu, flag);
-    if (m) { /* every record copy of this task has landed: the buffers hold the FP64 records */
-      repair_batch_staged(b, reinterpret_cast<double *>(s_rec[wib]), slot, (int32_t)t.x, iw, flag);
-      if (lane == 0) atomicAdd(b.repairs, (unsigned long long)__popc(m));
-    }
+    push_flagged(flag, ((unsigned long long)t.x << 32) | (unsigned)iw, b.rlist, b.rcount);
   }
 }
 
 /* Packed tiling: the (column, wavelength) items of the columns sorted by nz (longest first)
  * form one list; a warp takes 32 consecutive items, so partial wavelength tiles of one column
  * are filled with the next column's items (similar nz, as the list is sorted). */
-__global__ void __launch_bounds__(128, 5) k_batch_mixed_packed(const __grid_constant__ MixedBatchArgs b) {
+__global__ void __launch_bounds__(128, 5) k_batch_mixed_packed(const MixedBatchArgs b) {
   const int lane = threadIdx.x & 31;
   const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   float4 *s4 = b.s4 + slot * 32 * (int64_t)b.max_nz + lane; /* the warp's scratch: [z][lane], contiguous */
@@ -724,11 +576,7 @@ __global__ void __launch_bounds__(128, 5) k_batch_mixed_packed(const __grid_cons
       MDirect pa{b.rec + c.rec_off * MZN};
       flag = msolve_item(batch_item(b, c, iw), true, pa, s4, 32, b.repair_cond) || __ldg(b.colflag + col) != 0u;
     }
-    const unsigned m = __ballot_sync(0xffffffffu, flag);
-    if (m) { /* lanes may hold different columns: each computes its own records */
-      repair_batch_lanes(b, slot, col, iw, flag);
-      if (lane == 0) atomicAdd(b.repairs, (unsigned long long)__popc(m));
-    }
+    push_flagged(flag, ((unsigned long long)(unsigned)col << 32) | (unsigned)iw, b.rlist, b.rcount);
   }
 }
 

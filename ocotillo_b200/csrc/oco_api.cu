@@ -103,6 +103,7 @@ extern "C" void oco_destroy(oco_ctx *c) {
   c->scratch64.release();
   c->stats.release();
   c->colflag.release();
+  c->rlist.release();
   for (auto &s : c->stage) {
     s.rho.release();
     s.T.release();
@@ -297,8 +298,7 @@ static int check_params(oco_ctx *c, const oco_params *p) {
 static const int kSolveThreads = 128;
 
 /* Grid of the persistent solve kernel and its scratch: per resident thread and z, FP64
- * gamma, u, 1/kappa, q (32 B) or, for the mixed form, one float4 (16 B) plus the 32 B of the
- * FP64 re-solve of flagged items. */
+ * gamma, u, 1/kappa, q (32 B) or, for the mixed form, one float4 (16 B). */
 static int prepare_solve(oco_ctx *c, int form, int grey, int64_t nitems, int nz, int *blocks) {
   const bool mixed = form == OCO_FORM_MIXED;
   int bps = mixed ? solve_mixed_max_blocks_per_sm(kSolveThreads, c->nw)
@@ -309,7 +309,6 @@ static int prepare_solve(oco_ctx *c, int form, int grey, int64_t nitems, int nz,
   *blocks = (int)std::max<int64_t>(1, std::min(maxb, need));
   size_t slots = (size_t)(*blocks) * kSolveThreads;
   CU(c->scratch.ensure(slots * (size_t)nz * (mixed ? 16 : 4 * sizeof(double))));
-  if (mixed) CU(c->scratch64.ensure(slots * (size_t)nz * 4 * sizeof(double))); /* FP64 re-solves */
   return OCO_OK;
 }
 
@@ -381,22 +380,45 @@ static int run_chunk_mixed(oco_ctx *c, const oco_params *p, const double *rho, c
   a.slot_stride = (int64_t)slots;
   a.work = c->work.as<unsigned long long>();
   a.status = c->status.as<unsigned long long>();
-  a.rho = rho;
-  a.T = T;
-  a.lam64 = c->lam.as<double>();
-  a.fully_ionized_T = p->fully_ionized_T;
-  a.s64 = c->scratch64.as<double>();
   a.repair_cond = c->repair_cond;
-  a.repairs = c->stats.as<unsigned long long>();
   a.colflag = c->colflag.as<unsigned>();
+  CU(c->rlist.ensure((size_t)nb * p->nw * sizeof(unsigned long long)));
+  a.rlist = c->rlist.as<unsigned long long>();
+  a.rcount = c->stats.as<unsigned long long>() + 1;
+  CU(cudaMemsetAsync(a.rcount, 0, sizeof(unsigned long long), s));
   CU(cudaMemsetAsync(a.work, 0, sizeof(unsigned long long), s));
+  /* the FP64 re-solve of the flagged items (stable form), after the mixed solve */
+  RepairArgs r{};
+  r.list = a.rlist;
+  r.count = a.rcount;
+  r.block = 1;
+  r.rho = rho;
+  r.T = T;
+  r.nz = p->nz;
+  r.nw = p->nw;
+  r.dz = p->dz;
+  r.dz1 = a64.dz1;
+  r.dz2 = a64.dz2;
+  r.U = a64.U, r.U_zs = a64.U_zs, r.U_is = a64.U_is;
+  r.K = a64.K, r.K_zs = a64.K_zs, r.K_is = a64.K_is;
+  r.V = a64.V, r.V_zs = a64.V_zs, r.V_is = a64.V_is;
+  r.Vtop = a64.Vtop, r.Vbot = a64.Vbot;
+  r.ld_col = a64.ld_col, r.c_off = a64.c_off, r.layout = a64.layout;
+  r.lam64 = c->lam.as<double>();
+  r.fully_ionized_T = p->fully_ionized_T;
+  CU(c->scratch64.ensure((size_t)c->num_sms * REPAIR_WARPS_PER_SM * 11 * p->nz * sizeof(double)));
+  r.scratch = c->scratch64.as<double>();
+  r.max_nz = p->nz;
+  r.repairs = c->stats.as<unsigned long long>();
+  r.status = c->status.as<unsigned long long>();
   if (c->prof) CU(cudaEventRecord(e2, s));
   CU(launch_solve_mixed(a, blocks, kSolveThreads, s));
+  CU(launch_repair(r, c->num_sms, s));
   if (c->prof) {
     CU(cudaEventRecord(e3, s));
     c->ev_solve.emplace_back(e2, e3);
   }
-  c->launches += 2;
+  c->launches += 3;
   return OCO_OK;
 }
 

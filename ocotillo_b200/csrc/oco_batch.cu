@@ -52,7 +52,7 @@ struct oco_batch {
      Vtop and Vbot), {-1, -1} if none: binding an array of an overlapping family fails */
   int64_t overlap[3][2] = {{-1, -1}, {-1, -1}, {-1, -1}};
   DevBuf cols, rec_pre, tasks, order, item_pre, lam, rec, scratch, work, status;
-  DevBuf lam64, scratch64, colflag; /* mixed form: FP64 tables, scratch and column marks of the re-solve */
+  DevBuf lam64, scratch64, colflag, rlist; /* mixed form: FP64 tables, scratch, column marks and flagged list of the re-solve */
   int64_t slots = 0; /* scratch slots (threads of the largest persistent grid) */
   int tiling = OCO_TILING_WARP_COLUMN, bps = 1, max_bps[2] = {1, 1}; /* max_bps 0: tiling not available */
   /* bound arrays */
@@ -90,15 +90,31 @@ static MixedBatchArgs batch_args(const oco_batch *b) {
   a.max_nz = b->max_nz;
   a.work = b->work.as<unsigned long long>();
   a.status = b->status.as<unsigned long long>();
-  a.rho = b->rho;
-  a.T = b->T;
-  a.lam64 = b->lam64.as<double>();
-  a.fully_ionized_T = b->fully_ionized_T;
-  a.s64 = b->scratch64.as<double>();
   a.repair_cond = b->c->repair_cond;
-  a.repairs = b->c->stats.as<unsigned long long>();
   a.colflag = b->colflag.as<unsigned>();
+  a.rlist = b->rlist.as<unsigned long long>();
+  a.rcount = b->status.as<unsigned long long>() + 4;
   return a;
+}
+
+/* The FP64 re-solve of the items the mixed batch kernel flags (stable form). */
+static RepairArgs repair_args(const oco_batch *b) {
+  RepairArgs r{};
+  r.list = b->rlist.as<unsigned long long>();
+  r.count = b->status.as<unsigned long long>() + 4;
+  r.block = 0;
+  r.rho = b->rho;
+  r.T = b->T;
+  r.U = b->U, r.K = b->K, r.V = b->V, r.Vtop = b->Vtop, r.Vbot = b->Vbot;
+  r.layout = b->layout;
+  r.cols = b->cols.as<MBatchCol>();
+  r.lam64 = b->lam64.as<double>();
+  r.fully_ionized_T = b->fully_ionized_T;
+  r.scratch = b->scratch64.as<double>();
+  r.max_nz = b->max_nz;
+  r.repairs = b->c->stats.as<unsigned long long>();
+  r.status = b->status.as<unsigned long long>();
+  return r;
 }
 
 static FP64BatchArgs fp64_args(const oco_batch *b) {
@@ -139,8 +155,10 @@ static int enqueue_run(oco_batch *b, cudaStream_t s) {
     CU(launch_pillars_mixed_batch(b->rho, b->T, b->cols.as<MBatchCol>(), b->rec_pre.as<int64_t>(), b->ncol, b->nrec,
                                   b->fully_ionized_T, b->rec.as<float>(), b->colflag.as<unsigned>(), s));
     const MixedBatchArgs a = batch_args(b);
+    CU(cudaMemsetAsync(a.rcount, 0, sizeof(unsigned long long), s));
     CU(launch_batch_mixed(a, b->tiling == OCO_TILING_PACKED ? BATCH_TILING_PACKED : BATCH_TILING_WARP_COLUMN, blocks,
                           kBatchThreads, s));
+    CU(launch_repair(repair_args(b), c->num_sms, s));
   } else {
     CU(launch_pillars_batch(b->rho, b->T, b->cols.as<MBatchCol>(), b->rec_pre.as<int64_t>(), b->ncol, b->nrec,
                             b->fully_ionized_T, b->rec.as<double>(), s));
@@ -330,8 +348,9 @@ static int batch_create(oco_ctx *c, const oco_batch_column *cols, int64_t ncol, 
     CU(b->rec.ensure((size_t)b->nrec * MIXED_ZN * sizeof(float)));
     CU(b->scratch.ensure((size_t)b->slots * b->max_nz * sizeof(float4)));
     CU(b->lam64.ensure(lam64.size() * sizeof(double)));
-    CU(b->scratch64.ensure((size_t)4 * b->slots * b->max_nz * sizeof(double)));
+    CU(b->scratch64.ensure((size_t)c->num_sms * REPAIR_WARPS_PER_SM * 11 * b->max_nz * sizeof(double)));
     CU(b->colflag.ensure((size_t)ncol * sizeof(unsigned)));
+    CU(b->rlist.ensure((size_t)b->nitems * sizeof(unsigned long long)));
   }
   CU(b->work.ensure(64));
   CU(b->status.ensure(64));
@@ -522,7 +541,7 @@ extern "C" void oco_batch_destroy(oco_batch *b) {
   if (b->pending) cudaStreamSynchronize(b->last); /* a null stream is the default stream */
   if (b->cap) cudaStreamSynchronize(b->cap);
   drop_graph(b);
-  for (DevBuf *d : {&b->lam64, &b->scratch64, &b->colflag, &b->cols, &b->rec_pre, &b->tasks, &b->order, &b->item_pre, &b->lam, &b->rec, &b->scratch,
+  for (DevBuf *d : {&b->lam64, &b->scratch64, &b->colflag, &b->rlist, &b->cols, &b->rec_pre, &b->tasks, &b->order, &b->item_pre, &b->lam, &b->rec, &b->scratch,
                     &b->work, &b->status})
     d->release();
   if (b->after_last) cudaEventDestroy(b->after_last);

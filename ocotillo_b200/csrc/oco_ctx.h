@@ -57,9 +57,10 @@ struct oco_ctx {
   DevBuf trapw; /* trapezoid weights of the wavelength grid, cm (oco_integrated_flux_device) */
   /* workspace */
   DevBuf pil, scratch, work, status;
-  /* mixed form: FP64 scratch of the in-place re-solve of ill-conditioned items, and counters
-   * ([0] items re-solved since the last oco_mixed_repairs) */
-  DevBuf scratch64, stats, colflag; /* colflag: columns of the chunk re-solved in FP64 entirely */
+  /* mixed form: the list of flagged items of a chunk, the FP64 re-solve's scratch, column marks
+   * and counters ([0] items re-solved since the last oco_mixed_repairs, [1] items flagged in the
+   * current chunk) */
+  DevBuf scratch64, stats, colflag, rlist;
   float repair_cond = 100.0f; /* oco_set_mixed_repair */
   Stage stage[2];
   int64_t launches = 0;

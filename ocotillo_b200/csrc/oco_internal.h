@@ -123,15 +123,11 @@ struct MixedArgs {
   int64_t slot_stride; /* resident threads the scratch is sized for */
   unsigned long long *work;
   unsigned long long *status;
-  /* FP64 re-solve (stable form) of the items whose emergent flux the FP32 arithmetic cannot
-   * resolve: a warp that flags items re-solves them at once, in place */
-  const double *rho, *T; /* the chunk's inputs [ncol][nz] */
-  const double *lam64;   /* [NL][nw] FP64 wavelength table */
-  double fully_ionized_T;
-  double *s64;           /* FP64 scratch [warp slot][4][nz][32]: gamma, u, 1/kappa, q */
-  float repair_cond;     /* re-solve when the boundary-flux condition number exceeds this */
-  unsigned long long *repairs; /* [0] items re-solved in FP64 (accumulates) */
-  const unsigned *colflag;     /* [ncol] columns re-solved in FP64 entirely (record kernel) */
+  /* Items whose emergent flux the FP32 arithmetic cannot resolve are appended to rlist
+   * (chunk-local id cl*nw + iw; *rcount of them) for the FP64 re-solve (RepairArgs). */
+  float repair_cond;           /* flag when the boundary-flux condition number exceeds this */
+  const unsigned *colflag;     /* [ncol] columns flagged entirely (record kernel) */
+  unsigned long long *rlist, *rcount;
 };
 
 /* One column of a ragged batch as the batch kernels see it (built from oco_batch_column). */
@@ -165,15 +161,40 @@ struct MixedBatchArgs {
   int max_nz;
   unsigned long long *work;
   unsigned long long *status;
-  /* FP64 re-solve of ill-conditioned items (as in MixedArgs) */
-  const double *rho, *T;   /* the bound inputs (column profiles at in_off) */
-  const double *lam64;     /* packed [NL][nw] FP64 tables: a column's starts at lam_off / MIXED_LN * NL */
-  double fully_ionized_T;
-  double *s64;             /* FP64 scratch [warp slot][4][max_nz][32] */
+  /* flagged items as in MixedArgs; id (column << 32) | wavelength */
   float repair_cond;
-  unsigned long long *repairs;
-  const unsigned *colflag; /* [ncol] columns re-solved in FP64 entirely */
+  const unsigned *colflag; /* [ncol] columns flagged entirely */
+  unsigned long long *rlist, *rcount;
 };
+
+/* The FP64 re-solve (stable form) of the items the mixed kernels flagged (kernels_repair.cu):
+ * one warp per item, the records, opacities and row coefficients computed by the 32 lanes, the
+ * elimination and back-substitution by one lane, results stored over the mixed ones.  The
+ * arithmetic is solve_item's, operation for operation, so a re-solved item equals the stable
+ * FP64 form bit for bit.  block != 0: items of a block chunk (the outputs as in SolveArgs);
+ * otherwise items of a ragged batch (the outputs as in FP64BatchArgs). */
+struct RepairArgs {
+  const unsigned long long *list, *count;
+  int block;
+  /* block chunk */
+  const double *rho, *T; /* the chunk's inputs [ncol][nz] */
+  int nz, nw;
+  double dz, dz1, dz2;
+  double *U, *K, *V, *Vtop, *Vbot;
+  int64_t U_zs, U_is, K_zs, K_is, V_zs, V_is, ld_col, c_off;
+  int layout;
+  /* batch */
+  const MBatchCol *cols;   /* lam_off indexes the mixed tables: the FP64 table starts at lam_off / MIXED_LN * NL */
+  /* both */
+  const double *lam64;     /* [NL][nw] (block) or packed tables (batch) */
+  double fully_ionized_T;
+  double *scratch;         /* per warp 11 arrays of max_nz doubles */
+  int max_nz;
+  unsigned long long *repairs; /* += *count */
+  unsigned long long *status;  /* zero-pivot words as in SolveArgs */
+};
+constexpr int REPAIR_WARPS_PER_SM = 16; /* persistent grid of the re-solve: 4 blocks of 128 threads per SM */
+cudaError_t launch_repair(const RepairArgs &a, int num_sms, cudaStream_t s);
 
 /* Arguments of the ragged-batch kernels (plain and stable FP64 forms; warp-column tiling). */
 struct FP64BatchArgs {
@@ -256,8 +277,8 @@ cudaError_t launch_bounded_wait_check(long long limit, unsigned long long *statu
 /* Mixed-precision kernels (kernels_mixed.cu). */
 constexpr int MIXED_ZN = 64; /* floats per mixed record */
 /* Default condition number of the mixed form's emergent flux above which an item is re-solved
- * in FP64 (stable form): the flux is a weighted sum of boundary differences D_k = u_k - q_k
- * U_{k+1}, and its condition number is sum |w_k| (u_k + q_k U_{k+1}) / |sum w_k D_k|. */
+ * in FP64 (stable form, k_repair): the flux is a weighted sum of boundary differences
+ * D_k = u_k - q_k U_{k+1}, and its condition number is sum |w_k| (u_k + q_k U_{k+1}) / |sum w_k D_k|. */
 constexpr float MIXED_REPAIR_COND = 100.0f;
 constexpr int MIXED_LN = 29; /* fields of the mixed wavelength table */
 /* colflag[ncol] (cleared by the caller) marks columns to re-solve in FP64 (mx::pillar). */

@@ -136,8 +136,9 @@ def sensitive_block():
 
 
 def test_mixed_emergent_flux_on_sensitive_agn_columns(engine, oracle, sensitive_block):
-    """The 1e-4 bar on the emergent flux holds on the grid's most sensitive columns: the
-    kernels flag the items whose flux condition number exceeds 100 and re-solve them in FP64."""
+    """The 1e-4 bar on the emergent flux holds on the grid's most sensitive columns: the mixed
+    kernels flag the items whose flux condition number exceeds 100 and a second kernel re-solves
+    them in FP64."""
     rho, T, dz, wa = sensitive_block
     engine.set_wavelengths(wa)
     engine.set_mixed_repair(100.0)
@@ -147,26 +148,28 @@ def test_mixed_emergent_flux_on_sensitive_agn_columns(engine, oracle, sensitive_
     ref = oracle.solve_block(rho, T, wa, dz, form=oracle.FORM_STABLE, backend="ocomath", want=("V",))
     err = np.maximum(_rel(out["Vtop"], ref["V"][..., -1]), _rel(out["Vbot"], ref["V"][..., 0]))
     assert err.max() <= TOL_FLUX, err.max()
-    items = err.size
-    assert 0 < repaired < 0.05 * items, repaired
+    # 40 of these 64 columns are the grid's most sensitive, so a large share of their items is
+    # re-solved (about 0.07% of the whole grid's); the count only has to be positive and bounded
+    assert 0 < repaired < 0.5 * err.size, repaired
 
 
 def test_mixed_repair_is_the_stable_fp64_solve(engine, oracle, sensitive_block):
-    """Without the re-solve some items of these columns miss 1e-4; with it, the items it changed
-    equal the stable FP64 form to rounding (this unit contracts FMAs, so not bit for bit)."""
+    """Without the re-solve some items of these columns miss 1e-4; with it, every item it changed
+    equals the stable FP64 form bit for bit (U at every z, kappa, V and the emergent fluxes)."""
     rho, T, dz, wa = sensitive_block
     engine.set_wavelengths(wa)
     engine.set_mixed_repair(float("inf"))
-    raw = engine.solve_block(rho, T, dz, form="mixed", want=("Vtop", "Vbot"))
+    raw = engine.solve_block(rho, T, dz, form="mixed")
     assert engine.mixed_repairs() == 0
     engine.set_mixed_repair(100.0)
-    fixed = engine.solve_block(rho, T, dz, form="mixed", want=("Vtop", "Vbot"))
+    fixed = engine.solve_block(rho, T, dz, form="mixed")
+    stable = engine.solve_block(rho, T, dz, form="stable")
+    changed = (raw["Vtop"] != fixed["Vtop"]) | (raw["Vbot"] != fixed["Vbot"])
+    assert changed.any()
+    for key in ("U", "kappa", "V", "Vtop", "Vbot"):
+        a, b = fixed[key][changed], stable[key][changed]
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), key
     ref = oracle.solve_block(rho, T, wa, dz, form=oracle.FORM_STABLE, backend="ocomath", want=("V",))
-    for key, end in (("Vtop", -1), ("Vbot", 0)):
-        r = ref["V"][..., end]
-        changed = raw[key] != fixed[key]
-        assert changed.any()
-        assert _rel(fixed[key][changed], r[changed]).max() <= 1e-9, key
     worst_raw = max(_rel(raw["Vtop"], ref["V"][..., -1]).max(), _rel(raw["Vbot"], ref["V"][..., 0]).max())
     assert worst_raw > TOL_FLUX  # the columns are sensitive enough to need the re-solve
 
