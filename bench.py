@@ -316,19 +316,40 @@ class Grid:
         achieved = bytes_pt * pts_launch / (launch_ms / 1e3) / 1e9
         flops = 97.0 * pts_launch / (launch_ms / 1e3) / 1e12
         tpp = TRAFFIC_BYTES_PER_POINT.get(form) if (self.nz, self.nw, self.layout) == (512, 256, 1) else None
-        return {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+        res = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                 "traffic": tpp * pts_launch if tpp else None,
                 "traffic_source": "ncu capture of a 1024-column launch, scaled by points" if tpp else None,
                 "kernel": "k_solve_staged" if form != "mixed" else "k_solve_mixed_staged",
                 "launch_ms": launch_ms, "points_per_launch": pts_launch, "algorithmic_bytes_per_point": bytes_pt,
                 "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in pk else "fallback",
-                "algorithmic_tflops": flops, "flops_per_point": 97,
+                "algorithmic_tflops": flops, "census_flops_per_point": 97,
                 "solve_share_of_step": m["solve_ms"] / m["total_ms"], "pillars_ms_per_step": m["pil_ms"] / steps}
+        fc = FP_COUNTERS["mixed" if form == "mixed" else "plain"]
+        rate = pts_launch / (launch_ms / 1e3)
+        res["fp64"] = {"executed_flops_per_point": fc["fp64_flops_per_point"],
+                       "achieved_tflops": fc["fp64_flops_per_point"] * rate / 1e12, "peak_tflops": FP64_PEAK_TFLOPS,
+                       "frac": fc["fp64_flops_per_point"] * rate / 1e12 / FP64_PEAK_TFLOPS,
+                       "pipe_active": fc["fp64_pipe_active"], "peak_source": "nominal"}
+        res["fp32"] = {"executed_flops_per_point": fc["fp32_flops_per_point"],
+                       "achieved_tflops": fc["fp32_flops_per_point"] * rate / 1e12, "peak_tflops": FP32_PEAK_TFLOPS,
+                       "frac": fc["fp32_flops_per_point"] * rate / 1e12 / FP32_PEAK_TFLOPS,
+                       "fma_pipe_active": fc["fma_pipe_active"], "xu_active": fc["xu_active"], "peak_source": "nominal"}
+        res["fp_counters_source"] = "ncu counters of a 1024-column launch (profiles/fp_pipes_*); rate from this run"
+        return res
 
 
 # The reference's published rate for this path: 0.14415 us per mesh*lambda point (its README,
 # multiInTest sample, one CPU core) = 6.94e6 points/s.
 PUBLISHED_POINTS_PER_S = 1e6 / 0.14415
+
+# Executed floating-point work per mesh*lambda point of the solve kernels (ncu counters of a
+# 1024-column launch of this grid: profiles/fp_pipes_k_solve_staged_k_solve_mixed_staged_agn_32x32x512x256.txt):
+# FP64 flops = DADD + DMUL + 2 DFMA, FP32 flops = FADD + FMUL + 2 FFMA, and the pipes' activity.
+FP_COUNTERS = {"plain": {"fp64_flops_per_point": 347.6, "fp32_flops_per_point": 12.0, "fp64_pipe_active": 0.470,
+                         "fma_pipe_active": 0.096, "xu_active": 0.052},
+               "mixed": {"fp64_flops_per_point": 14.1, "fp32_flops_per_point": 128.9, "fp64_pipe_active": 0.052,
+                         "fma_pipe_active": 0.328, "xu_active": 0.461}}
+FP64_PEAK_TFLOPS, FP32_PEAK_TFLOPS = 37.0, 75.0  # nominal B200 (no measured FP figure in MEASURED_PEAKS.json)
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per mesh*lambda point of the solve
 # kernel, from one ncu --set full capture of a 1024-column launch of this grid (outputs 3.2 GB,
