@@ -219,6 +219,7 @@ __global__ void __launch_bounds__(128) k_solve(const SolveArgs a) {
 template <int FORM, bool GREY>
 __global__ void __launch_bounds__(128, 4) k_solve_staged(const SolveArgs a) {
   __shared__ __align__(128) double s_pil[WARPS_PER_BLOCK][2 * ZC * NF];
+  __shared__ __align__(16) double s_lam[WARPS_PER_BLOCK][NLF * 32]; /* the task's 32 wavelengths' constants */
   __shared__ __align__(8) unsigned long long s_bar[WARPS_PER_BLOCK][2];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -253,7 +254,10 @@ __global__ void __launch_bounds__(128, 4) k_solve_staged(const SolveArgs a) {
     const bool active = iw_raw < a.nw;
     const int iw = active ? iw_raw : a.nw - 1;
     pa.begin(a.pil + cl * (int64_t)a.nz * NF, lane);
-    solve_item<FORM, GREY>(BlockItem{a, cl, iw}, active, pa, gam, uu, o1, qs);
+    if (!GREY) store_lam_shared(&s_lam[wib][lane], a.lam, iw, a.nw);
+    __syncwarp();
+    solve_item<FORM, GREY, BlockItem, StagedPillars, LamS>(BlockItem{a, cl, iw}, active, pa, gam, uu, o1, qs,
+                                                          &s_lam[wib][lane]);
     if (__any_sync(0xffffffffu, pa.failed)) {
       if (lane == 0) atomicOr(&a.status[2], 1ull);
       /* let copies still in flight land (bounded) before the block's shared memory is released */

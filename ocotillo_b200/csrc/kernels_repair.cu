@@ -104,8 +104,7 @@ __device__ __forceinline__ void repair_item(const IT &it, double fit, const RScr
   const int nz = it.nz();
   const double dz = it.dz(), dz2 = it.dz2();
   const double *rho = it.rho(), *T = it.T();
-  Lam L;
-  load_lam(L, it.lam(), it.iw(), it.nw());
+  const LamR L(it, nullptr);
   double *Kb = it.K();
   const int64_t kz = it.kz();
   /* 1. records and opacities, 32 levels at a time */
