@@ -124,7 +124,8 @@ int oco_solve_block_device(oco_ctx *ctx, const oco_params *p, const double *rho,
                            double *Vtop, double *Vbot, void *stream);
 
 /* Waits for the context's work; returns OCO_EZEROPIVOT if a device-array solve since the
- * last call met a zero pivot. */
+ * last call met a zero pivot.  oco_last_error names the first such item's (ix, iy, iw) when
+ * every pending call had the same nx, ny and nw, and only the count otherwise. */
 int oco_synchronize(oco_ctx *ctx);
 
 /* Mixed form: the FP32 arithmetic resolves an emergent flux to ~1e-5 only where the flux is

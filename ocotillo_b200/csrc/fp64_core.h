@@ -272,7 +272,16 @@ __device__ __forceinline__ Opac opacity_grey(const R P, double sg) {
 /* The reverse sweep of one item (back-substitution, tridag :43-45; ghost zones :49-62; flux
  * :96-109) from the forward sweep's last u and its scratch (gam, uu, o1s and, stable form, qs at
  * stride it.ss()), storing U, V and the emergent fluxes through the item accessor. */
-template <int FORM, class IT>
+/* Issues an L2 prefetch of the line holding p. */
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(__cvta_generic_to_global(p)));
+}
+
+/* PF: the scratch was written long before (by another kernel) and few warps run, so its loads
+ * are DRAM latency: 1/kappa is loaded with the other scratch arrays 8 levels ahead of the
+ * serial chain and the next blocks of 8 levels are prefetched into L2 (the block solves keep
+ * PF off: their scratch is recent and many warps hide its latency). */
+template <int FORM, class IT, bool PF = false>
 __device__ __forceinline__ void solve_reverse(const IT &it, double u, const double *__restrict__ gam,
                                               const double *__restrict__ uu, const double *__restrict__ o1s,
                                               const double *__restrict__ qs) {
@@ -305,28 +314,49 @@ __device__ __forceinline__ void solve_reverse(const IT &it, double u, const doub
     if (Ub) __stcs(&Ub[(n + 4) * uz], 2.0 * fn - Uk[1]);
     if (Ub) __stcs(&Ub[(n + 5) * uz], 2.0 * fn - Uk[2]);
     double d0 = Dt[2], d1 = Dt[1], d2 = Dt[0], d3 = Dt[0], d4 = Dt[1], d5 = Dt[2];
-    auto emitD = [&](int j) -> double {
+    auto emitDo = [&](int j, double o1j) -> double {
       const double s1 = d2 + d3;
       const double s2 = (s1 + d1) + d4;
       const double s3 = (s2 + d0) + d5;
       const double df = -((1.0 / 60.0) * (((45.0 * s1) - 9.0 * s2) + s3));
-      const double v = ((-1.0 * o1s[j * ss]) * df) * dz1;
+      const double v = ((-1.0 * o1j) * df) * dz1;
       if (Vb) __stcs(&Vb[j * it.vz()], v);
       return v;
     };
+    auto emitD = [&](int j) -> double { return emitDo(j, o1s[j * ss]); };
     vtop = emitD(n - 1);
     double U0 = Uk[2], U1 = Uk[1], U2 = Uk[0], U3 = u; /* the four lowest U seen so far */
-    auto stepD = [&](int k, double uf, double qk, double gk1) {
+    auto stepDo = [&](int k, double uf, double qk, double gk1, double o1k3) {
       const double Dk = uf - qk * Un;
       Un = uf - gk1 * Un;
       if (Ub) __stcs(&Ub[(3 + k) * uz], Un);
       U3 = U2; U2 = U1; U1 = U0; U0 = Un;
       d5 = d4; d4 = d3; d3 = d2; d2 = d1; d1 = d0; d0 = Dk;
-      emitD(k + 3);
+      emitDo(k + 3, o1k3);
     };
+    auto stepD = [&](int k, double uf, double qk, double gk1) { stepDo(k, uf, qk, gk1, o1s[(k + 3) * ss]); };
     int k = n - 5;
     for (; k >= 7; k -= 8) { /* scratch loads of 8 steps hoisted off the serial chain */
       double ub[8], qb[8], gb[8];
+      if (PF) {
+        double ob[8];
+        for (int q = 16; q < 24 && k - q >= 0; q++) { /* the block after next */
+          prefetch_l2(&uu[(k - q) * ss]);
+          prefetch_l2(&qs[(k - q) * ss]);
+          prefetch_l2(&gam[(k - q + 1) * ss]);
+          prefetch_l2(&o1s[(k - q + 3) * ss]);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          ub[q] = uu[(k - q) * ss];
+          qb[q] = qs[(k - q) * ss];
+          gb[q] = gam[(k - q + 1) * ss];
+          ob[q] = o1s[(k - q + 3) * ss];
+        }
+#pragma unroll
+        for (int q = 0; q < 8; q++) stepDo(k - q, ub[q], qb[q], gb[q], ob[q]);
+        continue;
+      }
 #pragma unroll
       for (int q = 0; q < 8; q++) {
         ub[q] = uu[(k - q) * ss];

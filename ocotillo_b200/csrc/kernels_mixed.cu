@@ -373,17 +373,44 @@ __device__ __forceinline__ bool msolve_item(const MItem &it, bool active, PA &pa
   return flag;
 }
 
-/* Appends the warp's flagged items (lanes with flag set) to the re-solve list: one atomic per
- * warp, then each flagged lane writes its id at its rank among the flagged lanes. */
-__device__ __forceinline__ void push_flagged(bool flag, unsigned long long id, unsigned long long *list,
-                                             unsigned long long *count) {
+/* The re-solve's lists (RepairArgs): each flagged item's id goes to ilist (its index there is
+ * the item's slot, also stored beside its bit), and each word of flag bits (a column's 32
+ * wavelengths) that receives a bit goes to wlist once.  mark_tile serves the tilings whose warp
+ * task is one (column, 32-wavelength tile): the tile is one word and no other warp writes it, so
+ * lane 0 stores the warp's ballot.  mark_items serves the tilings whose 32 items may span
+ * columns: each flagged lane sets its bit, and the lane that finds its word empty lists it. */
+__device__ __forceinline__ void list_items(bool flag, unsigned m, unsigned long long id, int64_t word, int iw,
+                                           unsigned long long *ilist, unsigned long long *icount, int *slot) {
+  const int lane = threadIdx.x & 31, first = __ffs(m) - 1;
+  unsigned long long base = 0;
+  if (lane == first) base = atomicAdd(icount, (unsigned long long)__popc(m));
+  base = __shfl_sync(0xffffffffu, base, first);
+  if (flag) {
+    const unsigned long long pos = base + __popc(m & ((1u << lane) - 1u));
+    ilist[pos] = id;
+    slot[word * 32 + (iw & 31)] = (int)pos;
+  }
+}
+
+__device__ __forceinline__ void mark_tile(bool flag, int64_t word, int iw, unsigned long long id, unsigned *bits,
+                                          int *slot, unsigned long long *wlist, unsigned long long *wcount,
+                                          unsigned long long *ilist, unsigned long long *icount) {
   const unsigned m = __ballot_sync(0xffffffffu, flag);
   if (!m) return;
-  const int lane = threadIdx.x & 31;
-  unsigned long long base = 0;
-  if (lane == __ffs(m) - 1) base = atomicAdd(count, (unsigned long long)__popc(m));
-  base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
-  if (flag) list[base + __popc(m & ((1u << lane) - 1u))] = id;
+  if ((threadIdx.x & 31) == 0) {
+    bits[word] = m;
+    wlist[atomicAdd(wcount, 1ull)] = (unsigned long long)word;
+  }
+  list_items(flag, m, id, word, iw, ilist, icount, slot);
+}
+
+__device__ __forceinline__ void mark_items(bool flag, int64_t word, int iw, unsigned long long id, unsigned *bits,
+                                           int *slot, unsigned long long *wlist, unsigned long long *wcount,
+                                           unsigned long long *ilist, unsigned long long *icount) {
+  const unsigned m = __ballot_sync(0xffffffffu, flag);
+  if (!m) return;
+  if (flag && atomicOr(bits + word, 1u << (iw & 31)) == 0u) wlist[atomicAdd(wcount, 1ull)] = (unsigned long long)word;
+  list_items(flag, m, id, word, iw, ilist, icount, slot);
 }
 
 __global__ void __launch_bounds__(128, 5) k_solve_mixed_staged(const MixedArgs a) {
@@ -426,7 +453,8 @@ __global__ void __launch_bounds__(128, 5) k_solve_mixed_staged(const MixedArgs a
       pa.wait(1);
       return;
     }
-    push_flagged(flag, (unsigned long long)(cl * a.nw + iw), a.rlist, a.rcount);
+    mark_tile(flag, cl * ntiles + iw / 32, iw, (unsigned long long)(cl * a.nw + iw), a.rbits, a.rslot, a.rlist,
+              a.rcount, a.ilist, a.icount);
   }
 }
 
@@ -443,13 +471,16 @@ __global__ void __launch_bounds__(128, 5) k_solve_mixed(const MixedArgs a) {
     if (task >= ntasks) break;
     const int64_t item = (int64_t)task * 32 + lane;
     bool flag = false;
+    int64_t word = 0;
+    int iw = 0;
     if (item < nitems) {
       const int64_t cl = item / a.nw;
-      const int iw = (int)(item - cl * a.nw);
+      iw = (int)(item - cl * a.nw);
       MDirect pa{a.rec + cl * (int64_t)a.nz * MZN};
       flag = msolve_item(block_item(a, cl, iw), true, pa, s4, 32, a.repair_cond) || __ldg(a.colflag + cl) != 0u;
+      word = cl * ((a.nw + 31) / 32) + iw / 32;
     }
-    push_flagged(flag, (unsigned long long)item, a.rlist, a.rcount);
+    mark_items(flag, word, iw, (unsigned long long)item, a.rbits, a.rslot, a.rlist, a.rcount, a.ilist, a.icount);
   }
 }
 
@@ -541,7 +572,8 @@ __global__ void __launch_bounds__(128, 5) k_batch_mixed_staged(const MixedBatchA
       pa.wait(1);
       return;
     }
-    push_flagged(flag, ((unsigned long long)t.x << 32) | (unsigned)iw, b.rlist, b.rcount);
+    mark_tile(flag, (int64_t)t.x * b.rwstride + iw / 32, iw, ((unsigned long long)t.x << 32) | (unsigned)iw, b.rbits,
+              b.rslot, b.rlist, b.rcount, b.ilist, b.icount);
   }
 }
 
@@ -576,7 +608,8 @@ __global__ void __launch_bounds__(128, 5) k_batch_mixed_packed(const MixedBatchA
       MDirect pa{b.rec + c.rec_off * MZN};
       flag = msolve_item(batch_item(b, c, iw), true, pa, s4, 32, b.repair_cond) || __ldg(b.colflag + col) != 0u;
     }
-    push_flagged(flag, ((unsigned long long)(unsigned)col << 32) | (unsigned)iw, b.rlist, b.rcount);
+    mark_items(flag, (int64_t)col * b.rwstride + iw / 32, iw, ((unsigned long long)(unsigned)col << 32) | (unsigned)iw,
+               b.rbits, b.rslot, b.rlist, b.rcount, b.ilist, b.icount);
   }
 }
 

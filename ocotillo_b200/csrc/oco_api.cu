@@ -100,7 +100,9 @@ extern "C" void oco_destroy(oco_ctx *c) {
   c->tmpV.release();
   c->work.release();
   c->status.release();
-  c->scratch64.release();
+  c->rbits.release();
+  c->ilist.release();
+  c->rslot.release();
   c->stats.release();
   c->colflag.release();
   c->rlist.release();
@@ -363,6 +365,9 @@ static int run_chunk_mixed(oco_ctx *c, const oco_params *p, const double *rho, c
   int rc = prepare_solve(c, OCO_FORM_MIXED, 0, nb * p->nw, p->nz, &blocks);
   if (rc) return rc;
   const size_t slots = (size_t)blocks * kSolveThreads;
+  /* the re-solve takes over the mixed solve's scratch: at least its per-warp arrays and 32 slots */
+  const int rsolve_blocks = REPAIR_SOLVE_BLOCKS_PER_SM * c->num_sms, rcoef_blocks = REPAIR_COEF_BLOCKS_PER_SM * c->num_sms;
+  CU(c->scratch.ensure(((size_t)rsolve_blocks * (REPAIR_THREADS / 32) * 4 + 32 * 5) * p->nz * sizeof(double)));
   MixedArgs a{};
   a.rec = rec;
   a.lam = c->lam32.as<float>();
@@ -382,15 +387,29 @@ static int run_chunk_mixed(oco_ctx *c, const oco_params *p, const double *rho, c
   a.status = c->status.as<unsigned long long>();
   a.repair_cond = c->repair_cond;
   a.colflag = c->colflag.as<unsigned>();
-  CU(c->rlist.ensure((size_t)nb * p->nw * sizeof(unsigned long long)));
+  const int64_t nwords = (p->nw + 31) / 32;
+  CU(c->rbits.ensure((size_t)nb * nwords * sizeof(unsigned)));
+  CU(c->rlist.ensure((size_t)nb * nwords * sizeof(unsigned long long)));
+  CU(c->ilist.ensure((size_t)nb * p->nw * sizeof(unsigned long long)));
+  CU(c->rslot.ensure((size_t)nb * nwords * 32 * sizeof(int)));
+  a.rbits = c->rbits.as<unsigned>();
+  a.rslot = c->rslot.as<int>();
   a.rlist = c->rlist.as<unsigned long long>();
   a.rcount = c->stats.as<unsigned long long>() + 1;
-  CU(cudaMemsetAsync(a.rcount, 0, sizeof(unsigned long long), s));
+  a.ilist = c->ilist.as<unsigned long long>();
+  a.icount = c->stats.as<unsigned long long>() + 2;
+  CU(cudaMemsetAsync(a.rcount, 0, 2 * sizeof(unsigned long long), s));
+  CU(cudaMemsetAsync(a.rbits, 0, (size_t)nb * nwords * sizeof(unsigned), s));
   CU(cudaMemsetAsync(a.work, 0, sizeof(unsigned long long), s));
   /* the FP64 re-solve of the flagged items (stable form), after the mixed solve */
   RepairArgs r{};
   r.list = a.rlist;
   r.count = a.rcount;
+  r.ilist = a.ilist;
+  r.icount = a.icount;
+  r.bits = a.rbits;
+  r.slot = a.rslot;
+  r.wstride = nwords;
   r.block = 1;
   r.rho = rho;
   r.T = T;
@@ -406,19 +425,19 @@ static int run_chunk_mixed(oco_ctx *c, const oco_params *p, const double *rho, c
   r.ld_col = a64.ld_col, r.c_off = a64.c_off, r.layout = a64.layout;
   r.lam64 = c->lam.as<double>();
   r.fully_ionized_T = p->fully_ionized_T;
-  CU(c->scratch64.ensure((size_t)c->num_sms * REPAIR_WARPS_PER_SM * 11 * p->nz * sizeof(double)));
-  r.scratch = c->scratch64.as<double>();
+  r.scratch = c->scratch.as<double>(); /* the mixed solve's */
   r.max_nz = p->nz;
+  r.cap = repair_capacity(c->scratch.n, p->nz, rsolve_blocks);
   r.repairs = c->stats.as<unsigned long long>();
   r.status = c->status.as<unsigned long long>();
   if (c->prof) CU(cudaEventRecord(e2, s));
   CU(launch_solve_mixed(a, blocks, kSolveThreads, s));
-  CU(launch_repair(r, c->num_sms, s));
+  CU(launch_repair(r, rcoef_blocks, rsolve_blocks, s));
   if (c->prof) {
     CU(cudaEventRecord(e3, s));
     c->ev_solve.emplace_back(e2, e3);
   }
-  c->launches += 3;
+  c->launches += 4;
   return OCO_OK;
 }
 
@@ -480,6 +499,13 @@ static int read_status(oco_ctx *c, cudaStream_t s, const oco_params *p) {
   CU(cudaStreamSynchronize(s));
   if (st[2])
     return oco_set_err(c, OCO_ETIMEDOUT, "a bounded wait for a pillar copy ran out; results are incomplete");
+  const bool mixed = c->status_dims_mixed;
+  c->status_dims_mixed = false;
+  if (st[0] && mixed)
+    return oco_set_err(c, OCO_EZEROPIVOT,
+                       "ERROR tridiag: bet == 0 in %llu (column, wavelength) items of pending calls with different "
+                       "block dimensions; the first item's location is not known",
+                       st[0]);
   if (st[0]) {
     unsigned long long item = st[1];
     long long col = (long long)(item / (unsigned long long)p->nw), iw = (long long)(item % p->nw);
@@ -582,9 +608,14 @@ extern "C" int oco_solve_block_device(oco_ctx *c, const oco_params *p, const dou
     const int64_t nb = std::min(ch, ncol - c0);
     if ((rc = device_chunk(c, p, rho, T, c0, nb, U, kappa, V, Vtop, Vbot, s))) return rc;
   }
+  if (!c->status_pending) {
+    c->status_params = *p;
+    c->status_dims_mixed = false;
+  } else if (c->status_params.nx != p->nx || c->status_params.ny != p->ny || c->status_params.nw != p->nw) {
+    c->status_dims_mixed = true;
+  }
   c->status_pending = true;
   c->status_stream = s;
-  c->status_params = *p;
   return OCO_OK;
 }
 

@@ -52,7 +52,7 @@ struct oco_batch {
      Vtop and Vbot), {-1, -1} if none: binding an array of an overlapping family fails */
   int64_t overlap[3][2] = {{-1, -1}, {-1, -1}, {-1, -1}};
   DevBuf cols, rec_pre, tasks, order, item_pre, lam, rec, scratch, work, status;
-  DevBuf lam64, scratch64, colflag, rlist; /* mixed form: FP64 tables, scratch, column marks and flagged list of the re-solve */
+  DevBuf lam64, colflag, rbits, rslot, rlist, ilist; /* mixed form: FP64 tables, column marks, flag words, slots, listed words and items of the re-solve */
   int64_t slots = 0; /* scratch slots (threads of the largest persistent grid) */
   int tiling = OCO_TILING_WARP_COLUMN, bps = 1, max_bps[2] = {1, 1}; /* max_bps 0: tiling not available */
   /* bound arrays */
@@ -92,8 +92,13 @@ static MixedBatchArgs batch_args(const oco_batch *b) {
   a.status = b->status.as<unsigned long long>();
   a.repair_cond = b->c->repair_cond;
   a.colflag = b->colflag.as<unsigned>();
+  a.rbits = b->rbits.as<unsigned>();
+  a.rslot = b->rslot.as<int>();
+  a.rwstride = (b->max_nw + 31) / 32;
   a.rlist = b->rlist.as<unsigned long long>();
   a.rcount = b->status.as<unsigned long long>() + 4;
+  a.ilist = b->ilist.as<unsigned long long>();
+  a.icount = b->status.as<unsigned long long>() + 5;
   return a;
 }
 
@@ -102,6 +107,11 @@ static RepairArgs repair_args(const oco_batch *b) {
   RepairArgs r{};
   r.list = b->rlist.as<unsigned long long>();
   r.count = b->status.as<unsigned long long>() + 4;
+  r.ilist = b->ilist.as<unsigned long long>();
+  r.icount = b->status.as<unsigned long long>() + 5;
+  r.bits = b->rbits.as<unsigned>();
+  r.slot = b->rslot.as<int>();
+  r.wstride = (b->max_nw + 31) / 32;
   r.block = 0;
   r.rho = b->rho;
   r.T = b->T;
@@ -110,8 +120,9 @@ static RepairArgs repair_args(const oco_batch *b) {
   r.cols = b->cols.as<MBatchCol>();
   r.lam64 = b->lam64.as<double>();
   r.fully_ionized_T = b->fully_ionized_T;
-  r.scratch = b->scratch64.as<double>();
+  r.scratch = b->scratch.as<double>(); /* the mixed solve's */
   r.max_nz = b->max_nz;
+  r.cap = repair_capacity(b->scratch.n, b->max_nz, REPAIR_SOLVE_BLOCKS_PER_SM * b->c->num_sms);
   r.repairs = b->c->stats.as<unsigned long long>();
   r.status = b->status.as<unsigned long long>();
   return r;
@@ -155,10 +166,11 @@ static int enqueue_run(oco_batch *b, cudaStream_t s) {
     CU(launch_pillars_mixed_batch(b->rho, b->T, b->cols.as<MBatchCol>(), b->rec_pre.as<int64_t>(), b->ncol, b->nrec,
                                   b->fully_ionized_T, b->rec.as<float>(), b->colflag.as<unsigned>(), s));
     const MixedBatchArgs a = batch_args(b);
-    CU(cudaMemsetAsync(a.rcount, 0, sizeof(unsigned long long), s));
+    CU(cudaMemsetAsync(a.rcount, 0, 2 * sizeof(unsigned long long), s)); /* rcount, icount */
+    CU(cudaMemsetAsync(a.rbits, 0, (size_t)b->ncol * a.rwstride * sizeof(unsigned), s));
     CU(launch_batch_mixed(a, b->tiling == OCO_TILING_PACKED ? BATCH_TILING_PACKED : BATCH_TILING_WARP_COLUMN, blocks,
                           kBatchThreads, s));
-    CU(launch_repair(repair_args(b), c->num_sms, s));
+    CU(launch_repair(repair_args(b), REPAIR_COEF_BLOCKS_PER_SM * c->num_sms, REPAIR_SOLVE_BLOCKS_PER_SM * c->num_sms, s));
   } else {
     CU(launch_pillars_batch(b->rho, b->T, b->cols.as<MBatchCol>(), b->rec_pre.as<int64_t>(), b->ncol, b->nrec,
                             b->fully_ionized_T, b->rec.as<double>(), s));
@@ -346,11 +358,17 @@ static int batch_create(oco_ctx *c, const oco_batch_column *cols, int64_t ncol, 
   } else {
     CU(b->lam.ensure(lam.size() * sizeof(float)));
     CU(b->rec.ensure((size_t)b->nrec * MIXED_ZN * sizeof(float)));
-    CU(b->scratch.ensure((size_t)b->slots * b->max_nz * sizeof(float4)));
+    CU(b->scratch.ensure(std::max((size_t)b->slots * sizeof(float4),
+                                  ((size_t)REPAIR_SOLVE_BLOCKS_PER_SM * c->num_sms * (REPAIR_THREADS / 32) * 4 + 32 * 5) *
+                                      sizeof(double)) *
+                         b->max_nz)); /* the re-solve takes it over after the mixed solve */
     CU(b->lam64.ensure(lam64.size() * sizeof(double)));
-    CU(b->scratch64.ensure((size_t)c->num_sms * REPAIR_WARPS_PER_SM * 11 * b->max_nz * sizeof(double)));
     CU(b->colflag.ensure((size_t)ncol * sizeof(unsigned)));
-    CU(b->rlist.ensure((size_t)b->nitems * sizeof(unsigned long long)));
+    const size_t words = (size_t)ncol * ((b->max_nw + 31) / 32);
+    CU(b->rbits.ensure(words * sizeof(unsigned)));
+    CU(b->rlist.ensure(words * sizeof(unsigned long long)));
+    CU(b->ilist.ensure((size_t)b->nitems * sizeof(unsigned long long)));
+    CU(b->rslot.ensure(words * 32 * sizeof(int)));
   }
   CU(b->work.ensure(64));
   CU(b->status.ensure(64));
@@ -513,7 +531,7 @@ extern "C" int oco_batch_run(oco_batch *b, void *stream) {
   b->last = s;
   b->pending = true;
   b->info.graph_launches++;
-  c->launches += 2;
+  c->launches += b->form == OCO_FORM_MIXED ? 4 : 2; /* records, solve (+ the re-solve's two kernels) */
   return OCO_OK;
 }
 
@@ -541,7 +559,7 @@ extern "C" void oco_batch_destroy(oco_batch *b) {
   if (b->pending) cudaStreamSynchronize(b->last); /* a null stream is the default stream */
   if (b->cap) cudaStreamSynchronize(b->cap);
   drop_graph(b);
-  for (DevBuf *d : {&b->lam64, &b->scratch64, &b->colflag, &b->rlist, &b->cols, &b->rec_pre, &b->tasks, &b->order, &b->item_pre, &b->lam, &b->rec, &b->scratch,
+  for (DevBuf *d : {&b->lam64, &b->colflag, &b->rbits, &b->rslot, &b->rlist, &b->ilist, &b->cols, &b->rec_pre, &b->tasks, &b->order, &b->item_pre, &b->lam, &b->rec, &b->scratch,
                     &b->work, &b->status})
     d->release();
   if (b->after_last) cudaEventDestroy(b->after_last);

@@ -57,10 +57,10 @@ struct oco_ctx {
   DevBuf trapw; /* trapezoid weights of the wavelength grid, cm (oco_integrated_flux_device) */
   /* workspace */
   DevBuf pil, scratch, work, status;
-  /* mixed form: the list of flagged items of a chunk, the FP64 re-solve's scratch, column marks
-   * and counters ([0] items re-solved since the last oco_mixed_repairs, [1] items flagged in the
-   * current chunk) */
-  DevBuf scratch64, stats, colflag, rlist;
+  /* mixed form: a chunk's flag words (one bit per item) with each flagged item's slot beside its
+   * bit, the lists of words holding flags and of flagged items, column marks, and counters ([0] items re-solved since the last
+   * oco_mixed_repairs, [1] words and [2] items listed in the current chunk) */
+  DevBuf rbits, rslot, stats, colflag, rlist, ilist;
   float repair_cond = 100.0f; /* oco_set_mixed_repair */
   Stage stage[2];
   int64_t launches = 0;
@@ -75,7 +75,8 @@ struct oco_ctx {
   /* device-array calls defer the zero-pivot check to oco_synchronize */
   bool status_pending = false;
   cudaStream_t status_stream = nullptr;
-  oco_params status_params{};
+  oco_params status_params{};  /* the first pending call's, which locate the first bad item */
+  bool status_dims_mixed = false; /* pending calls of different nx, ny or nw: no location */
   cudaEvent_t order_ev = nullptr; /* orders a device call on another stream after the pending one */
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_solve, ev_pil;

@@ -123,11 +123,15 @@ struct MixedArgs {
   int64_t slot_stride; /* resident threads the scratch is sized for */
   unsigned long long *work;
   unsigned long long *status;
-  /* Items whose emergent flux the FP32 arithmetic cannot resolve are appended to rlist
-   * (chunk-local id cl*nw + iw; *rcount of them) for the FP64 re-solve (RepairArgs). */
+  /* Items whose emergent flux the FP32 arithmetic cannot resolve are appended to ilist
+   * (chunk-local id cl*nw + iw; *icount of them) and set their bit in
+   * rbits[cl * ceil(nw/32) + iw/32] (cleared by the caller); each word that receives a bit is
+   * appended once to rlist (*rcount of them).  Both lists feed the FP64 re-solve (RepairArgs). */
   float repair_cond;           /* flag when the boundary-flux condition number exceeds this */
   const unsigned *colflag;     /* [ncol] columns flagged entirely (record kernel) */
-  unsigned long long *rlist, *rcount;
+  unsigned *rbits;
+  int *rslot;              /* [word * 32 + bit]: the flagged item's index in ilist */
+  unsigned long long *rlist, *rcount, *ilist, *icount;
 };
 
 /* One column of a ragged batch as the batch kernels see it (built from oco_batch_column). */
@@ -161,20 +165,28 @@ struct MixedBatchArgs {
   int max_nz;
   unsigned long long *work;
   unsigned long long *status;
-  /* flagged items as in MixedArgs; id (column << 32) | wavelength */
+  /* flagged items as in MixedArgs: item id (column << 32) | wavelength, word
+   * rbits[col * rwstride + iw/32] */
   float repair_cond;
   const unsigned *colflag; /* [ncol] columns flagged entirely */
-  unsigned long long *rlist, *rcount;
+  unsigned *rbits;
+  int *rslot;              /* [word * 32 + bit]: the flagged item's index in ilist */
+  int rwstride;            /* ceil(max nw / 32) */
+  unsigned long long *rlist, *rcount, *ilist, *icount;
 };
 
 /* The FP64 re-solve (stable form) of the items the mixed kernels flagged (kernels_repair.cu):
- * one warp per item, the records, opacities and row coefficients computed by the 32 lanes, the
- * elimination and back-substitution by one lane, results stored over the mixed ones.  The
- * arithmetic is solve_item's, operation for operation, so a re-solved item equals the stable
- * FP64 form bit for bit.  block != 0: items of a block chunk (the outputs as in SolveArgs);
- * otherwise items of a ragged batch (the outputs as in FP64BatchArgs). */
+ * k_repair_coef computes the items' row coefficients in parallel over (listed word, chunk of
+ * levels) into one slot per item, k_repair_solve runs each item's recurrences, one lane per
+ * slot; a re-solved item equals the stable FP64 form bit for bit and is stored over the mixed
+ * one.  block != 0: items of a block chunk (the outputs as in SolveArgs); otherwise items of a
+ * ragged batch (the outputs as in FP64BatchArgs). */
 struct RepairArgs {
-  const unsigned long long *list, *count;
+  const unsigned long long *list, *count;   /* listed words: index col * wstride + word into bits */
+  const unsigned long long *ilist, *icount; /* listed items (ids as in MixedArgs / MixedBatchArgs); index = slot */
+  const unsigned *bits;
+  const int *slot;                          /* [word * 32 + bit]: the item's index in ilist */
+  int64_t wstride;
   int block;
   /* block chunk */
   const double *rho, *T; /* the chunk's inputs [ncol][nz] */
@@ -188,13 +200,20 @@ struct RepairArgs {
   /* both */
   const double *lam64;     /* [NL][nw] (block) or packed tables (batch) */
   double fully_ionized_T;
-  double *scratch;         /* per warp 11 arrays of max_nz doubles */
+  double *scratch;         /* the mixed solve's scratch: cap slots x 5 x max_nz doubles, then per
+                              k_repair_solve warp 4 x max_nz doubles (repair_capacity) */
+  int64_t cap;             /* slots: items beyond are re-solved one warp per item */
   int max_nz;
-  unsigned long long *repairs; /* += *count */
+  unsigned long long *repairs; /* += the re-solved items */
   unsigned long long *status;  /* zero-pivot words as in SolveArgs */
 };
-constexpr int REPAIR_WARPS_PER_SM = 16; /* persistent grid of the re-solve: 4 blocks of 128 threads per SM */
-cudaError_t launch_repair(const RepairArgs &a, int num_sms, cudaStream_t s);
+/* Threads per block of k_repair_solve. */
+constexpr int REPAIR_THREADS = 64;
+constexpr int REPAIR_SOLVE_BLOCKS_PER_SM = 6;
+constexpr int REPAIR_COEF_BLOCKS_PER_SM = 4;
+/* Slots that a scratch of scratch_bytes holds beside k_repair_solve's per-warp arrays. */
+int64_t repair_capacity(size_t scratch_bytes, int max_nz, int solve_blocks);
+cudaError_t launch_repair(const RepairArgs &a, int coef_blocks, int solve_blocks, cudaStream_t s);
 
 /* Arguments of the ragged-batch kernels (plain and stable FP64 forms; warp-column tiling). */
 struct FP64BatchArgs {
