@@ -355,16 +355,16 @@ __device__ __forceinline__ void solve_reverse(const IT &it, double u, const doub
         }
 #pragma unroll
         for (int q = 0; q < 8; q++) stepDo(k - q, ub[q], qb[q], gb[q], ob[q]);
-        continue;
-      }
+      } else {
 #pragma unroll
-      for (int q = 0; q < 8; q++) {
-        ub[q] = uu[(k - q) * ss];
-        qb[q] = qs[(k - q) * ss];
-        gb[q] = gam[(k - q + 1) * ss];
-      }
+        for (int q = 0; q < 8; q++) {
+          ub[q] = uu[(k - q) * ss];
+          qb[q] = qs[(k - q) * ss];
+          gb[q] = gam[(k - q + 1) * ss];
+        }
 #pragma unroll
-      for (int q = 0; q < 8; q++) stepD(k - q, ub[q], qb[q], gb[q]);
+        for (int q = 0; q < 8; q++) stepD(k - q, ub[q], qb[q], gb[q]);
+      }
     }
     for (; k >= 0; k--) stepD(k, uu[k * ss], qs[k * ss], gam[(k + 1) * ss]);
     if (Ub) __stcs(&Ub[2 * uz], 2.0 * U0 - U1);

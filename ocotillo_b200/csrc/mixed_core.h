@@ -168,6 +168,13 @@ MX_HD void put_l2(double v, float *o) {
   o[1] = (float)i;
 }
 
+/* FP64 logarithm and exponential of the record's wavelength-independent factors, which the
+ * record keeps in FP32: the math library's (an ulp or so), where the FP64 forms need ocomath's
+ * correctly rounded ones for bit-parity with the oracle.  Saha's root keeps ocomath's, so that
+ * the negative-neutral-fraction test below sees the FP64 forms' value. */
+MX_HD double dlog(double v) { return log(v); }
+MX_HD double dexp(double v) { return exp(v); }
+
 /* ---- per-(column, z) record (gas_state.f90:30-110, c_o :143-163) ------------------------ */
 /* Returns true when the cell's neutral hydrogen density is negative.  The reference's Saha root
  * 0.5*(sqrt(C^2 + 4C) - C) (gas_state.f90:63) cancels for large C and can round above 1 below
@@ -186,45 +193,50 @@ MX_HD bool pillar(double r, double t, double fully_ionized_T, float *o) {
   double Pe = (ne * k_cgs) * t;
   double escat = (alpha_e * nHII) * (rho1 * mp);
   double theta = 5040.0 * T1, theta1 = 1.0 / theta;
-  double lgt = oco_log10(theta);
+  double lgt = log10(theta);
   double ktemp1 = k1_cgs * T1;
   double chi[7];
   for (int n = 1; n <= 6; n++) {
     double n1 = 1.0 / (double)n;
     chi[n] = RydbergEnergy * (1.0 - n1 * n1);
   }
-  const double lionf = ionf > 0.0 ? oco_log(ionf) * kLog2e : (double)kNeg;
+  const double lionf = ionf > 0.0 ? dlog(ionf) * kLog2e : (double)kNeg;
   o[MZ_TH] = (float)(theta);
+  /* E_n/E_n0 = exp(-(chi_n - chi_n0)/kT) as e_n / e_n0 with e_n = exp(-chi_n/kT) (chi_1 = 0; e_6 >= 5e-34
+   * at the 2000 K floor) */
+  double e[7];
+  e[1] = 1.0;
+  for (int n = 2; n <= 6; n++) e[n] = dexp(-(chi[n] * ktemp1));
   for (int n0 = 1; n0 <= 6; n0++) {
     o[MZ_R + rrow(n0)] = 1.0f;
-    for (int n = n0 + 1; n <= 6; n++) o[MZ_R + rrow(n0) + (n - n0)] = oco_exp(-((chi[n] - chi[n0]) * ktemp1));
+    for (int n = n0 + 1; n <= 6; n++) o[MZ_R + rrow(n0) + (n - n0)] = (float)(e[n] / e[n0]);
   }
   for (int k2 = MZ_R + 21; k2 < MZ_END; k2++) o[k2] = 0.0f;
   /* Unsold: 0.5 kT/Ry (exp(-chi_6/kT) - exp(-Ry/kT)) = 0.5 kT/Ry e^{-chi_6/kT} (1 - e^{-(Ry-chi_6)/kT}) */
-  double lu = oco_log((0.5 * (k_cgs * t)) * RydbergEnergy1) - chi[6] * ktemp1 +
-              oco_log(1.0 - oco_exp(-((RydbergEnergy - chi[6]) * ktemp1)));
+  double lu = dlog((0.5 * (k_cgs * t)) * RydbergEnergy1) - chi[6] * ktemp1 +
+              dlog(1.0 - dexp(-((RydbergEnergy - chi[6]) * ktemp1)));
   put_l2(ionf > 0.0 ? lionf + lu * kLog2e : (double)kNeg, o + MZ_PU);
   for (int n = 1; n <= 6; n++)
     put_l2(ionf > 0.0 ? lionf - (chi[n] * ktemp1) * kLog2e : (double)kNeg, o + MZ_PE + 2 * (n - 1));
   /* hm_bf_factor = 4.158e-10 Pe theta^2.5 10^(0.754 theta), in logs */
   double lhm = (Pe > 0.0 && ionf > 0.0)
-                   ? (oco_log(4.158e-10 * Pe) + 2.5 * oco_log(theta)) * kLog2e + 0.754 * theta * kLog2_10 + lionf
+                   ? (dlog(4.158e-10 * Pe) + 2.5 * dlog(theta)) * kLog2e + 0.754 * theta * kLog2_10 + lionf
                    : (double)kNeg;
   put_l2(lhm, o + MZ_LHM);
   const double aff = ((ionf * ne) * k_cgs) * t;
-  put_l2(aff > 0.0 ? oco_log(aff) * kLog2e : (double)kNeg, o + MZ_LAFF);
-  put_l2(escat > 0.0 ? oco_log(escat) * kLog2e : (double)kNeg, o + MZ_LESC);
+  put_l2(aff > 0.0 ? dlog(aff) * kLog2e : (double)kNeg, o + MZ_LAFF);
+  put_l2(escat > 0.0 ? dlog(escat) * kLog2e : (double)kNeg, o + MZ_LESC);
   /* energyfactor = 0.5 log10e theta1 / Iev * 10^(-theta Iev) */
-  double lef = oco_log(((0.5 * log10e) * theta1) * Iev1) * kLog2e - theta * Iev * kLog2_10;
+  double lef = dlog(((0.5 * log10e) * theta1) * Iev1) * kLog2e - theta * Iev * kLog2_10;
   put_l2(ionf > 0.0 ? lef + lionf : (double)kNeg, o + MZ_LIONFEF);
-  put_l2(oco_log(r) * kLog2e, o + MZ_LRHO);
+  put_l2(dlog(r) * kLog2e, o + MZ_LRHO);
   double nprod = ne * (nHI + nHII);
-  put_l2(nprod > 0.0 ? (oco_log(nprod) - 0.5 * oco_log(t)) * kLog2e : (double)kNeg, o + MZ_LZ2);
+  put_l2(nprod > 0.0 ? (dlog(nprod) - 0.5 * dlog(t)) * kLog2e : (double)kNeg, o + MZ_LZ2);
   o[MZ_LGT] = (float)(lgt);
   o[MZ_LGT2] = (float)((lgt * lgt));
   o[MZ_NEUTRAL] = (float)(((1.0 - x) > switch_ionfraction) ? 1.0 : 0.0);
   o[MZ_TH1L] = (float)((theta1 * log10e));
-  o[MZ_LNTPOW] = (float)((-1.5 * oco_log(t * 1e-4)));
+  o[MZ_LNTPOW] = (float)((-1.5 * dlog(t * 1e-4)));
   o[MZ_T1] = (float)(T1);
   split2(damping_factor_const * T1, o[MZ_DFT1], o[MZ_DFT1L]);
   for (int k2 = MZ_END; k2 < MZN; k2++) o[k2] = 0.0f;
