@@ -562,11 +562,14 @@ def measure_precision_c3(a, eng, dev):
     return res
 
 
-def run_stream(eng, dev, form, specs, arrays, pinned):
-    """Runs one job stream through a fresh server: each job is submitted at its arrival time,
-    and every finished job is fetched at once (emergent-flux planes into pinned host memory).
-    Per job: device latency (submit -> results complete on the device, server clock), fetch
-    latency (submit -> planes in host memory) and admission wait (submit -> admitted)."""
+def run_stream(eng, dev, form, specs, make, pinned, window=None):
+    """Runs one job stream through a fresh server.  Each job's inputs are generated on the device
+    (make(k)) when it arrives and released once the server has consumed them, so only queued jobs
+    hold input memory.  Open loop (window None): job k arrives at its arrival_s.  Closed loop
+    (window w): a job arrives whenever fewer than w are outstanding, which keeps the server
+    saturated.  Every finished job is fetched at once (emergent-flux planes into pinned host
+    memory).  Per job: device latency (submit -> results complete on the device, server clock),
+    fetch latency (submit -> planes in host memory) and admission wait (submit -> admitted)."""
     import torch
     from ocotillo_b200 import Server, workloads
     srv = Server(dev.index or 0, max_jobs=4, max_nz=1024, reserve_bytes=24e9)
@@ -574,21 +577,26 @@ def run_stream(eng, dev, form, specs, arrays, pinned):
     jid = srv.submit(wr, wt, workloads.log_wavelengths(64), 1e16 / 127, form=form)  # warm-up
     srv.wait(jid)
     srv.fetch(jid)
+    del wr, wt
     torch.cuda.synchronize(dev)
-    ids, jobs = {}, []
+    ids = {}
     pending = list(range(len(specs)))
     outstanding = set()
+    live = {}  # inputs of submitted jobs the server has not consumed yet
     done = {}
     t0 = time.monotonic()
     while pending or outstanding:
         now = time.monotonic()
-        while pending and t0 + specs[pending[0]]["arrival_s"] <= now:
+        while pending and (len(outstanding) < window if window else t0 + specs[pending[0]]["arrival_s"] <= now):
             k = pending.pop(0)
-            rho, T, dz = arrays[k]
+            rho, T, dz = make(k)
             ids[k] = srv.submit(rho, T, workloads.log_wavelengths(specs[k]["nw"]), dz, form=form)
+            live[k] = (rho, T)
             outstanding.add(k)
         for k in list(outstanding):
             st = srv.status(ids[k])
+            if k in live and (st["inputs_consumed"] or st["state"] in ("done", "failed")):
+                del live[k]
             if st["state"] == "done":
                 sp = specs[k]
                 n = sp["nw"] * sp["nx"] * sp["ny"]
@@ -598,7 +606,7 @@ def run_stream(eng, dev, form, specs, arrays, pinned):
                 outstanding.discard(k)
             elif st["state"] == "failed":
                 raise RuntimeError(f"serving job {k} failed: {st['error']}")
-        if pending and not outstanding:
+        if pending and not outstanding and not window:
             time.sleep(max(0.0, min(0.002, t0 + specs[pending[0]]["arrival_s"] - time.monotonic())))
         else:
             time.sleep(0.0005)
@@ -625,16 +633,15 @@ def run_stream(eng, dev, form, specs, arrays, pinned):
 
 def measure_serving_sweep(a, eng, dev):
     """Config 'serving form': the Poisson job stream (seed 5) at rising arrival rates.  The
-    saturation rate comes from the same jobs all submitted at once (jobs / makespan); the mixed
-    form then runs at 0.3, 0.5, 0.7 and 0.9 of its saturation rate and the plain FP64 form at half
-    of its own.  Job inputs are generated on the device once and reused by every run (the same
-    seed gives the same jobs at every rate; only the arrival times scale)."""
+    saturation rate comes from the same jobs run in a closed loop that keeps 8 jobs outstanding
+    (jobs / makespan); the mixed form then runs at 0.3, 0.5, 0.7 and 0.9 of its saturation rate and
+    the plain FP64 form at half of its own.  Each job's inputs are generated on the device when it
+    arrives (the same seed gives the same jobs at every rate; only the arrival times scale)."""
     import torch
     from ocotillo_b200 import workloads
     n = a.serve_jobs
     base = workloads.serving_stream(n, 1.0, seed=5)
-    arrays = [workloads.job_arrays_device(sp, eng) for sp in base]
-    torch.cuda.synchronize(dev)
+    make = lambda k: workloads.job_arrays_device(base[k], eng)  # the same inputs at every rate
     maxn = max(sp["nw"] * sp["nx"] * sp["ny"] for sp in base)
     pinned = [torch.empty(maxn, dtype=torch.float64, pin_memory=True).numpy() for _ in range(2)]
     points = int(sum(sp["nx"] * sp["ny"] * sp["nz"] * sp["nw"] for sp in base))
@@ -644,16 +651,14 @@ def measure_serving_sweep(a, eng, dev):
            "latency": "p50/p99_ms: submit to results complete on the device; fetch_*: submit to planes in host memory"}
     fracs = {"mixed": (0.3, 0.5, 0.7, 0.9), "plain": (0.5,)}
     for form in ("mixed", "plain"):
-        sat_specs = [dict(sp, arrival_s=0.0) for sp in base]
-        sat = run_stream(eng, dev, form, sat_specs, arrays, pinned)
+        sat = run_stream(eng, dev, form, base, make, pinned, window=8)
         sat_rate = n / sat["makespan_s"]
-        runs = {"saturation": dict(sat, rate_jobs_per_s=sat_rate)}
+        runs = {"saturation": dict(sat, rate_jobs_per_s=sat_rate, loop="closed, 8 jobs outstanding")}
         for f in fracs[form]:
             specs = [dict(sp, arrival_s=sp["arrival_s"] / (f * sat_rate)) for sp in base]
-            runs[f"{f:g}x_saturation"] = dict(run_stream(eng, dev, form, specs, arrays, pinned),
+            runs[f"{f:g}x_saturation"] = dict(run_stream(eng, dev, form, specs, make, pinned),
                                               rate_jobs_per_s=f * sat_rate)
         res[form] = runs
-    del arrays
     torch.cuda.empty_cache()
     mx = res["mixed"]
     res["headline"] = {"serving_saturation_jobs_per_s": mx["saturation"]["rate_jobs_per_s"],
