@@ -80,6 +80,7 @@ extern "C" int oco_create(oco_ctx **out, int device) {
     double gb = atof(g);
     if (gb > 0.0) c->budget_bytes = std::max<size_t>((size_t)(gb * (1ull << 30)), 1);
   }
+  if (const char *r = getenv("OCO_REPAIR_SLOTS")) c->repair_slots_max = std::max<int64_t>(0, atoll(r));
   *out = c;
   return OCO_OK;
 }
@@ -342,6 +343,11 @@ static int64_t chunk_columns(oco_ctx *c, const oco_params *p, bool host_path, bo
   return std::min(ch, ncol);
 }
 
+int64_t oco_ctx_repair_slots(const oco_ctx *c, int64_t cap) {
+  if (c->repair_slots_max >= 0 && c->repair_slots_max < cap) cap = c->repair_slots_max & ~(int64_t)31;
+  return cap;
+}
+
 /* One chunk: pillars + persistent solve. Outputs described by the strides in a. */
 static int run_chunk_mixed(oco_ctx *c, const oco_params *p, const double *rho, const double *T, int64_t nb,
                            const SolveArgs &a64, cudaStream_t s) {
@@ -427,7 +433,7 @@ static int run_chunk_mixed(oco_ctx *c, const oco_params *p, const double *rho, c
   r.fully_ionized_T = p->fully_ionized_T;
   r.scratch = c->scratch.as<double>(); /* the mixed solve's */
   r.max_nz = p->nz;
-  r.cap = repair_capacity(c->scratch.n, p->nz, rsolve_blocks);
+  r.cap = oco_ctx_repair_slots(c, repair_capacity(c->scratch.n, p->nz, rsolve_blocks));
   r.repairs = c->stats.as<unsigned long long>();
   r.status = c->status.as<unsigned long long>();
   if (c->prof) CU(cudaEventRecord(e2, s));

@@ -122,7 +122,7 @@ static RepairArgs repair_args(const oco_batch *b) {
   r.fully_ionized_T = b->fully_ionized_T;
   r.scratch = b->scratch.as<double>(); /* the mixed solve's */
   r.max_nz = b->max_nz;
-  r.cap = repair_capacity(b->scratch.n, b->max_nz, REPAIR_SOLVE_BLOCKS_PER_SM * b->c->num_sms);
+  r.cap = oco_ctx_repair_slots(b->c, repair_capacity(b->scratch.n, b->max_nz, REPAIR_SOLVE_BLOCKS_PER_SM * b->c->num_sms));
   r.repairs = b->c->stats.as<unsigned long long>();
   r.status = b->status.as<unsigned long long>();
   return r;

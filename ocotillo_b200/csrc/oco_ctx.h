@@ -62,6 +62,7 @@ struct oco_ctx {
    * oco_mixed_repairs, [1] words and [2] items listed in the current chunk) */
   DevBuf rbits, rslot, stats, colflag, rlist, ilist;
   float repair_cond = 100.0f; /* oco_set_mixed_repair */
+  int64_t repair_slots_max = -1; /* OCO_REPAIR_SLOTS: caps the re-solve's slots (the rest go one warp per item) */
   Stage stage[2];
   int64_t launches = 0;
   size_t budget_bytes = 8ull << 30; /* chunk budget for pillars + staged outputs */
@@ -107,6 +108,10 @@ int oco_ctx_read_status(oco_ctx *c, cudaStream_t s, const oco_params *p);
 int oco_ctx_check_params(oco_ctx *c, const oco_params *p);
 /* Full device-resident persistent grid of a form (blocks). */
 int oco_ctx_full_blocks(oco_ctx *c, int form, int grey);
+/* The mixed re-solve's slots: a scratch capacity, capped by the context's OCO_REPAIR_SLOTS (the
+ * environment variable read at creation; rounded down to a multiple of 32).  Items beyond the
+ * slots are re-solved one warp per item; the cap lets tests reach that path. */
+int64_t oco_ctx_repair_slots(const oco_ctx *c, int64_t cap);
 
 /* Records a message for oco_last_error (on the context, if any, and the calling thread) and
  * returns code. */

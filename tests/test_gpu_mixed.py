@@ -215,3 +215,87 @@ def test_mixed_repair_in_device_layout_and_batch(engine, oracle, sensitive_block
         vb = out["Vbot"].cpu().numpy().reshape(ncol, nw)
         assert max(_rel(vt, rtop).max(), _rel(vb, rbot).max()) <= TOL_FLUX, tiling
     b.close()
+
+
+def _batch_fluxes(eng, rho, T, dz, wa, tiling):
+    """Emergent fluxes (per column, nw values) of the block's columns as a ragged batch of eng."""
+    import torch
+    nx, ny, nz = rho.shape
+    nw, ncol = len(wa), nx * ny
+    dev = torch.device("cuda:0")
+    b = eng.batch(np.full(ncol, nz), np.full(ncol, nw), np.full(ncol, dz), wa, np.zeros(ncol, dtype=np.int64),
+                  layout=1, form="mixed")
+    out = b.alloc(dev)
+    b.bind(torch.from_numpy(rho.reshape(-1)).to(dev), torch.from_numpy(T.reshape(-1)).to(dev), out)
+    b.set_tiling(tiling)
+    b.run()
+    b.wait()
+    res = {k: out[k].cpu().numpy().copy() for k in ("U", "kappa", "V", "Vtop", "Vbot")}
+    b.close()
+    return res
+
+
+def test_mixed_repair_beyond_the_slots(engine, sensitive_block, monkeypatch):
+    """With the re-solve's slots capped at 32 (OCO_REPAIR_SLOTS, read when a context is created),
+    the flagged items beyond them take the one-warp-per-item path; block and batch results equal
+    those of a context with all its slots (the stable FP64 form for re-solved items) bit for bit."""
+    from ocotillo_b200 import TILING_PACKED, TILING_WARP_COLUMN, Engine
+    rho, T, dz, wa = sensitive_block
+    monkeypatch.setenv("OCO_REPAIR_SLOTS", "32")
+    capped = Engine(0)
+    monkeypatch.delenv("OCO_REPAIR_SLOTS")
+    try:
+        capped.set_wavelengths(wa)
+        capped.set_mixed_repair(100.0)
+        capped.mixed_repairs()
+        a = capped.solve_block(rho, T, dz, form="mixed")
+        n = capped.mixed_repairs()
+        ab = {t: _batch_fluxes(capped, rho, T, dz, wa, t) for t in (TILING_WARP_COLUMN, TILING_PACKED)}
+    finally:
+        capped.close()
+    assert n > 1000, n  # most of the flagged items go beyond the 32 slots
+    engine.set_wavelengths(wa)
+    engine.set_mixed_repair(100.0)
+    b = engine.solve_block(rho, T, dz, form="mixed")
+    for key in ("U", "kappa", "V", "Vtop", "Vbot"):
+        assert np.array_equal(a[key].view(np.uint64), b[key].view(np.uint64)), key
+    for t in (TILING_WARP_COLUMN, TILING_PACKED):
+        bb = _batch_fluxes(engine, rho, T, dz, wa, t)
+        for key in ("U", "kappa", "V", "Vtop", "Vbot"):
+            assert np.array_equal(ab[t][key].view(np.uint64), bb[key].view(np.uint64)), (t, key)
+
+
+# Columns of the batching config's construction (workloads.ragged_batch(8192, seed=4)) holding a
+# cell where the reference's Saha root 0.5 (sqrt(C^2 + 4C) - C) rounds above 1 in a numpy
+# evaluation (C ~ 4e8 .. 7e9 at T ~ 13,000-19,000 K): the neutral fraction is then negative, and
+# the reference's opacity terms proportional to it turn negative.
+NEGATIVE_NEUTRAL_COLUMNS = [194, 4198, 4795, 5044, 6758, 8159]
+
+
+def test_mixed_negative_neutral_fraction_columns(engine, oracle):
+    """Log-space opacities cannot carry a negative term, so the record kernel flags a column with
+    such a cell whole: with the condition-number threshold off, its items are re-solved in FP64
+    all or none per column (the GPU's Saha decides which columns, within an ulp of numpy's), at
+    least one column is; with the default threshold every emergent flux meets 1e-4."""
+    from ocotillo_b200 import workloads
+    d = workloads.ragged_batch(ncol=8192, seed=4)
+    off = np.concatenate([[0], np.cumsum(d["nz"])])
+    whole = 0
+    for c in NEGATIVE_NEUTRAL_COLUMNS:
+        nz, nw, dz = int(d["nz"][c]), int(d["nw"][c]), float(d["dz"][c])
+        rho = np.ascontiguousarray(d["rho"][off[c]:off[c] + nz].reshape(1, 1, nz))
+        T = np.ascontiguousarray(d["T"][off[c]:off[c] + nz].reshape(1, 1, nz))
+        wa = workloads.log_wavelengths(nw)
+        engine.set_wavelengths(wa)
+        engine.set_mixed_repair(float("inf"))
+        engine.mixed_repairs()
+        engine.solve_block(rho, T, dz, form="mixed", want=("Vtop", "Vbot"))
+        n = engine.mixed_repairs()
+        assert n in (0, nw), (c, n, nw)
+        whole += n == nw
+        engine.set_mixed_repair(100.0)
+        out = engine.solve_block(rho, T, dz, form="mixed", want=("Vtop", "Vbot"))
+        ref = oracle.solve_block(rho, T, wa, dz, form=oracle.FORM_STABLE, backend="ocomath", want=("V",))
+        err = max(_rel(out["Vtop"], ref["V"][..., -1]).max(), _rel(out["Vbot"], ref["V"][..., 0]).max())
+        assert err <= TOL_FLUX, (c, err)
+    assert whole >= 1
