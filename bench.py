@@ -520,6 +520,41 @@ def measure_batch(a, eng, dev):
     plain, _ = _time_batch(a, eng, dev, d, "plain")
     res["plain"] = plain
     res["ratio_mixed_vs_plain"] = res["value"] / plain["value"]
+    res["emergent_flux_rel_err"] = batch_flux_error(eng, dev, d)
+    return res
+
+
+def batch_flux_error(eng, dev, d):
+    """The mixed batch's emergent fluxes against the stable FP64 batch's, every item of the batch
+    (both runs store only Vtop and Vbot), with the re-solve at its current threshold."""
+    import torch
+    from ocotillo_b200 import OcoError
+    fl, rep = {}, 0
+    for form in ("stable", "mixed"):
+        b = eng.batch(d["nz"], d["nw"], d["dz"], d["waves"], d["wave_off"], layout=1, form=form)
+        rho = torch.from_numpy(d["rho"]).to(dev)
+        T = torch.from_numpy(d["T"]).to(dev)
+        out = b.bind(rho, T, b.alloc(dev, want=("Vtop", "Vbot")))
+        eng.mixed_repairs()
+        b.run()
+        try:
+            b.wait()
+        except OcoError as e:
+            if e.code != -3:
+                raise
+        rep = eng.mixed_repairs() if form == "mixed" else rep
+        fl[form] = torch.stack([out["Vtop"], out["Vbot"]])
+        b.close()
+        del out, rho, T
+    ra, rb = fl["mixed"], fl["stable"]
+    ok = torch.isfinite(rb) & (rb != 0)
+    rel = ((ra - rb).abs() / rb.abs())[ok].double()
+    items = int(rb[0].numel())
+    res = {"reference_form": "stable", "items": items, "repaired_items": int(rep), "repaired_frac": rep / items,
+           "max": float(rel.max()), "p99": float(torch.quantile(rel[torch.randperm(rel.numel(), device=rel.device)[:1 << 24]].float(), 0.99)),
+           "frac_above_1e-4": float((rel > 1e-4).double().mean()), "sample": "every item of the batch (Vtop and Vbot)"}
+    del fl, ra, rb, rel
+    torch.cuda.empty_cache()
     return res
 
 
@@ -898,6 +933,10 @@ def headline(extra, e2e_mixed, cpu1):
     bt = extra.get("batch")
     if bt:
         h.update({"c4_mixed_value": bt["value"], "c4_mixed_ratio": bt["ratio_mixed_vs_plain"]})
+        if "emergent_flux_rel_err" in bt:
+            e4 = bt["emergent_flux_rel_err"]
+            h.update({"c4_flux_err_max": e4["max"], "c4_flux_frac_above_1e-4": e4["frac_above_1e-4"],
+                      "c4_repaired_frac": e4["repaired_frac"]})
     sv = extra.get("serving")
     if sv and sv.get("headline"):
         h.update(sv["headline"])
