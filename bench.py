@@ -355,7 +355,7 @@ FP64_PEAK_TFLOPS, FP32_PEAK_TFLOPS = 37.0, 75.0  # nominal B200 (no measured FP 
 # kernel, from one ncu --set full capture of a 1024-column launch of this grid (outputs 3.2 GB,
 # larger than L2), scaled to a launch by its points: profiles/k_solve_staged_plain_agn_32x32x512x256.txt
 # and profiles/k_solve_mixed_staged_agn_32x32x512x256.txt.
-TRAFFIC_BYTES_PER_POINT = {"plain": 72.2, "mixed": 56.8}
+TRAFFIC_BYTES_PER_POINT = {"plain": 71.8, "mixed": 56.7}
 
 
 def flux_error(g, form_a, form_b, eps=1e-7, seed=7):
