@@ -184,7 +184,7 @@ def run_reference(a):
             "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_dict(a, a.form),  # the reference loop is the plain form's arithmetic
+            "config": config_dict(a, "plain"),  # the reference loop is the plain form's arithmetic
             "cpu_baseline": {"value": v, "unit": "points/s", "cores": procs, "kind": "port",
                              "sample": f"{cols} columns x nz={a.nz} x nw={a.nw} per step, glibc math, "
                                        f"{procs} processes"},
