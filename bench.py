@@ -234,9 +234,7 @@ class Grid:
         self.wa = workloads.log_wavelengths(nw)
         self.layout = LAYOUT_REFERENCE if a.layout == "reference" else LAYOUT_LAMBDA_FASTEST
         self.CH = min(a.chunk_cols, self.ncol)
-        if self.ncol % self.CH:
-            raise SystemExit(f"--chunk-cols {self.CH} must divide the grid's {self.ncol} columns")
-        self.nchunk = self.ncol // self.CH
+        self.nchunk = -(-self.ncol // self.CH)  # the last chunk may be smaller
         mk = lambda shape: torch.empty(shape, dtype=torch.float64, device=dev)
         CH, mz = self.CH, self.mz
         self.sets = []
@@ -246,16 +244,24 @@ class Grid:
             else:
                 o = {"U": mk((mz, CH, nw)), "kappa": mk((nz, CH, nw)), "V": mk((nz, CH, nw))}
             self.sets.append(o)
-        self.Vtop, self.Vbot = mk((self.nchunk, nw, CH)), mk((self.nchunk, nw, CH))
+        # emergent-flux planes per chunk [nw][columns of the chunk]; slots past a short last chunk
+        # stay NaN, which every comparison leaves out
+        self.Vtop = torch.full((self.nchunk, nw, CH), float("nan"), dtype=torch.float64, device=dev)
+        self.Vbot = torch.full((self.nchunk, nw, CH), float("nan"), dtype=torch.float64, device=dev)
         self.stream = torch.cuda.current_stream(dev)
         self.zero_pivot = False
 
     def step(self, form, fields=True):
         for k in range(self.nchunk):
-            o = dict(self.sets[k % 2]) if fields else {}
-            o["Vtop"], o["Vbot"] = self.Vtop[k], self.Vbot[k]
-            r = self.rho[k * self.CH:(k + 1) * self.CH].reshape(self.CH, 1, self.nz)
-            t = self.T[k * self.CH:(k + 1) * self.CH].reshape(self.CH, 1, self.nz)
+            c0 = k * self.CH
+            n = min(self.CH, self.ncol - c0)
+            # the chunk's arrays: the first n columns' worth of each buffer (columns are dimension
+            # 1 of every one of them), contiguous
+            head = lambda x: x.view(-1)[:x.numel() // self.CH * n].view(x.shape[0], n, *x.shape[2:])
+            o = {key: head(v) for key, v in self.sets[k % 2].items()} if fields else {}
+            o["Vtop"], o["Vbot"] = head(self.Vtop[k]), head(self.Vbot[k])
+            r = self.rho[c0:c0 + n].reshape(n, 1, self.nz)
+            t = self.T[c0:c0 + n].reshape(n, 1, self.nz)
             self.eng.solve_block_device(r, t, self.dz, o, form=form, layout=self.layout, stream=self.stream)
 
     def sync(self):
