@@ -340,6 +340,8 @@ static int64_t chunk_columns(oco_ctx *c, const oco_params *p, bool host_path, bo
     per_col += (size_t)p->nw * ((u ? (size_t)(p->nz + 6) : 0) + (k ? (size_t)p->nz : 0) + (v ? (size_t)p->nz : 0)) *
                sizeof(double);
   int64_t ch = (int64_t)std::max<size_t>(1, c->budget_bytes / per_col);
+  if (p->form == OCO_FORM_MIXED) /* the FP64 re-solve indexes a chunk's flagged items with 32-bit slots */
+    ch = std::min<int64_t>(ch, std::max<int64_t>(1, INT32_MAX / p->nw));
   return std::min(ch, ncol);
 }
 

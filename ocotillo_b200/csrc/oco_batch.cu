@@ -304,6 +304,9 @@ static int batch_create(oco_ctx *c, const oco_batch_column *cols, int64_t ncol, 
     b->need_flux = std::max(b->need_flux, q.flux_off + q.nw);
   }
   b->nrec = rpre[(size_t)ncol];
+  if (!fp64 && b->nitems > INT32_MAX) /* the FP64 re-solve indexes flagged items with 32-bit slots */
+    return oco_set_err(c, OCO_EINVAL, "oco_batch_create: a mixed batch holds at most 2^31-1 (column, wavelength) "
+                       "items (got %lld)", (long long)b->nitems);
   {
     std::vector<int64_t> off((size_t)ncol), len((size_t)ncol);
     for (int f = 0; f < 3; f++) {

@@ -348,3 +348,16 @@ def test_batch_plain_bitwise_oracle(engine, oracle):
     for k, v in out.items():
         assert _same(v, first[k]), k
     b.close()
+
+
+def test_mixed_batch_refuses_more_items_than_32_bit_slots(engine):
+    """The mixed form's FP64 re-solve indexes a batch's flagged items with 32-bit slots, so a
+    mixed batch of 2^31 or more (column, wavelength) items is refused at creation (before any
+    device allocation); the FP64 forms have no such limit."""
+    from ocotillo_b200 import OcoError
+    ncol, nw = (1 << 21) + 1, 1024  # 2^31 + 1024 items
+    wa = np.geomspace(100.0, 1e5, nw)
+    with pytest.raises(OcoError) as e:
+        engine.batch(np.full(ncol, 2), np.full(ncol, nw), np.full(ncol, 1e10), wa, np.zeros(ncol, dtype=np.int64),
+                     layout=1, form="mixed")
+    assert e.value.code == -1 and "2^31-1" in str(e.value)
