@@ -17,6 +17,8 @@
  */
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <cstdint>
 
 #include "oco_internal.h"
@@ -103,27 +105,49 @@ namespace oco {
 
 /* Reference-layout output from a lambda-fastest chunk: for each column col of the chunk, the
  * (rows x nw) plane src[z * src_zs + col * nw + iw] goes to dst[(iw * ld_col + c_off + col) *
- * rows + z].  Tiles of 64 z x 32 wavelengths through shared memory, so that the reads run
- * along lambda and the writes along z (256-byte runs both ways), eight elements per thread in
- * flight.  Block (32, 8); grid (ceil(nw/32), ceil(rows/64), <= 65535) with a loop over
- * columns. */
+ * rows + z].  Tiles of 64 z x 32 wavelengths through shared memory, so that the reads run along
+ * lambda and the writes along z (256-byte runs both ways).  A persistent grid walks the tiles
+ * (lambda tiles fastest, then z tiles, then columns), each block loading its next tile into
+ * registers while it writes the current one out of shared memory, so that every block keeps a
+ * tile's loads in flight throughout.  Block (32, 8). */
 constexpr int TZ = 64; /* z rows per tile */
 __global__ void __launch_bounds__(256) k_lambda_to_reference(const double *__restrict__ src, int64_t src_zs,
                                                              double *__restrict__ dst, int64_t ld_col,
                                                              int64_t c_off, int64_t nb, int rows, int nw) {
   __shared__ double tile[TZ][33];
-  const int w0 = blockIdx.x * 32, z0 = blockIdx.y * TZ;
   const int tx = threadIdx.x, ty = threadIdx.y;
-  for (int64_t col = blockIdx.z; col < nb; col += gridDim.z) {
-    double v[TZ / 8];
+  const int ntw = (nw + 31) / 32, ntz = (rows + TZ - 1) / TZ;
+  const int64_t per_col = (int64_t)ntw * ntz, ntiles = nb * per_col;
+  int64_t t = blockIdx.x;
+  if (t >= ntiles) return;
+  double v[TZ / 8];
+  auto coords = [&](int64_t tt, int64_t &col, int &z0, int &w0) {
+    col = tt / per_col;
+    const int r = (int)(tt - col * per_col);
+    const int zt = r / ntw;
+    z0 = zt * TZ;
+    w0 = (r - zt * ntw) * 32;
+  };
+  auto load = [&](int64_t tt) {
+    int64_t col;
+    int z0, w0;
+    coords(tt, col, z0, w0);
 #pragma unroll
-    for (int i = 0; i < TZ / 8; i++) { /* all loads of the tile first */
+    for (int i = 0; i < TZ / 8; i++) {
       const int z = z0 + ty + 8 * i, iw = w0 + tx;
       v[i] = (z < rows && iw < nw) ? src[(int64_t)z * src_zs + col * nw + iw] : 0.0;
     }
+  };
+  load(t);
+  for (;;) {
+    int64_t col;
+    int z0, w0;
+    coords(t, col, z0, w0);
 #pragma unroll
     for (int i = 0; i < TZ / 8; i++) tile[ty + 8 * i][tx] = v[i];
     __syncthreads();
+    const int64_t tn = t + gridDim.x;
+    if (tn < ntiles) load(tn); /* the next tile's loads in flight during this tile's stores */
 #pragma unroll
     for (int j = 0; j < TZ / 8; j++) {
       const int lw = ty + 8 * (j >> 1), zz = tx + 32 * (j & 1);
@@ -131,14 +155,17 @@ __global__ void __launch_bounds__(256) k_lambda_to_reference(const double *__res
       if (z < rows && iw < nw) dst[((int64_t)iw * ld_col + c_off + col) * rows + z] = tile[zz][lw];
     }
     __syncthreads();
+    if (tn >= ntiles) break;
+    t = tn;
   }
 }
 
 cudaError_t launch_lambda_to_reference(const double *src, int64_t src_zs, double *dst, int64_t ld_col, int64_t c_off,
-                                       int64_t nb, int rows, int nw, cudaStream_t s) {
+                                       int64_t nb, int rows, int nw, int num_sms, cudaStream_t s) {
   if (nb <= 0) return cudaSuccess;
-  const dim3 grid((unsigned)((nw + 31) / 32), (unsigned)((rows + TZ - 1) / TZ), (unsigned)(nb < 65535 ? nb : 65535));
-  k_lambda_to_reference<<<grid, dim3(32, 8), 0, s>>>(src, src_zs, dst, ld_col, c_off, nb, rows, nw);
+  const int64_t ntiles = nb * ((nw + 31) / 32) * (int64_t)((rows + TZ - 1) / TZ);
+  const int64_t blocks = std::min<int64_t>(ntiles, (int64_t)num_sms * 8); /* 8 resident blocks of 256 per SM */
+  k_lambda_to_reference<<<(unsigned)blocks, dim3(32, 8), 0, s>>>(src, src_zs, dst, ld_col, c_off, nb, rows, nw);
   return cudaGetLastError();
 }
 

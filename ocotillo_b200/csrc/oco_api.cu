@@ -585,9 +585,9 @@ static int device_chunk(oco_ctx *c, const oco_params *p, const double *rho, cons
   a.Vbot = Vbot ? Vbot + c0 : nullptr;
   int rc = run_chunk(c, p, rho + c0 * p->nz, T + c0 * p->nz, nb, a, s);
   if (rc) return rc;
-  if (U) CU(launch_lambda_to_reference(c->tmpU.as<double>(), items, U, ncol, c0, nb, mz, nw, s));
-  if (kappa) CU(launch_lambda_to_reference(c->tmpK.as<double>(), items, kappa, ncol, c0, nb, nz, nw, s));
-  if (V) CU(launch_lambda_to_reference(c->tmpV.as<double>(), items, V, ncol, c0, nb, nz, nw, s));
+  if (U) CU(launch_lambda_to_reference(c->tmpU.as<double>(), items, U, ncol, c0, nb, mz, nw, c->num_sms, s));
+  if (kappa) CU(launch_lambda_to_reference(c->tmpK.as<double>(), items, kappa, ncol, c0, nb, nz, nw, c->num_sms, s));
+  if (V) CU(launch_lambda_to_reference(c->tmpV.as<double>(), items, V, ncol, c0, nb, nz, nw, c->num_sms, s));
   c->launches += (U ? 1 : 0) + (kappa ? 1 : 0) + (V ? 1 : 0);
   return OCO_OK;
 }

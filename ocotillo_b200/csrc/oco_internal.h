@@ -265,7 +265,7 @@ cudaError_t launch_integrated_flux(const double *V, const double *w, int64_t nco
 /* Copies a lambda-fastest chunk plane set (src[z * src_zs + col * nw + iw], rows z values)
  * into reference-layout arrays (dst[(iw * ld_col + c_off + col) * rows + z]). */
 cudaError_t launch_lambda_to_reference(const double *src, int64_t src_zs, double *dst, int64_t ld_col, int64_t c_off,
-                                       int64_t nb, int rows, int nw, cudaStream_t s);
+                                       int64_t nb, int rows, int nw, int num_sms, cudaStream_t s);
 
 /* One z-block file of an Athena snapshot in device memory (kernels_inputs.cu): raw = the five
  * fields [5][nzl][nyl][nxl] as stored; the block arrays rho, T are (nxl, nyl, nz), z fastest. */
