@@ -300,10 +300,12 @@ struct BatchItem {
 };
 
 /* Warp-column tiling: tasks (column, 32-wavelength tile) from the device queue, longest
- * columns first; the column's records stream through the warp's shared-memory buffers. */
+ * columns first; the column's records stream through the warp's shared-memory buffers and
+ * the tile's wavelength constants sit in the warp's shared-memory table (as k_solve_staged). */
 template <int FORM>
 __global__ void __launch_bounds__(128, 4) k_batch_fp64_staged(const FP64BatchArgs b) {
   __shared__ __align__(128) double s_pil[WARPS_PER_BLOCK][2 * ZC * NF];
+  __shared__ __align__(16) double s_lam[WARPS_PER_BLOCK][NLF * 32]; /* the task's 32 wavelengths' constants */
   __shared__ __align__(8) unsigned long long s_bar[WARPS_PER_BLOCK][2];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -337,7 +339,10 @@ __global__ void __launch_bounds__(128, 4) k_batch_fp64_staged(const FP64BatchArg
     const int iw = active ? iw_raw : nw - 1;
     pa.nz = __ldg(&c->nz);
     pa.begin(b.pil + __ldg(&c->rec_off) * NF, lane);
-    solve_item<FORM, false>(BatchItem{b, c, (int64_t)t.x, iw}, active, pa, gam, uu, o1, qs);
+    store_lam_shared(&s_lam[wib][lane], b.lam + __ldg(&c->lam_off), iw, nw);
+    __syncwarp();
+    solve_item<FORM, false, BatchItem, StagedPillars, LamS>(BatchItem{b, c, (int64_t)t.x, iw}, active, pa, gam, uu, o1,
+                                                           qs, &s_lam[wib][lane]);
     if (__any_sync(0xffffffffu, pa.failed)) {
       if (lane == 0) atomicOr(&b.status[2], 1ull);
       pa.wait(0);
