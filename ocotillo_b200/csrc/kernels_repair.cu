@@ -279,15 +279,21 @@ constexpr int CWARPS = 4; /* warps per block of k_repair_coef */
 __global__ void __launch_bounds__(CWARPS * 32, 4) k_repair_coef(const RepairArgs a) {
   __shared__ __align__(16) double s_rec[CWARPS][32 * NF];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t n_words = (int64_t)*a.count;
   const int nch = (a.max_nz + CZ - 1) / CZ;
+  const unsigned long long ntasks = (unsigned long long)(n_words * nch);
   const Slots S(a);
   double *rec = &s_rec[wib][lane * NF]; /* each lane reads only its own record */
-  for (int64_t t = warp; t < n_words * nch; t += nwarps) {
-    const int64_t k = t / nch;
-    const int c = (int)(t - k * nch);
+  /* tasks from a device counter, chunk-major (task t: chunk t / n_words of word t % n_words):
+   * a task's cost grows with its word's flagged items, so a fixed assignment would leave some
+   * warps with several times the mean */
+  for (;;) {
+    unsigned long long t = 0;
+    if (lane == 0) t = atomicAdd(a.queue, 1ull);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= ntasks) break;
+    const int c = (int)(t / (unsigned long long)n_words);
+    const int64_t k = (int64_t)(t - (unsigned long long)c * n_words);
     const int64_t w = (int64_t)a.list[k];
     const int64_t col = w / a.wstride;
     const int word = (int)(w - col * a.wstride);

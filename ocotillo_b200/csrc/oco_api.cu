@@ -406,7 +406,7 @@ static int run_chunk_mixed(oco_ctx *c, const oco_params *p, const double *rho, c
   a.rcount = c->stats.as<unsigned long long>() + 1;
   a.ilist = c->ilist.as<unsigned long long>();
   a.icount = c->stats.as<unsigned long long>() + 2;
-  CU(cudaMemsetAsync(a.rcount, 0, 2 * sizeof(unsigned long long), s));
+  CU(cudaMemsetAsync(a.rcount, 0, 3 * sizeof(unsigned long long), s)); /* rcount, icount, the re-solve's queue */
   CU(cudaMemsetAsync(a.rbits, 0, (size_t)nb * nwords * sizeof(unsigned), s));
   CU(cudaMemsetAsync(a.work, 0, sizeof(unsigned long long), s));
   /* the FP64 re-solve of the flagged items (stable form), after the mixed solve */
@@ -436,6 +436,7 @@ static int run_chunk_mixed(oco_ctx *c, const oco_params *p, const double *rho, c
   r.scratch = c->scratch.as<double>(); /* the mixed solve's */
   r.max_nz = p->nz;
   r.cap = oco_ctx_repair_slots(c, repair_capacity(c->scratch.n, p->nz, rsolve_blocks));
+  r.queue = c->stats.as<unsigned long long>() + 3;
   r.repairs = c->stats.as<unsigned long long>();
   r.status = c->status.as<unsigned long long>();
   if (c->prof) CU(cudaEventRecord(e2, s));

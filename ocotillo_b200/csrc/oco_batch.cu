@@ -123,6 +123,7 @@ static RepairArgs repair_args(const oco_batch *b) {
   r.scratch = b->scratch.as<double>(); /* the mixed solve's */
   r.max_nz = b->max_nz;
   r.cap = oco_ctx_repair_slots(b->c, repair_capacity(b->scratch.n, b->max_nz, REPAIR_SOLVE_BLOCKS_PER_SM * b->c->num_sms));
+  r.queue = b->status.as<unsigned long long>() + 6;
   r.repairs = b->c->stats.as<unsigned long long>();
   r.status = b->status.as<unsigned long long>();
   return r;
@@ -166,7 +167,7 @@ static int enqueue_run(oco_batch *b, cudaStream_t s) {
     CU(launch_pillars_mixed_batch(b->rho, b->T, b->cols.as<MBatchCol>(), b->rec_pre.as<int64_t>(), b->ncol, b->nrec,
                                   b->fully_ionized_T, b->rec.as<float>(), b->colflag.as<unsigned>(), s));
     const MixedBatchArgs a = batch_args(b);
-    CU(cudaMemsetAsync(a.rcount, 0, 2 * sizeof(unsigned long long), s)); /* rcount, icount */
+    CU(cudaMemsetAsync(a.rcount, 0, 3 * sizeof(unsigned long long), s)); /* rcount, icount, the re-solve's queue */
     CU(cudaMemsetAsync(a.rbits, 0, (size_t)b->ncol * a.rwstride * sizeof(unsigned), s));
     CU(launch_batch_mixed(a, b->tiling == OCO_TILING_PACKED ? BATCH_TILING_PACKED : BATCH_TILING_WARP_COLUMN, blocks,
                           kBatchThreads, s));

@@ -204,6 +204,7 @@ struct RepairArgs {
                               k_repair_solve warp 4 x max_nz doubles (repair_capacity) */
   int64_t cap;             /* slots: items beyond are re-solved one warp per item */
   int max_nz;
+  unsigned long long *queue;   /* k_repair_coef's task counter, zero at launch */
   unsigned long long *repairs; /* += the re-solved items */
   unsigned long long *status;  /* zero-pivot words as in SolveArgs */
 };
