@@ -7,7 +7,7 @@
  *                     items with direct loads when nw is small.  Forward sweep: log2-space
  *                     opacity, scaled rows and the difference-form Thomas elimination in FP32
  *                     (the source function's exponent as integer + FP32 fraction),
- *                     writing kappa and a 16-byte scratch record per z (|gamma| or q, 1/kappa, u
+ *                     writing kappa and a scratch record per z (|gamma| or q, 1/kappa, u
  *                     mantissa and exponent); reverse sweep: extended-range FP32
  *                     back-substitution, the differences D_j, and the flux from a 6-value
  *                     window of differences, with FP64 outputs.
@@ -158,10 +158,58 @@ __device__ __forceinline__ MItem block_item(const MixedArgs &a, int64_t cl, int 
   return it;
 }
 
-/* One (column, wavelength) item.  Scratch: one float4 per z at s4[z * ss], each warp's levels
- * contiguous (ss = 32), so that a warp reads and writes one sequential stream (see the forward
- * sweep).  An inactive lane runs the forward sweep (to keep a staged warp in step) and writes
- * nothing. */
+/* The warp's Thomas scratch, one sequential stream per warp.  A record per level is
+ * {v, 1/kappa, u mantissa, u exponent} (see the forward sweep); two formats:
+ *   MScratch16  one float4 per lane, 512 bytes per level;
+ *   MScratch12  12 bytes per lane, 384 per level: the 32 lanes' {v, 1/kappa} pairs (float2),
+ *               then their u mantissas, with u's exponent packed into the spare bits of 1/kappa
+ *               and of the mantissa (pack_o1_u, mixed_core.h: u's mantissa lies in [1, 2)).  A
+ *               record whose u does not fit (exponent outside [-512, 511], or a mantissa that
+ *               is not normal) makes put() return false and the item is flagged for the FP64
+ *               re-solve (on the AGN and Athena-style grids the exponent stays in [-420, 90]).
+ * Both store the same values, so the results are the same bits.  The 12-byte records move a
+ * quarter less scratch for ~4% more instructions: the ragged batches (longest columns first, up
+ * to 2048 levels) use them (c4 batch 25.0 -> 23.7 ms), the block solves keep float4 records
+ * (12-byte records measured 0.7% slower on the 512-level AGN grid, 2% on the 1024-level
+ * precision grid). */
+struct MScratch16 {
+  static constexpr int LEVEL = 32 * 16;
+  char *w; /* the warp's level 0 */
+  int lane;
+  __device__ __forceinline__ float4 *p(int j) const { return (float4 *)(w + (int64_t)j * LEVEL) + lane; }
+  __device__ __forceinline__ const char *level(int j) const { return w + (int64_t)j * LEVEL; }
+  __device__ __forceinline__ bool put(int j, const float4 &r) const {
+    *p(j) = r;
+    return true;
+  }
+  __device__ __forceinline__ float4 get(int j) const { return *p(j); }
+  __device__ __forceinline__ float o1(int j) const { return p(j)->y; }
+};
+struct MScratch12 {
+  static constexpr int LEVEL = 32 * 12;
+  char *w; /* the warp's level 0 */
+  int lane;
+  __device__ __forceinline__ float2 *p2(int j) const { return (float2 *)(w + (int64_t)j * LEVEL) + lane; }
+  __device__ __forceinline__ float *p1(int j) const { return (float *)(w + (int64_t)j * LEVEL + 256) + lane; }
+  __device__ __forceinline__ const char *level(int j) const { return w + (int64_t)j * LEVEL; }
+  __device__ __forceinline__ bool put(int j, const float4 &r) const {
+    int w1, w2;
+    const bool fits = pack_o1_u(r.y, r.z, __float_as_int(r.w), w1, w2);
+    *p2(j) = make_float2(r.x, __int_as_float(w1));
+    *p1(j) = __int_as_float(w2);
+    return fits;
+  }
+  __device__ __forceinline__ float4 get(int j) const {
+    const float2 a = *p2(j);
+    float o1, m;
+    int e;
+    unpack_o1_u(__float_as_int(a.y), __float_as_int(*p1(j)), o1, m, e);
+    return make_float4(a.x, o1, m, __int_as_float(e));
+  }
+  __device__ __forceinline__ float o1(int j) const { return __int_as_float(__float_as_int(p2(j)->y) & 0x7fffffff); }
+};
+/* One (column, wavelength) item, its scratch records in sc.  An inactive lane runs the forward
+ * sweep (to keep a staged warp in step) and writes nothing. */
 /* Returns whether the item's emergent flux is ill-conditioned for this arithmetic: with
  * D_k = u_k - q_k U_{k+1} (all three terms >= 0) and the boundary flux proportional to
  * 37 D_a - 8 D_b + D_c (the 6th-order stencil with mirrored ghost differences; a, b, c the
@@ -169,11 +217,10 @@ __device__ __forceinline__ MItem block_item(const MixedArgs &a, int64_t cl, int 
  * errors of u, q and U is
  *   (37 C_a + 8 C_b + C_c) / |37 D_a - 8 D_b + D_c|,   C_k = u_k + q_k U_{k+1};
  * FP32 leaves relative errors of a few 1e-6 in u, q and U, so above `cond` the item is
- * flagged for the FP64 re-solve (kernels_repair.cu).  Columns with nz < 4 are never flagged (their flux is the
- * reference's stencil on U). */
-template <class PA>
-__device__ __forceinline__ bool msolve_item(const MItem &it, bool active, PA &pa, float4 *__restrict__ s4,
-                                            int64_t ss, float cond) {
+ * flagged for the FP64 re-solve (kernels_repair.cu).  Columns with nz < 4 are not tested (their flux is the
+ * reference's stencil on U).  An item whose scratch records do not fit MScratch is flagged too. */
+template <class PA, class SC>
+__device__ __forceinline__ bool msolve_item(const MItem &it, bool active, PA &pa, const SC &sc, float cond) {
   const int nz = it.nz;
   Lam32 L;
   load_lam32(L, it.lam, it.iw, it.nw);
@@ -196,6 +243,7 @@ __device__ __forceinline__ bool msolve_item(const MItem &it, bool active, PA &pa
    * smaller of q_j = h_j/(c_j+h_j) and |gamma_{j+1}| = c_j/(c_j+h_j) (they sum to 1; a negative
    * v_j stores -|gamma_{j+1}|), written once row j+1 is known */
   float4 pend = make_float4(0.0f, o1, u.m, __int_as_float(u.e));
+  bool fits = true;
   for (int j = 1; j < nz; j++) {
     cur = nxt;
     kc = kn;
@@ -210,7 +258,7 @@ __device__ __forceinline__ bool msolve_item(const MItem &it, bool active, PA &pa
     const float rr = rcp(cprev + h);
     const float qv = h * rr, gv = cprev * rr;
     pend.x = (qv < gv) ? qv : -gv;
-    s4[(int64_t)(j - 1) * ss] = pend;
+    fits &= sc.put(j - 1, pend);
     h = r.e + (r.a * rr) * h; /* a'/(c'+h) is O(1); a' h alone can overflow */
     const float rb = rcp(r.c + h);
     u = xaxpy(xexp2(r.ldi, r.ldf), r.w * rb, u, r.a * rb);
@@ -219,9 +267,9 @@ __device__ __forceinline__ bool msolve_item(const MItem &it, bool active, PA &pa
     pend = make_float4(0.0f, o1, u.m, __int_as_float(u.e));
     cprev = r.c;
   }
-  s4[(int64_t)(nz - 1) * ss] = pend;
+  fits &= sc.put(nz - 1, pend);
   if (!active) return false;
-  bool flag = false;
+  bool flag = !fits;
 
   /* reverse sweep */
   const int n = nz;
@@ -236,13 +284,13 @@ __device__ __forceinline__ bool msolve_item(const MItem &it, bool active, PA &pa
     double Uk[3];
     /* D_{n-2}, D_{n-3}, D_{n-4} first (top ghosts mirror them) */
     double Dt[3];
-    const float nx4_top_o1 = s4[(int64_t)(n - 1) * ss].y; /* 1/kappa_{n-1} */
+    const float nx4_top_o1 = sc.o1(n - 1); /* 1/kappa_{n-1} */
     float o1t[3];
     double Ct[3]; /* C_k = u_k + q_k U_{k+1} of the top differences */
 #pragma unroll
     for (int t = 0; t < 3; t++) {
       const int k = n - 2 - t;
-      const float4 w = s4[(int64_t)k * ss];
+      const float4 w = sc.get(k);
       o1t[t] = w.y;
       const float g1 = (w.x >= 0.0f) ? 1.0f - w.x : -w.x;
       const float qk = (w.x >= 0.0f) ? w.x : 1.0f + w.x;
@@ -305,20 +353,20 @@ __device__ __forceinline__ bool msolve_item(const MItem &it, bool active, PA &pa
        * have usually left L2) */
       if (k - PF + 1 - OCO_MIXED_L2_AHEAD >= 0 && (threadIdx.x & 31) == 0) /* PF levels, one bulk request */
         asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(__cvta_generic_to_global(
-                         s4 + (int64_t)(k - PF + 1 - OCO_MIXED_L2_AHEAD) * ss)),
-                     "r"((uint32_t)(PF * 32 * sizeof(float4)))
+                         sc.level(k - PF + 1 - OCO_MIXED_L2_AHEAD))),
+                     "r"((uint32_t)(PF * SC::LEVEL))
                      : "memory");
 #pragma unroll
-      for (int q = 0; q < PF; q++) w[q] = s4[(int64_t)(k - q) * ss];
+      for (int q = 0; q < PF; q++) w[q] = sc.get(k - q);
 #pragma unroll
       for (int q = 0; q < PF; q++) step(k - q, w[q]);
     }
-    for (; k >= 0; k--) step(k, s4[(int64_t)k * ss]);
+    for (; k >= 0; k--) step(k, sc.get(k));
     { /* condition number of the bottom flux from D_0, D_1, D_2 (d0, d1, d2) and U_1..U_3 */
       double Cb = 0.0;
 #pragma unroll
       for (int t = 0; t < 3; t++) {
-        const float4 w = s4[(int64_t)t * ss];
+        const float4 w = sc.get(t);
         const float qk = (w.x >= 0.0f) ? w.x : 1.0f + w.x;
         XF uj;
         uj.m = w.z;
@@ -346,7 +394,7 @@ __device__ __forceinline__ bool msolve_item(const MItem &it, bool active, PA &pa
     const int n1 = 3, n2 = nz + 2;
     f[n1 + nz - 1] = xtod(Un);
     for (int j = nz - 2; j >= 0; j--) {
-      const float4 w = s4[(int64_t)j * ss];
+      const float4 w = sc.get(j);
       const float g1 = (w.x >= 0.0f) ? 1.0f - w.x : -w.x;
       XF uj;
       uj.m = w.z;
@@ -364,7 +412,7 @@ __device__ __forceinline__ bool msolve_item(const MItem &it, bool active, PA &pa
     for (int j = 0; j < nz; j++) {
       const int c = n1 + j;
       const double df = (1.0 / 60.0) * (((45.0 * (f[c + 1] - f[c - 1])) - 9.0 * (f[c + 2] - f[c - 2])) + (f[c + 3] - f[c - 3]));
-      const double v = ((-(double)s4[(int64_t)j * ss].y) * df) * dz1;
+      const double v = ((-(double)sc.o1(j)) * df) * dz1;
       if (Vb) __stcs(&Vb[(int64_t)j * it.vz], v);
       if (j == 0) vbot = v;
       if (j == nz - 1) vtop = v;
@@ -415,6 +463,7 @@ __device__ __forceinline__ void mark_items(bool flag, int64_t word, int iw, unsi
   list_items(flag, m, id, word, iw, ilist, icount, slot);
 }
 
+template <class SC>
 __global__ void __launch_bounds__(128, 5) k_solve_mixed_staged(const MixedArgs a) {
   __shared__ __align__(128) float s_rec[MWARPS][2 * MZC * MZN];
   __shared__ __align__(8) unsigned long long s_bar[MWARPS][2];
@@ -422,7 +471,7 @@ __global__ void __launch_bounds__(128, 5) k_solve_mixed_staged(const MixedArgs a
   const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int ntiles = (a.nw + 31) / 32;
   const unsigned long long ntasks = (unsigned long long)a.ncol * ntiles;
-  float4 *s4 = a.s4 + slot * 32 * (int64_t)a.nz + lane; /* the warp's scratch: [z][lane], contiguous */
+  const SC sc{(char *)(a.s4 + slot * 32 * (int64_t)a.nz), lane}; /* the warp's scratch, contiguous */
   MStaged pa;
   pa.buf = s_rec[wib];
   pa.bar0 = msmem(&s_bar[wib][0]);
@@ -447,7 +496,7 @@ __global__ void __launch_bounds__(128, 5) k_solve_mixed_staged(const MixedArgs a
     const bool active = iw_raw < a.nw;
     const int iw = active ? iw_raw : a.nw - 1;
     pa.begin(a.rec + cl * (int64_t)a.nz * MZN);
-    const bool flag = msolve_item(block_item(a, cl, iw), active, pa, s4, 32, a.repair_cond) ||
+    const bool flag = msolve_item(block_item(a, cl, iw), active, pa, sc, a.repair_cond) ||
                       (active && __ldg(a.colflag + cl) != 0u);
     if (__any_sync(0xffffffffu, pa.failed)) {
       if (lane == 0) atomicOr(&a.status[2], 1ull);
@@ -460,12 +509,13 @@ __global__ void __launch_bounds__(128, 5) k_solve_mixed_staged(const MixedArgs a
   }
 }
 
+template <class SC>
 __global__ void __launch_bounds__(128, 5) k_solve_mixed(const MixedArgs a) {
   const int lane = threadIdx.x & 31;
   const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nitems = a.ncol * a.nw;
   const unsigned long long ntasks = (unsigned long long)((nitems + 31) / 32);
-  float4 *s4 = a.s4 + slot * 32 * (int64_t)a.nz + lane; /* the warp's scratch: [z][lane], contiguous */
+  const SC sc{(char *)(a.s4 + slot * 32 * (int64_t)a.nz), lane}; /* the warp's scratch, contiguous */
   for (;;) {
     unsigned long long task = 0;
     if (lane == 0) task = atomicAdd(a.work, 1ull);
@@ -479,7 +529,7 @@ __global__ void __launch_bounds__(128, 5) k_solve_mixed(const MixedArgs a) {
       const int64_t cl = item / a.nw;
       iw = (int)(item - cl * a.nw);
       MDirect pa{a.rec + cl * (int64_t)a.nz * MZN};
-      flag = msolve_item(block_item(a, cl, iw), true, pa, s4, 32, a.repair_cond) || __ldg(a.colflag + cl) != 0u;
+      flag = msolve_item(block_item(a, cl, iw), true, pa, sc, a.repair_cond) || __ldg(a.colflag + cl) != 0u;
       word = cl * ((a.nw + 31) / 32) + iw / 32;
     }
     mark_items(flag, word, iw, (unsigned long long)item, a.rbits, a.rslot, a.rlist, a.rcount, a.ilist, a.icount);
@@ -488,20 +538,19 @@ __global__ void __launch_bounds__(128, 5) k_solve_mixed(const MixedArgs a) {
 
 static bool mixed_uses_staging(int nw) { return (nw >= 64) || (nw % 32) == 0; }
 
+static const void *solve_mixed_fn(int nw) {
+  return mixed_uses_staging(nw) ? (const void *)k_solve_mixed_staged<MScratch16> : (const void *)k_solve_mixed<MScratch16>;
+}
+
 int solve_mixed_max_blocks_per_sm(int threads, int nw) {
   int n = 0;
-  const cudaError_t e = mixed_uses_staging(nw)
-                            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solve_mixed_staged, threads, 0)
-                            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solve_mixed, threads, 0);
+  const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, solve_mixed_fn(nw), threads, 0);
   return (e == cudaSuccess && n > 0) ? n : 1;
 }
 
 cudaError_t launch_solve_mixed(const MixedArgs &a, int blocks, int threads, cudaStream_t s) {
-  if (mixed_uses_staging(a.nw))
-    k_solve_mixed_staged<<<blocks, threads, 0, s>>>(a);
-  else
-    k_solve_mixed<<<blocks, threads, 0, s>>>(a);
-  return cudaGetLastError();
+  void *args[] = {(void *)&a};
+  return cudaLaunchKernel(solve_mixed_fn(a.nw), dim3(blocks), dim3(threads), args, 0, s);
 }
 
 /* ---- ragged batches ---------------------------------------------------------------------- */
@@ -536,12 +585,13 @@ __device__ __forceinline__ MItem batch_item(const MixedBatchArgs &b, const MBatc
 
 /* Warp-column tiling: tasks (column, 32-wavelength tile) from the device queue, longest
  * columns first; the column's records stream through the warp's shared-memory buffers. */
+template <class SC>
 __global__ void __launch_bounds__(128, 5) k_batch_mixed_staged(const MixedBatchArgs b) {
   __shared__ __align__(128) float s_rec[MWARPS][2 * MZC * MZN];
   __shared__ __align__(8) unsigned long long s_bar[MWARPS][2];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  float4 *s4 = b.s4 + slot * 32 * (int64_t)b.max_nz + lane; /* the warp's scratch: [z][lane], contiguous */
+  const SC sc{(char *)(b.s4 + slot * 32 * (int64_t)b.max_nz), lane}; /* the warp's scratch, contiguous */
   MStaged pa;
   pa.buf = s_rec[wib];
   pa.bar0 = msmem(&s_bar[wib][0]);
@@ -566,7 +616,7 @@ __global__ void __launch_bounds__(128, 5) k_batch_mixed_staged(const MixedBatchA
     const int iw = active ? iw_raw : c.nw - 1;
     pa.nz = c.nz;
     pa.begin(b.rec + c.rec_off * MZN);
-    const bool flag = msolve_item(batch_item(b, c, iw), active, pa, s4, 32, b.repair_cond) ||
+    const bool flag = msolve_item(batch_item(b, c, iw), active, pa, sc, b.repair_cond) ||
                       (active && __ldg(b.colflag + t.x) != 0u);
     if (__any_sync(0xffffffffu, pa.failed)) {
       if (lane == 0) atomicOr(&b.status[2], 1ull);
@@ -582,10 +632,11 @@ __global__ void __launch_bounds__(128, 5) k_batch_mixed_staged(const MixedBatchA
 /* Packed tiling: the (column, wavelength) items of the columns sorted by nz (longest first)
  * form one list; a warp takes 32 consecutive items, so partial wavelength tiles of one column
  * are filled with the next column's items (similar nz, as the list is sorted). */
+template <class SC>
 __global__ void __launch_bounds__(128, 5) k_batch_mixed_packed(const MixedBatchArgs b) {
   const int lane = threadIdx.x & 31;
   const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  float4 *s4 = b.s4 + slot * 32 * (int64_t)b.max_nz + lane; /* the warp's scratch: [z][lane], contiguous */
+  const SC sc{(char *)(b.s4 + slot * 32 * (int64_t)b.max_nz), lane}; /* the warp's scratch, contiguous */
   for (;;) {
     unsigned long long task = 0;
     if (lane == 0) task = atomicAdd(b.work, 1ull);
@@ -608,28 +659,28 @@ __global__ void __launch_bounds__(128, 5) k_batch_mixed_packed(const MixedBatchA
       iw = (int)(item - __ldg(b.item_pre + lo));
       const MBatchCol c = b.cols[col];
       MDirect pa{b.rec + c.rec_off * MZN};
-      flag = msolve_item(batch_item(b, c, iw), true, pa, s4, 32, b.repair_cond) || __ldg(b.colflag + col) != 0u;
+      flag = msolve_item(batch_item(b, c, iw), true, pa, sc, b.repair_cond) || __ldg(b.colflag + col) != 0u;
     }
     mark_items(flag, (int64_t)col * b.rwstride + iw / 32, iw, ((unsigned long long)(unsigned)col << 32) | (unsigned)iw,
                b.rbits, b.rslot, b.rlist, b.rcount, b.ilist, b.icount);
   }
 }
 
+static const void *batch_mixed_fn(int tiling) {
+  return tiling == BATCH_TILING_PACKED ? (const void *)k_batch_mixed_packed<MScratch12>
+                                       : (const void *)k_batch_mixed_staged<MScratch12>;
+}
+
 int batch_mixed_max_blocks_per_sm(int tiling, int threads) {
   int n = 0;
-  cudaError_t e = tiling == BATCH_TILING_PACKED
-                      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_mixed_packed, threads, 0)
-                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_mixed_staged, threads, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_mixed_fn(tiling), threads, 0);
   if (e != cudaSuccess || n < 1) n = 1;
   return n;
 }
 
 cudaError_t launch_batch_mixed(const MixedBatchArgs &a, int tiling, int blocks, int threads, cudaStream_t s) {
-  if (tiling == BATCH_TILING_PACKED)
-    k_batch_mixed_packed<<<blocks, threads, 0, s>>>(a);
-  else
-    k_batch_mixed_staged<<<blocks, threads, 0, s>>>(a);
-  return cudaGetLastError();
+  void *args[] = {(void *)&a};
+  return cudaLaunchKernel(batch_mixed_fn(tiling), dim3(blocks), dim3(threads), args, 0, s);
 }
 
 }  // namespace oco

@@ -516,6 +516,22 @@ MX_HD double xtod(XF x) {
   return (double)x.m * oco_u2d((uint64_t)(int64_t)(x.e + 1023) << 52);
 }
 
+/* 1/kappa (> 0) and an XF u = m 2^e with m in [1, 2) in two 32-bit words: w1 = 1/kappa with
+ * bit 9 of e + 512 in its sign bit, w2 = m's 23 fraction bits with bits 0-8 of e + 512 in its
+ * sign and exponent field.  Returns whether the pair fits (e in [-512, 511], m normal in
+ * [1, 2)); unpacking a fitting pair gives the same bits back. */
+MX_HD bool pack_o1_u(float o1, float m, int e, int &w1, int &w2) {
+  const int mb = f2bits(m), eb = e + 512;
+  w1 = f2bits(o1) | ((eb & 0x200) << 22);
+  w2 = (mb & 0x7fffff) | ((eb & 0x1ff) << 23);
+  return ((unsigned)eb < 1024u) & ((mb >> 23) == 127);
+}
+MX_HD void unpack_o1_u(int w1, int w2, float &o1, float &m, int &e) {
+  o1 = bits2f(w1 & 0x7fffffff);
+  m = bits2f((w2 & 0x7fffff) | 0x3f800000);
+  e = (((w2 >> 23) & 0x1ff) | ((w1 >> 22) & 0x200)) - 512;
+}
+
 /* ---- scaled tridiagonal rows (auxiliary.f90:125-201 divided by kappa_i^2) ------------- */
 struct Row32 {
   float a, c, e;  /* sub, super, diagonal excess -(a+b+c) */

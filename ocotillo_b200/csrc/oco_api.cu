@@ -301,7 +301,7 @@ static int check_params(oco_ctx *c, const oco_params *p) {
 static const int kSolveThreads = 128;
 
 /* Grid of the persistent solve kernel and its scratch: per resident thread and z, FP64
- * gamma, u, 1/kappa, q (32 B) or, for the mixed form, one float4 (16 B). */
+ * gamma, u, 1/kappa, q (32 B) or, for the mixed form, one record of at most 16 B. */
 static int prepare_solve(oco_ctx *c, int form, int grey, int64_t nitems, int nz, int *blocks) {
   const bool mixed = form == OCO_FORM_MIXED;
   int bps = mixed ? solve_mixed_max_blocks_per_sm(kSolveThreads, c->nw)

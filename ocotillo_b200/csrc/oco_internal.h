@@ -160,7 +160,7 @@ struct MixedBatchArgs {
   int64_t ncol, ntasks, nitems;
   double *U, *K, *V, *Vtop, *Vbot;
   int layout;
-  float4 *s4;        /* scratch [warp slot][max_nz][32] */
+  float4 *s4;        /* scratch: per warp slot max_nz levels of 32 12-byte records (MScratch12) */
   int64_t slot_stride; /* resident threads the scratch is sized for */
   int max_nz;
   unsigned long long *work;

@@ -46,3 +46,14 @@ extern "C" void mixed_host_solve(const double *rho, const double *T, const doubl
     }
   }
 }
+
+// The 12-byte scratch record's packing of 1/kappa and u (pack_o1_u / unpack_o1_u) over n triples:
+// fits[i], and the unpacked values' bits.
+extern "C" void mixed_host_pack_roundtrip(const float *o1, const float *m, const int *e, int n, int *fits, float *o1r,
+                                          float *mr, int *er) {
+  for (int i = 0; i < n; i++) {
+    int w1, w2;
+    fits[i] = mx::pack_o1_u(o1[i], m[i], e[i], w1, w2) ? 1 : 0;
+    mx::unpack_o1_u(w1, w2, o1r[i], mr[i], er[i]);
+  }
+}

@@ -109,3 +109,38 @@ def test_mixed_host_short_columns(host_lib, oracle, nz, nw):
         rV = ref["V"].reshape(nw, 6, nz)
         for end in (-1, 0):
             assert rel(V[..., end], rV[..., end]).max() <= 1e-4, end
+
+
+def test_scratch_record_packing(host_lib):
+    """The ragged-batch kernels' 12-byte scratch record packs u's exponent into the spare bits
+    of 1/kappa (> 0) and of u's mantissa (in [1, 2)): every fitting record comes back with the
+    same bits, and every record outside the packable range reports that it does not fit (the
+    kernel then flags the item for the FP64 re-solve)."""
+    rng = np.random.default_rng(7)
+    n = 200000
+    o1 = (10.0 ** rng.uniform(-38, 38, n)).astype(np.float32)
+    m = (1.0 + rng.random(n)).astype(np.float32)
+    m[m >= 2.0] = np.float32(1.9999999)
+    e = rng.integers(-600, 600, n).astype(np.int32)
+    edge = np.array([-512, 511, -513, 512, 0, -1], dtype=np.int32)
+    e[:edge.size] = edge
+    o1[:4] = [np.float32(1.0), np.finfo(np.float32).max, np.finfo(np.float32).tiny, np.float32(3e-39)]
+    m[6:12] = [1.0, np.nextafter(np.float32(2.0), np.float32(0.0)), 0.0, 2.0, 0.5, -1.5]
+    fits = np.zeros(n, dtype=np.int32)
+    o1r = np.zeros(n, dtype=np.float32)
+    mr = np.zeros(n, dtype=np.float32)
+    er = np.zeros(n, dtype=np.int32)
+    pf = ctypes.POINTER(ctypes.c_float)
+    pi = ctypes.POINTER(ctypes.c_int)
+    host_lib.mixed_host_pack_roundtrip.argtypes = [pf, pf, pi, ctypes.c_int, pi, pf, pf, pi]
+    host_lib.mixed_host_pack_roundtrip(o1.ctypes.data_as(pf), m.ctypes.data_as(pf), e.ctypes.data_as(pi), n,
+                                       fits.ctypes.data_as(pi), o1r.ctypes.data_as(pf), mr.ctypes.data_as(pf),
+                                       er.ctypes.data_as(pi))
+    normal_m = (m >= 1.0) & (m < 2.0)
+    expect = (e >= -512) & (e <= 511) & normal_m
+    assert np.array_equal(fits.astype(bool), expect)
+    ok = expect
+    assert ok.sum() > n // 2
+    assert np.array_equal(o1r[ok].view(np.uint32), o1[ok].view(np.uint32))
+    assert np.array_equal(mr[ok].view(np.uint32), m[ok].view(np.uint32))
+    assert np.array_equal(er[ok], e[ok])
