@@ -36,34 +36,70 @@ namespace oco {
 #endif
 #endif
 
-__global__ void __launch_bounds__(256) k_pillars(const double *__restrict__ rho,
-                                                 const double *__restrict__ T, int64_t n,
-                                                 double fully_ionized_T, int grey,
-                                                 double *__restrict__ pil) {
-  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  pillar_record(rho[i], T[i], fully_ionized_T, grey, pil + i * NF);
+constexpr int PIL_THREADS = 128;
+constexpr int PIL_STRIDE = NF + 1; /* doubles per record in shared memory (odd: no bank conflicts) */
+
+/* Writes the warp's records (lane l: record i0 + l, held in r) to pil with coalesced stores:
+ * each lane puts its record in the warp's shared buffer, then the warp copies the 32
+ * consecutive records out (records at or beyond n are not written). */
+__device__ __forceinline__ void store_pillars(const double *r, double *__restrict__ buf, double *__restrict__ pil,
+                                              int64_t i0, int64_t n) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < NF; k++) buf[lane * PIL_STRIDE + k] = r[k];
+  __syncwarp();
+  double *o = pil + i0 * NF;
+#pragma unroll
+  for (int m = 0; m < NF; m++) {
+    const int j = lane + 32 * m, q = j / NF, f = j % NF;
+    if (i0 + q < n) o[j] = buf[q * PIL_STRIDE + f];
+  }
+}
+
+__global__ void __launch_bounds__(PIL_THREADS) k_pillars(const double *__restrict__ rho,
+                                                         const double *__restrict__ T, int64_t n,
+                                                         double fully_ionized_T, int grey,
+                                                         double *__restrict__ pil) {
+  __shared__ double s_buf[PIL_THREADS / 32][32 * PIL_STRIDE];
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t i0 = i - (threadIdx.x & 31);
+  if (i0 >= n) return; /* whole warp past the end */
+  double r[NF];
+#pragma unroll
+  for (int k = 0; k < NF; k++) r[k] = 0.0; /* grey records set three fields */
+  if (i < n) pillar_record(rho[i], T[i], fully_ionized_T, grey, r);
+  store_pillars(r, s_buf[threadIdx.x >> 5], pil, i0, n);
 }
 
 /* Batch records: thread i is record i of the dense [sum nz] list; its column comes from a
  * binary search of the nz prefix sums rec_pre[0..ncol]. */
-__global__ void __launch_bounds__(256) k_pillars_batch(const double *__restrict__ rho,
-                                                       const double *__restrict__ T,
-                                                       const MBatchCol *__restrict__ cols,
-                                                       const int64_t *__restrict__ rec_pre, int64_t ncol, int64_t n,
-                                                       double fully_ionized_T, double *__restrict__ pil) {
+__global__ void __launch_bounds__(PIL_THREADS) k_pillars_batch(const double *__restrict__ rho,
+                                                               const double *__restrict__ T,
+                                                               const MBatchCol *__restrict__ cols,
+                                                               const int64_t *__restrict__ rec_pre, int64_t ncol,
+                                                               int64_t n, double fully_ionized_T,
+                                                               double *__restrict__ pil) {
+  __shared__ double s_buf[PIL_THREADS / 32][32 * PIL_STRIDE];
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int64_t lo = 0, hi = ncol;
-  while (hi - lo > 1) {
-    const int64_t mid = (lo + hi) >> 1;
-    if (rec_pre[mid] <= i)
-      lo = mid;
-    else
-      hi = mid;
+  const int64_t i0 = i - (threadIdx.x & 31);
+  if (i0 >= n) return; /* whole warp past the end */
+  double r[NF];
+  if (i < n) {
+    int64_t lo = 0, hi = ncol;
+    while (hi - lo > 1) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (rec_pre[mid] <= i)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const int64_t src = cols[lo].in_off + (i - rec_pre[lo]);
+    pillar_record(rho[src], T[src], fully_ionized_T, 0, r);
+  } else {
+#pragma unroll
+    for (int k = 0; k < NF; k++) r[k] = 0.0; /* not stored */
   }
-  const int64_t src = cols[lo].in_off + (i - rec_pre[lo]);
-  pillar_record(rho[src], T[src], fully_ionized_T, 0, pil + i * NF);
+  store_pillars(r, s_buf[threadIdx.x >> 5], pil, i0, n);
 }
 
 /* ---- pillar access ------------------------------------------------------------------- */
@@ -355,8 +391,8 @@ __global__ void __launch_bounds__(128, 4) k_batch_fp64_staged(const FP64BatchArg
 cudaError_t launch_pillars_batch(const double *rho, const double *T, const MBatchCol *cols, const int64_t *rec_pre,
                                  int64_t ncol, int64_t nrec, double fully_ionized_T, double *pil, cudaStream_t s) {
   if (nrec == 0) return cudaSuccess;
-  k_pillars_batch<<<(unsigned)((nrec + 255) / 256), 256, 0, s>>>(rho, T, cols, rec_pre, ncol, nrec, fully_ionized_T,
-                                                                 pil);
+  k_pillars_batch<<<(unsigned)((nrec + PIL_THREADS - 1) / PIL_THREADS), PIL_THREADS, 0, s>>>(
+      rho, T, cols, rec_pre, ncol, nrec, fully_ionized_T, pil);
   return cudaGetLastError();
 }
 
@@ -379,9 +415,8 @@ cudaError_t launch_pillars(const double *rho, const double *T, int64_t ncol, int
                            double fully_ionized_T, int grey, double *pil, cudaStream_t s) {
   int64_t n = ncol * nz;
   if (n == 0) return cudaSuccess;
-  int threads = 256;
-  int64_t blocks = (n + threads - 1) / threads;
-  k_pillars<<<(unsigned)blocks, threads, 0, s>>>(rho, T, n, fully_ionized_T, grey, pil);
+  const int64_t blocks = (n + PIL_THREADS - 1) / PIL_THREADS;
+  k_pillars<<<(unsigned)blocks, PIL_THREADS, 0, s>>>(rho, T, n, fully_ionized_T, grey, pil);
   return cudaGetLastError();
 }
 
