@@ -565,7 +565,7 @@ __device__ __forceinline__ MItem batch_item(const MixedBatchArgs &b, const MBatc
   it.dzf = c.dzf;
   it.ldz2i = c.ldz2i;
   it.ldz2f = c.ldz2f;
-  it.dz2f = (float)(1.0 / (c.dz1 * c.dz1));
+  it.dz2f = (float)c.dz2; /* as block_item's (float)(dz * dz) */
   it.dz1 = c.dz1;
   if (b.layout == 0) { /* per column [lambda][z] (z fastest) */
     it.U = b.U ? b.U + c.u_off + (int64_t)iw * (c.nz + 6) : nullptr;

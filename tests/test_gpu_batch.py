@@ -1,11 +1,11 @@
 """Ragged batches (oco_batch_*): independent columns of different nz, dz and wavelength grids
 in one persistent launch replayed as a CUDA graph.
 
-Mixed form: per column the batch runs the arithmetic of the block solve's mixed form, so every
-column is compared with a 1x1 block solve of the same column (relative difference <= 1e-6:
-same operations, possibly contracted into FMAs differently by the two kernel instantiations),
-and a few columns with the stable FP64 oracle at the mixed form's tolerances.  Tilings and
-graph replays must give identical results.
+Mixed form: per column the batch runs the arithmetic of the block solve's mixed form (the
+batch kernels keep their Thomas scratch in 12-byte records, the block kernels in float4 ones,
+holding the same values), so every column must equal a 1x1 block solve of it bit for bit; a
+few columns are also compared with the stable FP64 oracle at the mixed form's tolerances.
+Tilings and graph replays must give identical results.
 
 Plain and stable FP64 forms: per item the block solve's FP64 arithmetic, so every column must
 equal a 1x1 block solve of it bit for bit, and the plain form must equal the oracle (reference
@@ -16,7 +16,6 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-TOL_SAME = 1e-6
 TOL_FLUX, TOL_KAPPA, TOL_U = 1e-4, 3e-5, 5e-4
 
 
@@ -114,10 +113,11 @@ def test_batch_matches_block_solve(engine, layout):
         vt = b.column(out, i, "Vtop").cpu().numpy()
         vb = b.column(out, i, "Vbot").cpu().numpy()
         what = f"column {i} nz={d['nz'][i]} nw={d['nw'][i]} layout={layout}"
-        assert _rel(U, ref["U"][:, 0, 0, :].T) <= TOL_SAME, what
-        assert _rel(K, ref["kappa"][:, 0, 0, :].T) <= TOL_SAME, what
-        vmax = np.abs(ref["V"][:, 0, 0, :]).max()
-        assert np.abs(V - ref["V"][:, 0, 0, :].T).max() <= TOL_SAME * vmax, what
+        # the same arithmetic per item (the batch kernels keep 12-byte scratch records, the
+        # block kernels float4 ones, which hold the same values): bit for bit
+        assert _same(U, ref["U"][:, 0, 0, :].T), what
+        assert _same(K, ref["kappa"][:, 0, 0, :].T), what
+        assert _same(V, ref["V"][:, 0, 0, :].T), what
         assert np.array_equal(vt, V[-1]) and np.array_equal(vb, V[0]), what
     b.close()
 
