@@ -57,3 +57,53 @@ extern "C" void mixed_host_pack_roundtrip(const float *o1, const float *m, const
     mx::unpack_o1_u(w1, w2, o1r[i], mr[i], er[i]);
   }
 }
+
+// The extended exponents of the forward sweep's u over every item of the columns (after each
+// item, solve_item_host leaves u's mantissas in work[nz, 2nz) and exponents in work[4nz, 5nz)):
+// out[0] = min exponent, out[1] = max, out[2] = mantissas outside [1, 2).
+extern "C" void mixed_host_u_exponents(const double *rho, const double *T, const double *wa, int ncol, int nz, int nw,
+                                       double dz, double fully_ionized_T, int *out) {
+  std::vector<double> tab((size_t)NL * nw);
+  fill_lambda_table(wa, nw, tab.data());
+  std::vector<float> Z((size_t)nz * mx::MZN), work((size_t)8 * nz);
+  std::vector<double> dwork((size_t)nz + 6), U((size_t)nz + 6), K((size_t)nz), V((size_t)nz);
+  int emin = 1 << 30, emax = -(1 << 30), bad = 0;
+  for (int c = 0; c < ncol; c++) {
+    for (int z = 0; z < nz; z++) mx::pillar(rho[(size_t)c * nz + z], T[(size_t)c * nz + z], fully_ionized_T, &Z[(size_t)z * mx::MZN]);
+    for (int iw = 0; iw < nw; iw++) {
+      auto t = [&](int f) { return tab[(size_t)f * nw + iw]; };
+      mx::LamIn li;
+      li.chi = t(L_CHI);
+      li.gff = t(L_GFF);
+      li.chi1 = t(L_CHI1);
+      li.wa3 = t(L_WA3);
+      li.s = t(L_SCOEF);
+      li.hmon = t(L_HMON);
+      li.f1 = t(L_F1);
+      li.f2 = t(L_F2);
+      li.f3 = t(L_F3);
+      for (int q = 0; q < 6; q++) li.gn[q] = t(L_GN1 + q);
+      li.nu9 = t(L_NU9);
+      li.l3nu = t(L_L3NU);
+      li.hnuk = t(L_HNUK);
+      li.wcm1 = t(L_WCM1);
+      li.sw5 = t(L_SW5);
+      float lr[mx::MLN];
+      mx::lambda_record(li, lr);
+      mx::Lam32 L;
+      mx::lam32_from(L, [&](int f) { return lr[f]; });
+      auto zat = [&](int z) { return &Z[(size_t)z * mx::MZN]; };
+      mx::solve_item_host(zat, L, nz, dz, work.data(), dwork.data(), U.data(), K.data(), V.data());
+      const float *um = work.data() + nz;
+      const int *ue = reinterpret_cast<const int *>(work.data() + 4 * nz);
+      for (int j = 0; j < nz; j++) {
+        emin = ue[j] < emin ? ue[j] : emin;
+        emax = ue[j] > emax ? ue[j] : emax;
+        if (!(um[j] >= 1.0f && um[j] < 2.0f)) bad++;
+      }
+    }
+  }
+  out[0] = emin;
+  out[1] = emax;
+  out[2] = bad;
+}

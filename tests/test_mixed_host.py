@@ -144,3 +144,41 @@ def test_scratch_record_packing(host_lib):
     assert np.array_equal(o1r[ok].view(np.uint32), o1[ok].view(np.uint32))
     assert np.array_equal(mr[ok].view(np.uint32), m[ok].view(np.uint32))
     assert np.array_equal(er[ok], e[ok])
+
+
+@pytest.mark.parametrize("case", ["agn", "precision", "athena"])
+def test_u_exponents_fit_the_packed_scratch_record(host_lib, case):
+    """The ragged-batch kernels pack u's binary exponent into 10 bits (e + 512 in [0, 1023]) and
+    rely on u's mantissa lying in [1, 2); an item whose records do not fit is flagged for the
+    FP64 re-solve, so this is about cost, not correctness.  On the benchmark constructions the
+    forward sweep's u keeps its mantissa normalised and its exponent well inside the range."""
+    from ocotillo_b200 import workloads
+    if case == "agn":
+        rho, T, dz = workloads.agn_block(2, 2, 512)
+        wa = workloads.log_wavelengths(64)
+    elif case == "precision":
+        rho, T, dz, _ = workloads.precision_block(2, 1, 1024)
+        wa = workloads.log_wavelengths(64)
+    else:
+        rng = np.random.default_rng(4)
+        cols = [workloads.athena_column(nz, rng) for nz in (64, 300, 2048)]
+        out = []
+        for r, t, d in cols:
+            out.append(_exponents(host_lib, r.reshape(1, -1), t.reshape(1, -1), workloads.log_wavelengths(48), d))
+        emin, emax, bad = min(o[0] for o in out), max(o[1] for o in out), sum(o[2] for o in out)
+        assert bad == 0 and -480 <= emin and emax <= 400, (emin, emax, bad)
+        return
+    nz = rho.shape[-1]
+    emin, emax, bad = _exponents(host_lib, rho.reshape(-1, nz), T.reshape(-1, nz), wa, dz)
+    assert bad == 0 and -480 <= emin and emax <= 400, (emin, emax, bad)
+
+
+def _exponents(h, rho, T, wa, dz):
+    ncol, nz = rho.shape
+    out = (ctypes.c_int * 3)()
+    h.mixed_host_u_exponents.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                         ctypes.c_double, ctypes.POINTER(ctypes.c_int)]
+    p = lambda a: np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(P)
+    wa = np.ascontiguousarray(wa, dtype=np.float64)
+    h.mixed_host_u_exponents(p(rho), p(T), wa.ctypes.data_as(P), ncol, nz, len(wa), dz, 2e4, out)
+    return out[0], out[1], out[2]
